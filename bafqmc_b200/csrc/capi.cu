@@ -1,0 +1,642 @@
+// C ABI of the B200 BAFQMC sweep (include/bafqmc_b200.h): host-side model set
+// up (lattice tables, kinetic propagators, HS factors, initial fields) and the
+// device state of a batch of chains.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bafqmc_b200.h"
+#include "kernels.h"
+#include "sweep.cuh"
+
+using bq::ChainDev;
+using bq::ChainScalars;
+using bq::PointDev;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(BAFQMC_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                                 \
+    do {                                                         \
+        cudaError_t _e = (call);                                 \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);      \
+    } while (0)
+
+typedef std::vector<double> dvec;
+struct zmat {   // row-major complex n x n
+    int n;
+    std::vector<double> a;   // interleaved
+    explicit zmat(int n_ = 0) : n(n_), a(2 * (size_t)n_ * n_, 0.0) {}
+    double& re(int i, int j) { return a[2 * ((size_t)i * n + j)]; }
+    double& im(int i, int j) { return a[2 * ((size_t)i * n + j) + 1]; }
+};
+
+zmat zmul(const zmat& A, const zmat& B) {
+    const int n = A.n;
+    zmat C(n);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k) {
+            const double ar = A.a[2 * ((size_t)i * n + k)], ai = A.a[2 * ((size_t)i * n + k) + 1];
+            if (ar == 0.0 && ai == 0.0) continue;
+            for (int j = 0; j < n; ++j) {
+                const double br = B.a[2 * ((size_t)k * n + j)], bi = B.a[2 * ((size_t)k * n + j) + 1];
+                C.a[2 * ((size_t)i * n + j)] += ar * br - ai * bi;
+                C.a[2 * ((size_t)i * n + j) + 1] += ar * bi + ai * br;
+            }
+        }
+    return C;
+}
+
+// exp(s * H) by scaling and squaring of the Taylor series (degree 24 after
+// scaling to norm <= 1/2; truncation error < 1e-30 relative before squaring).
+// Stands in for the ZHEEV-based opT_set (non_interact.f90:74-109).
+zmat expm_scaled(const zmat& H, double s) {
+    const int n = H.n;
+    zmat A(n);
+    double norm1 = 0.0;
+    for (int j = 0; j < n; ++j) {
+        double col = 0.0;
+        for (int i = 0; i < n; ++i) col += std::hypot(H.a[2 * ((size_t)i * n + j)], H.a[2 * ((size_t)i * n + j) + 1]);
+        norm1 = std::max(norm1, col);
+    }
+    norm1 *= std::fabs(s);
+    int sq = 0;
+    while (norm1 > 0.5) {
+        norm1 *= 0.5;
+        ++sq;
+    }
+    const double scale = s * std::ldexp(1.0, -sq);
+    for (size_t k = 0; k < A.a.size(); ++k) A.a[k] = H.a[k] * scale;
+    zmat E(n), term(n);
+    for (int i = 0; i < n; ++i) {
+        E.re(i, i) = 1.0;
+        term.re(i, i) = 1.0;
+    }
+    for (int k = 1; k <= 24; ++k) {
+        term = zmul(term, A);
+        const double inv = 1.0 / k;
+        for (size_t q = 0; q < term.a.size(); ++q) term.a[q] *= inv;
+        for (size_t q = 0; q < E.a.size(); ++q) E.a[q] += term.a[q];
+    }
+    for (int k = 0; k < sq; ++k) E = zmul(E, E);
+    return E;
+}
+
+const double kPI = std::acos(-1.0);
+
+struct HostLattice {   // lattice.f90:21-125 (Norb = 1)
+    int nlx, nly, lq;
+    std::vector<int> cellx, celly, inv_cell, bonds, imj;
+    std::vector<double> aimj, xk;
+    bool hasK;
+    int indexK;
+    int cell(int nx, int ny) const { return inv_cell[(size_t)(ny - 1) * nlx + (nx - 1)]; }
+
+    HostLattice(int lx, int ly) : nlx(lx), nly(ly), lq(lx * ly) {
+        inv_cell.assign((size_t)lq, 0);
+        cellx.resize(lq);
+        celly.resize(lq);
+        int nc = 0;
+        for (int ny = 1; ny <= nly; ++ny)
+            for (int nx = 1; nx <= nlx; ++nx) {
+                cellx[nc] = nx;
+                celly[nc] = ny;
+                inv_cell[(size_t)(ny - 1) * nlx + (nx - 1)] = nc;
+                ++nc;
+            }
+        auto npbc = [](int nr, int L) { return nr > L ? nr - L : (nr < 1 ? nr + L : nr); };
+        imj.resize((size_t)lq * lq);
+        for (int jj = 0; jj < lq; ++jj)
+            for (int ii = 0; ii < lq; ++ii) {
+                const int dx = ((cellx[ii] - cellx[jj]) % nlx + nlx) % nlx + 1;
+                const int dy = ((celly[ii] - celly[jj]) % nly + nly) % nly + 1;
+                imj[(size_t)ii * lq + jj] = cell(dx, dy);
+            }
+        const double a1[2] = {1.0, 0.0}, a2[2] = {0.5, std::sqrt(3.0) / 2.0};
+        const double b1[2] = {2.0 * kPI, -2.0 * kPI / std::sqrt(3.0)}, b2[2] = {0.0, 4.0 * kPI / std::sqrt(3.0)};
+        aimj.resize(2 * (size_t)lq);
+        xk.resize(2 * (size_t)lq);
+        for (int ii = 0; ii < lq; ++ii) {
+            const int ix = cellx[ii], iy = celly[ii];
+            aimj[2 * ii] = (ix - 1) * a1[0] + (iy - 1) * a2[0];
+            aimj[2 * ii + 1] = (ix - 1) * a1[1] + (iy - 1) * a2[1];
+            xk[2 * ii] = (ix - 1) * b1[0] / nlx + (iy - 1) * b2[0] / nly;
+            xk[2 * ii + 1] = (ix - 1) * b1[1] / nlx + (iy - 1) * b2[1] / nly;
+        }
+        bonds.resize(3 * (size_t)lq);
+        for (int iy = 1; iy <= nly; ++iy)
+            for (int ix = 1; ix <= nlx; ++ix) {
+                const int i = cell(ix, iy);
+                bonds[3 * i + 0] = cell(npbc(ix + 1, nlx), npbc(iy, nly));
+                bonds[3 * i + 1] = cell(npbc(ix, nlx), npbc(iy + 1, nly));
+                bonds[3 * i + 2] = cell(npbc(ix - 1, nlx), npbc(iy + 1, nly));
+            }
+        hasK = (nlx % 3 == 0) && (nly % 3 == 0);
+        indexK = hasK ? cell(2 * nlx / 3 + 1, nly / 3 + 1) : 0;
+    }
+    double k_dot_r(int k, int r) const { return xk[2 * k] * aimj[2 * r] + xk[2 * k + 1] * aimj[2 * r + 1]; }
+};
+
+struct PointHost {
+    bafqmc_point p;
+    int N, Lq, Nst;
+    double dtau;
+    zmat expP, expM, phaseK;
+    std::vector<int> bonds;
+    double alpha_re[2], alpha_im[2];
+    int active[2];
+};
+
+double ranf(int32_t& seed) {   // src/common/random.f90:1-11
+    const long long v = (48828125LL * (long long)seed) % 2147483648LL;
+    seed = (int32_t)(v < 0 ? v + 2147483648LL : v);
+    return (double)seed / 2147483648.0;
+}
+double rng_gaussian(int32_t& seed) {   // fields.f90:280-288
+    const double x1 = ranf(seed);
+    const double x2 = ranf(seed);
+    return std::sqrt(-2.0 * std::log(x1)) * std::cos(2.0 * kPI * x2);
+}
+
+}  // namespace
+
+struct bafqmc_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int npts = 0, nchains = 0, obs_stride = 0;
+    std::vector<PointHost> pts;
+    std::vector<int> chain_point;
+    std::vector<long long> arena_off, phi_off;
+    long long arena_total = 0, phi_total = 0;
+    std::vector<int> cls_list[bq::kNumClasses];
+    int* d_cls[bq::kNumClasses] = {nullptr, nullptr};
+    int* d_pstart = nullptr;
+    int* d_plist = nullptr;
+    double* d_pout = nullptr;
+    double* d_tmp = nullptr;
+    PointDev* d_pts = nullptr;
+    ChainDev* d_chains = nullptr;
+    double2* d_mats = nullptr;
+    int* d_bonds = nullptr;
+    double2* d_arena = nullptr;
+    double* d_phi = nullptr;
+    double* d_obs = nullptr;
+    ChainScalars* d_sc = nullptr;
+    bool have_fields = false, pre_done = false, bin_done = false;
+
+    bq::KernelArgs args() const {
+        bq::KernelArgs ka;
+        ka.pts = d_pts;
+        ka.chains = d_chains;
+        ka.nchains = nchains;
+        ka.obs_stride = obs_stride;
+        ka.arena = d_arena;
+        ka.phi = d_phi;
+        ka.obs = d_obs;
+        ka.sc = d_sc;
+        return ka;
+    }
+};
+
+namespace {
+
+int setup_point(const bafqmc_point& p, PointHost& out) {
+    if (p.sector != 0) return fail(BAFQMC_EUNSUPPORTED, "only the number-conserving sector (0) is built");
+    if (p.Lx < 1 || p.Ly < 1 || p.Ltrot < 1 || p.Nwrap < 1) return fail(BAFQMC_EARG, "non-positive lattice size");
+    if (p.Ltrot % p.Nwrap != 0) return fail(BAFQMC_EARG, "Ltrot is not a multiple of Nwrap");
+    if (p.U1 < -bq::kZero) return fail(BAFQMC_EARG, "U1 must be non-negative (relative-density channel)");
+    if (p.U2 > bq::kZero) return fail(BAFQMC_EARG, "U2 must be non-positive (total-density channel)");
+    if (p.LxTherm < 1 || p.LyTherm < 1 || p.LtrotTherm < 1 || p.LxTherm > p.Lx || p.LyTherm > p.Ly ||
+        p.LtrotTherm > p.Ltrot)
+        return fail(BAFQMC_EARG, "therm field size must not exceed the lattice");
+    if (p.iniType < 1 || p.iniType > 3) return fail(BAFQMC_EARG, "incorrect initype input");
+    out.p = p;
+    out.Lq = p.Lx * p.Ly;
+    out.N = out.Lq;
+    out.Nst = p.Ltrot / p.Nwrap;
+    out.dtau = p.beta / (double)p.Ltrot;
+    if (out.N > bq::class_nmax(bq::kNumClasses - 1))
+        return fail(BAFQMC_EUNSUPPORTED, "Ndim above the largest shared-memory class of this build");
+    HostLattice lat(p.Lx, p.Ly);
+    const int n = out.N;
+    zmat H(n);   // def_hamT (non_interact.f90:33-72), t = 1
+    for (int ii = 0; ii < n; ++ii)
+        for (int nb = 0; nb < 3; ++nb) {
+            const int jj = lat.bonds[3 * ii + nb];
+            H.re(ii, jj) += 1.0;
+            H.re(jj, ii) += 1.0;
+        }
+    for (int ii = 0; ii < n; ++ii) H.re(ii, ii) -= p.mu;
+    out.expP = expm_scaled(H, -out.dtau);
+    out.expM = expm_scaled(H, out.dtau);
+    out.phaseK = zmat(n);
+    if (lat.hasK) {
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                const double kr = lat.k_dot_r(lat.indexK, lat.imj[(size_t)i * n + j]);
+                out.phaseK.re(i, j) = std::cos(kr);
+                out.phaseK.im(i, j) = std::sin(kr);
+            }
+    }
+    out.bonds = lat.bonds;
+    const double U[2] = {p.U1, p.U2};
+    for (int ch = 0; ch < 2; ++ch) {   // opU_set (operator_Hubbard.f90:36-43)
+        out.alpha_re[ch] = 0.0;
+        out.alpha_im[ch] = 0.0;
+        if (U[ch] < -bq::kZero) out.alpha_re[ch] = std::sqrt(-2.0 * U[ch] * out.dtau);
+        if (U[ch] > bq::kZero) out.alpha_im[ch] = std::sqrt(2.0 * U[ch] * out.dtau);
+        out.active[ch] = std::fabs(U[ch]) > bq::kZero ? 1 : 0;
+    }
+    return BAFQMC_OK;
+}
+
+int class_of(int n) {
+    for (int c = 0; c < bq::kNumClasses; ++c)
+        if (n <= bq::class_nmax(c)) return c;
+    return -1;
+}
+
+void free_handle(bafqmc_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_bonds, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_cls[0], h->d_cls[1]};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bafqmc_last_error(void) { return g_err.c_str(); }
+
+int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
+                  bafqmc_handle** out) {
+    if (!out || !pts || npts < 1 || nchains < 1 || !chain_point) return fail(BAFQMC_EARG, "bad create arguments");
+    *out = nullptr;
+    bafqmc_handle* h = new bafqmc_handle();
+    h->device = device;
+    h->npts = npts;
+    h->nchains = nchains;
+    h->pts.resize(npts);
+    int maxlq = 0;
+    for (int i = 0; i < npts; ++i) {
+        int rc = setup_point(pts[i], h->pts[i]);
+        if (rc != BAFQMC_OK) {
+            delete h;
+            return rc;
+        }
+        maxlq = std::max(maxlq, h->pts[i].Lq);
+    }
+    h->obs_stride = bq::kObsScalars + maxlq;
+    h->chain_point.assign(chain_point, chain_point + nchains);
+    h->arena_off.resize(nchains);
+    h->phi_off.resize(nchains);
+    std::vector<std::vector<int>> per_point(npts);
+    for (int c = 0; c < nchains; ++c) {
+        const int p = chain_point[c];
+        if (p < 0 || p >= npts) {
+            delete h;
+            return fail(BAFQMC_EARG, "chain_point out of range");
+        }
+        const PointHost& ph = h->pts[p];
+        h->arena_off[c] = h->arena_total;
+        h->arena_total += bq::arena_size(ph.N, ph.Nst);
+        h->phi_off[c] = h->phi_total;
+        h->phi_total += (long long)ph.p.Ltrot * ph.N * 2;
+        h->cls_list[class_of(ph.N)].push_back(c);
+        per_point[p].push_back(c);
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete h;
+        return cuda_fail(e, "cudaSetDevice");
+    }
+    auto bail = [&](cudaError_t err, const char* where) {
+        int rc = cuda_fail(err, where);
+        free_handle(h);
+        return rc;
+    };
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate");
+    // a^k mod 2^31 table for the in-kernel skip-ahead of the LCG
+    std::vector<uint32_t> apow(bq::kMaxPow);
+    unsigned long long v = 1;
+    for (int k = 0; k < bq::kMaxPow; ++k) {
+        apow[k] = (uint32_t)v;
+        v = (v * 48828125ull) & 0x7fffffffull;
+    }
+    if ((e = bq::upload_pow_table(apow.data(), bq::kMaxPow)) != cudaSuccess) return bail(e, "upload_pow_table");
+    // point matrices: expP, expM, phaseK per point
+    size_t mat_total = 0;
+    std::vector<size_t> mat_off(npts), bond_off(npts);
+    size_t bond_total = 0;
+    for (int i = 0; i < npts; ++i) {
+        mat_off[i] = mat_total;
+        mat_total += 3 * (size_t)h->pts[i].N * h->pts[i].N;
+        bond_off[i] = bond_total;
+        bond_total += 3 * (size_t)h->pts[i].N;
+    }
+    std::vector<double> mats(2 * mat_total);
+    std::vector<int> bonds(bond_total);
+    for (int i = 0; i < npts; ++i) {
+        const PointHost& ph = h->pts[i];
+        const size_t nn = (size_t)ph.N * ph.N;
+        std::memcpy(&mats[2 * mat_off[i]], ph.expP.a.data(), sizeof(double) * 2 * nn);
+        std::memcpy(&mats[2 * (mat_off[i] + nn)], ph.expM.a.data(), sizeof(double) * 2 * nn);
+        std::memcpy(&mats[2 * (mat_off[i] + 2 * nn)], ph.phaseK.a.data(), sizeof(double) * 2 * nn);
+        std::memcpy(&bonds[bond_off[i]], ph.bonds.data(), sizeof(int) * 3 * ph.N);
+    }
+    if ((e = cudaMalloc(&h->d_mats, sizeof(double2) * mat_total)) != cudaSuccess) return bail(e, "cudaMalloc mats");
+    if ((e = cudaMalloc(&h->d_bonds, sizeof(int) * bond_total)) != cudaSuccess) return bail(e, "cudaMalloc bonds");
+    if ((e = cudaMemcpy(h->d_mats, mats.data(), sizeof(double2) * mat_total, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload mats");
+    if ((e = cudaMemcpy(h->d_bonds, bonds.data(), sizeof(int) * bond_total, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload bonds");
+    std::vector<PointDev> pd(npts);
+    for (int i = 0; i < npts; ++i) {
+        const PointHost& ph = h->pts[i];
+        PointDev& d = pd[i];
+        const size_t nn = (size_t)ph.N * ph.N;
+        d.N = ph.N;
+        d.L = ph.p.Ltrot;
+        d.Nwrap = ph.p.Nwrap;
+        d.Nst = ph.Nst;
+        d.Lq = ph.Lq;
+        d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
+        for (int ch = 0; ch < 2; ++ch) {
+            d.active[ch] = ph.active[ch];
+            d.alpha_re[ch] = ph.alpha_re[ch];
+            d.alpha_im[ch] = ph.alpha_im[ch];
+        }
+        d.shiftLoc = ph.p.shiftLoc;
+        d.U1 = ph.p.U1;
+        d.U2 = ph.p.U2;
+        d.RT = 1.0;
+        d.expP = h->d_mats + mat_off[i];
+        d.expM = h->d_mats + mat_off[i] + nn;
+        d.phaseK = h->d_mats + mat_off[i] + 2 * nn;
+        d.bonds = h->d_bonds + bond_off[i];
+    }
+    std::vector<ChainDev> cd(nchains);
+    for (int c = 0; c < nchains; ++c) {
+        cd[c].point = chain_point[c];
+        cd[c].pad = 0;
+        cd[c].arena_off = h->arena_off[c];
+        cd[c].phi_off = h->phi_off[c];
+    }
+    std::vector<int> pstart(npts + 1, 0), plist;
+    for (int p = 0; p < npts; ++p) {
+        pstart[p + 1] = pstart[p] + (int)per_point[p].size();
+        plist.insert(plist.end(), per_point[p].begin(), per_point[p].end());
+    }
+    if ((e = cudaMalloc(&h->d_pts, sizeof(PointDev) * npts)) != cudaSuccess) return bail(e, "cudaMalloc pts");
+    if ((e = cudaMalloc(&h->d_chains, sizeof(ChainDev) * nchains)) != cudaSuccess) return bail(e, "cudaMalloc chains");
+    if ((e = cudaMalloc(&h->d_arena, sizeof(double2) * h->arena_total)) != cudaSuccess) return bail(e, "cudaMalloc arena");
+    if ((e = cudaMalloc(&h->d_phi, sizeof(double) * h->phi_total)) != cudaSuccess) return bail(e, "cudaMalloc phi");
+    if ((e = cudaMalloc(&h->d_obs, sizeof(double) * (size_t)nchains * h->obs_stride)) != cudaSuccess)
+        return bail(e, "cudaMalloc obs");
+    if ((e = cudaMalloc(&h->d_sc, sizeof(ChainScalars) * nchains)) != cudaSuccess) return bail(e, "cudaMalloc sc");
+    if ((e = cudaMalloc(&h->d_pstart, sizeof(int) * (npts + 1))) != cudaSuccess) return bail(e, "cudaMalloc pstart");
+    if ((e = cudaMalloc(&h->d_plist, sizeof(int) * nchains)) != cudaSuccess) return bail(e, "cudaMalloc plist");
+    if ((e = cudaMalloc(&h->d_pout, sizeof(double) * (size_t)npts * h->obs_stride)) != cudaSuccess)
+        return bail(e, "cudaMalloc pout");
+    if ((e = cudaMalloc(&h->d_tmp, sizeof(double) * nchains)) != cudaSuccess) return bail(e, "cudaMalloc tmp");
+    for (int c = 0; c < bq::kNumClasses; ++c) {
+        if (h->cls_list[c].empty()) continue;
+        if ((e = cudaMalloc(&h->d_cls[c], sizeof(int) * h->cls_list[c].size())) != cudaSuccess)
+            return bail(e, "cudaMalloc cls");
+        if ((e = cudaMemcpy(h->d_cls[c], h->cls_list[c].data(), sizeof(int) * h->cls_list[c].size(),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(e, "upload cls");
+    }
+    if ((e = cudaMemcpy(h->d_pts, pd.data(), sizeof(PointDev) * npts, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload pts");
+    if ((e = cudaMemcpy(h->d_chains, cd.data(), sizeof(ChainDev) * nchains, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload chains");
+    if ((e = cudaMemcpy(h->d_pstart, pstart.data(), sizeof(int) * (npts + 1), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload pstart");
+    if ((e = cudaMemcpy(h->d_plist, plist.data(), sizeof(int) * nchains, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "upload plist");
+    if ((e = cudaMemset(h->d_arena, 0, sizeof(double2) * h->arena_total)) != cudaSuccess) return bail(e, "memset arena");
+    if ((e = cudaMemset(h->d_obs, 0, sizeof(double) * (size_t)nchains * h->obs_stride)) != cudaSuccess)
+        return bail(e, "memset obs");
+    if ((e = cudaMemset(h->d_sc, 0, sizeof(ChainScalars) * nchains)) != cudaSuccess) return bail(e, "memset sc");
+    if ((e = cudaMemset(h->d_phi, 0, sizeof(double) * h->phi_total)) != cudaSuccess) return bail(e, "memset phi");
+    *out = h;
+    return BAFQMC_OK;
+}
+
+void bafqmc_destroy(bafqmc_handle* h) { free_handle(h); }
+
+int bafqmc_point_dim(const bafqmc_handle* h, int point, int* ndim, int* lq, int* ltrot, int* nst) {
+    if (!h || point < 0 || point >= h->npts) return fail(BAFQMC_EARG, "bad point");
+    const PointHost& p = h->pts[point];
+    if (ndim) *ndim = p.N;
+    if (lq) *lq = p.Lq;
+    if (ltrot) *ltrot = p.p.Ltrot;
+    if (nst) *nst = p.Nst;
+    return BAFQMC_OK;
+}
+int bafqmc_obs_stride(const bafqmc_handle* h) { return h ? h->obs_stride : fail(BAFQMC_EARG, "null handle"); }
+int bafqmc_num_chains(const bafqmc_handle* h) { return h ? h->nchains : fail(BAFQMC_EARG, "null handle"); }
+
+static int upload_state(bafqmc_handle* h, const int32_t* seeds, const double* phi) {
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->d_phi, phi, sizeof(double) * h->phi_total, cudaMemcpyHostToDevice, h->stream));
+    std::vector<ChainScalars> sc(h->nchains);
+    std::memset(sc.data(), 0, sizeof(ChainScalars) * h->nchains);
+    for (int c = 0; c < h->nchains; ++c) sc[c].seed = (uint32_t)seeds[c];
+    CK(cudaMemcpyAsync(h->d_sc, sc.data(), sizeof(ChainScalars) * h->nchains, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_fields = true;
+    h->pre_done = false;
+    h->bin_done = false;
+    return BAFQMC_OK;
+}
+
+int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds) {
+    if (!h || !seeds) return fail(BAFQMC_EARG, "null argument");
+    std::vector<double> phi(h->phi_total);
+    std::vector<int32_t> adv(h->nchains);
+    for (int c = 0; c < h->nchains; ++c) {
+        const PointHost& ph = h->pts[h->chain_point[c]];
+        const bafqmc_point& p = ph.p;
+        int32_t s = seeds[c];
+        const int ndT = p.LxTherm * p.LyTherm;
+        std::vector<double> therm((size_t)p.LtrotTherm * ndT * 2);
+        const double bias[2] = {p.iniBias1, p.iniBias2};
+        for (int nt = 0; nt < p.LtrotTherm; ++nt)   // conf_set (fields.f90:115-154)
+            for (int ii = 0; ii < ndT; ++ii)
+                for (int ns = 0; ns < 2; ++ns) {
+                    double x;
+                    if (p.iniType == 1) {
+                        x = ranf(s);
+                        x = bias[ns] + p.iniAmpl * (x - 0.5);
+                    } else if (p.iniType == 2) {
+                        x = bias[ns] + p.iniAmpl * rng_gaussian(s);
+                    } else {
+                        x = bias[ns] + p.iniAmpl * std::fabs(rng_gaussian(s));
+                    }
+                    therm[((size_t)nt * ndT + ii) * 2 + ns] = x;
+                }
+        adv[c] = s;
+        double* out = phi.data() + h->phi_off[c];   // conf_transfer (fields.f90:156-234)
+        const int n = ph.N;
+        for (int nt = 0; nt < p.LtrotTherm; ++nt)
+            for (int ny = 1; ny <= p.Ly; ++ny)
+                for (int nx = 1; nx <= p.Lx; ++nx) {
+                    const int tx = nx > p.LxTherm ? nx - p.LxTherm : nx;
+                    const int ty = ny > p.LyTherm ? ny - p.LyTherm : ny;
+                    const int iit = (ty - 1) * p.LxTherm + (tx - 1);
+                    const int ii = (ny - 1) * p.Lx + (nx - 1);
+                    for (int ns = 0; ns < 2; ++ns)
+                        out[((size_t)nt * n + ii) * 2 + ns] = therm[((size_t)nt * ndT + iit) * 2 + ns];
+                }
+        for (int nt = p.LtrotTherm; nt < p.Ltrot; ++nt)
+            for (int k = 0; k < 2 * n; ++k) out[(size_t)nt * n * 2 + k] = out[(size_t)(nt - p.LtrotTherm) * n * 2 + k];
+    }
+    return upload_state(h, adv.data(), phi.data());
+}
+
+int bafqmc_set_state(bafqmc_handle* h, const int32_t* seeds, const double* phi) {
+    if (!h || !seeds || !phi) return fail(BAFQMC_EARG, "null argument");
+    return upload_state(h, seeds, phi);
+}
+
+int bafqmc_get_state(bafqmc_handle* h, int32_t* seeds, double* phi) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    CK(cudaSetDevice(h->device));
+    if (phi) CK(cudaMemcpyAsync(phi, h->d_phi, sizeof(double) * h->phi_total, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<ChainScalars> sc(h->nchains);
+    CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (seeds)
+        for (int c = 0; c < h->nchains; ++c) seeds[c] = (int32_t)sc[c].seed;
+    return BAFQMC_OK;
+}
+
+int bafqmc_warmup_prior(bafqmc_handle* h, int nwarm) {
+    if (!h || nwarm < 0) return fail(BAFQMC_EARG, "bad warm-up arguments");
+    if (!h->have_fields) return fail(BAFQMC_ESTATE, "fields not initialised");
+    if (nwarm == 0) return BAFQMC_OK;
+    CK(cudaSetDevice(h->device));
+    CK(bq::launch_warmup(h->args(), nwarm, h->stream));
+    h->pre_done = false;
+    return BAFQMC_OK;
+}
+
+int bafqmc_pre(bafqmc_handle* h) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    if (!h->have_fields) return fail(BAFQMC_ESTATE, "fields not initialised");
+    CK(cudaSetDevice(h->device));
+    for (int c = 0; c < bq::kNumClasses; ++c)
+        CK(bq::launch_pre(c, h->args(), h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
+    h->pre_done = true;
+    return BAFQMC_OK;
+}
+
+int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
+    if (!h || nsweep < 1) return fail(BAFQMC_EARG, "bad sweep arguments");
+    if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
+    CK(cudaSetDevice(h->device));
+    const bq::KernelArgs ka = h->args();
+    CK(bq::launch_bin_reset(ka, h->stream));
+    for (int s = 0; s < nsweep; ++s)
+        for (int c = 0; c < bq::kNumClasses; ++c)
+            CK(bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
+    CK(bq::launch_bin_finish(ka, h->stream));
+    h->bin_done = true;
+    return BAFQMC_OK;
+}
+
+int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs) {
+    if (!h || !chain_obs) return fail(BAFQMC_EARG, "null argument");
+    if (!h->bin_done) return fail(BAFQMC_ESTATE, "no bin has been measured");
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(chain_obs, h->d_obs, sizeof(double) * (size_t)h->nchains * h->obs_stride,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BAFQMC_OK;
+}
+
+int bafqmc_bin_point_obs(bafqmc_handle* h, double* point_obs) {
+    if (!h || !point_obs) return fail(BAFQMC_EARG, "null argument");
+    if (!h->bin_done) return fail(BAFQMC_ESTATE, "no bin has been measured");
+    CK(cudaSetDevice(h->device));
+    CK(bq::launch_point_average(h->args(), h->npts, h->d_pstart, h->d_plist, h->d_pout, h->stream));
+    CK(cudaMemcpyAsync(point_obs, h->d_pout, sizeof(double) * (size_t)h->npts * h->obs_stride,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BAFQMC_OK;
+}
+
+int bafqmc_get_green(bafqmc_handle* h, int chain, double* G) {
+    if (!h || !G || chain < 0 || chain >= h->nchains) return fail(BAFQMC_EARG, "bad chain");
+    CK(cudaSetDevice(h->device));
+    const int n = h->pts[h->chain_point[chain]].N;
+    CK(cudaMemcpyAsync(G, h->d_arena + h->arena_off[chain], sizeof(double2) * n * n, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BAFQMC_OK;
+}
+
+int bafqmc_log_weight(bafqmc_handle* h, double* out) {
+    if (!h || !out) return fail(BAFQMC_EARG, "null argument");
+    CK(cudaSetDevice(h->device));
+    CK(bq::launch_field_norm(h->args(), h->d_tmp, h->stream));
+    std::vector<double> fn(h->nchains);
+    std::vector<ChainScalars> sc(h->nchains);
+    CK(cudaMemcpyAsync(fn.data(), h->d_tmp, sizeof(double) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < h->nchains; ++c) out[c] = fn[c] - 2.0 * sc[c].logdetM;
+    return BAFQMC_OK;
+}
+
+int bafqmc_counters(bafqmc_handle* h, double* out) {
+    if (!h || !out) return fail(BAFQMC_EARG, "null argument");
+    CK(cudaSetDevice(h->device));
+    std::vector<ChainScalars> sc(h->nchains);
+    CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < h->nchains; ++c) {
+        double* o = out + (size_t)c * BAFQMC_COUNTERS;
+        o[0] = sc[c].acc_sum[0];
+        o[1] = sc[c].acc_sum[1];
+        o[2] = sc[c].therm_acc_sum[0];
+        o[3] = sc[c].therm_acc_sum[1];
+        o[4] = sc[c].xmax;
+        o[5] = sc[c].xmean;
+        o[6] = (double)sc[c].status;
+        o[7] = (double)sc[c].seed;
+        o[8] = (double)sc[c].nobs;
+        o[9] = 0.0;
+    }
+    return BAFQMC_OK;
+}
+
+int bafqmc_synchronize(bafqmc_handle* h) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    return BAFQMC_OK;
+}
+
+void* bafqmc_stream(bafqmc_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Device-side data layout and per-chain sweep routines for the BAFQMC
+// number-conserving solver (src/number_conserving/src/*.f90).
+//
+// One CTA owns one Markov chain for a whole sweep.  Shared memory holds four
+// N x N complex matrices: G, the current U factor of the propagated side, and
+// two workspaces that hold e^{-dtau K} / e^{+dtau K} while slices are
+// propagated and serve the QR stabilisation at wrap slices.  The stored UDV
+// slots, the V/D factors and the fields stay in HBM.
+#pragma once
+#include "linalg.cuh"
+
+namespace bq {
+
+constexpr double kZero = 1.0e-10;          // calc_basic.f90:5
+constexpr uint32_t kLcgA = 48828125u;       // random.f90:9
+constexpr int kMaxPow = 2 * 160 + 2;        // a^k mod 2^31 table for k <= 2*NMAX_ALL + 1
+
+// Observable accumulator layout per chain (obser_equal.f90:6-18 and the bin
+// writer fourier_trans.f90:250-348).  Complex values take two slots.
+enum ObsIndex {
+    O_DENSITY_UP = 0, O_DENSITY_DO, O_DENSITY_TOTAL, O_KINETIC, O_DOUBLEOCC, O_SQUAREOCC,
+    O_NUM_UP, O_NUM_DO, O_NUMSQUARE_UP, O_NUMSQUARE_DO, O_ONSITE_N2_UP, O_ONSITE_N2_DO,
+    O_INTERACTION, O_ENERGY,
+    O_SF_K = 14,        // re, im
+    O_PSF_GAMMA = 16,   // re, im
+    O_DW_K = 18,        // re, im
+    O_DEN_UPUP = 20,    // re, im  (sum over r of den_corr_up(r)/Lq == FFT at k=0)
+    O_DEN_DODO = 22,    // re, im
+    O_DEN_UPDO = 24,    // re, im
+    O_SITE = 26,        // Lq values of density_site_total
+};
+constexpr int kObsScalars = 26;
+
+struct PointDev {
+    int N, L, Nwrap, Nst, Lq, hasK;
+    int active[2];
+    double alpha_re[2], alpha_im[2];
+    double shiftLoc, U1, U2, RT;
+    const cplx* expP;      // e^{-dtau K}, N*N row-major
+    const cplx* expM;      // e^{+dtau K}
+    const cplx* phaseK;    // exp(i K.r_{imj(i,j)}), N*N (only if hasK)
+    const int* bonds;      // N*3: neighbour of site i along bond 1..3 (lattice.f90:98-111)
+};
+
+struct ChainScalars {
+    uint32_t seed;
+    int status;
+    long long nc[2], nacc[2];   // current bin, per channel (AccCounter)
+    long long nobs;             // measurements in the current bin
+    double acc_sum[2];          // sum over bins of nacc/nc (AccCounter%acc)
+    double therm_acc_sum[2];    // sum over warm-up sweeps of nacc/nc
+    double xmax, xmean;         // stabilisation drift (Prop%Xmaxm, Prop%Xmeanm)
+    double logdetM;             // sum log D of the last (I-B) factorisation at tau = beta
+    double pad;
+};
+
+struct ChainDev {
+    int point;
+    int pad;
+    long long arena_off;   // in cplx units
+    long long phi_off;     // in doubles
+};
+
+// Per-chain arena layout (cplx units).
+struct Arena {
+    cplx *G, *URc, *VRc, *ULc, *VLc, *DRc, *DLc, *slots;
+    int N;
+    DEVI cplx* URs(int s) const { return slots + (long)s * (4 * N * N + 2 * N); }
+    DEVI cplx* VRs(int s) const { return URs(s) + N * N; }
+    DEVI cplx* ULs(int s) const { return URs(s) + 2 * N * N; }
+    DEVI cplx* VLs(int s) const { return URs(s) + 3 * N * N; }
+    DEVI cplx* DRs(int s) const { return URs(s) + 4 * N * N; }
+    DEVI cplx* DLs(int s) const { return URs(s) + 4 * N * N + N; }
+};
+
+__host__ __device__ inline long long arena_size(int N, int Nst) {
+    return 5LL * N * N + 2LL * N + (long long)(Nst + 1) * (4LL * N * N + 2LL * N);
+}
+
+DEVI Arena make_arena(cplx* base, int N) {
+    Arena a;
+    a.N = N;
+    a.G = base;
+    a.URc = base + N * N;
+    a.VRc = base + 2 * N * N;
+    a.ULc = base + 3 * N * N;
+    a.VLc = base + 4 * N * N;
+    a.DRc = base + 5 * N * N;
+    a.DLc = base + 5 * N * N + N;
+    a.slots = base + 5 * N * N + 2 * N;
+    return a;
+}
+
+DEVI uint32_t lcg_mul(uint32_t apow, uint32_t s) {
+    return (uint32_t)(((unsigned long long)apow * (unsigned long long)s) & 0x7fffffffull);
+}
+DEVI double lcg_u(uint32_t s) { return (double)s * (1.0 / 2147483648.0); }
+
+// a^k mod 2^31 by square-and-multiply (any k >= 0).
+DEVI uint32_t lcg_pow(unsigned long long k) {
+    unsigned long long r = 1, b = kLcgA;
+    while (k) {
+        if (k & 1ull) r = (r * b) & 0x7fffffffull;
+        b = (b * b) & 0x7fffffffull;
+        k >>= 1;
+    }
+    return (uint32_t)r;
+}
+
+}  // namespace bq

@@ -1,0 +1,830 @@
+// Sweep kernels for the BAFQMC number-conserving solver on sm_100a.
+//
+// One CTA = one Markov chain.  sweep_kernel runs one full sweep (left then
+// right traversal of imaginary time, local_sweep.f90:96-134 with is_beta
+// = .true.) including every local update, slice propagation, stabilisation
+// and equal-time measurement of that chain.  pre_kernel builds the right UDV
+// slots and G(beta) (local_sweep.f90:80-94); warmup_kernel is the prior-only
+// warm-up (local_sweep.f90:64-78).
+#include "sweep.cuh"
+#include "kernels.h"
+
+namespace bq {
+
+__constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
+
+template <int NMAX> struct Cfg;
+template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3; };
+
+template <int NMAX>
+struct Smem {
+    cplx *G, *U, *W1, *W2;
+    cplx *tau, *col[2], *row[2], *delta, *eao, *ean, *ebo, *ebn, *coef, *cbc;
+    double *rg, *u2, *phin, *vn1, *vn2, *d, *red, *obs;
+    int *piv, *ipiv, *accf, *ibc;
+    uint32_t* seed;
+
+    static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
+    static constexpr size_t bytes() {
+        return sizeof(cplx) * (4 * NMAX * NMAX + 11 * NMAX + 2 + 4) +
+               sizeof(double) * (6 * NMAX + kRed + kObsScalars + NMAX) +
+               sizeof(int) * (3 * NMAX + 4) + 16;
+    }
+    DEVI void carve(unsigned char* base) {
+        cplx* c = reinterpret_cast<cplx*>(base);
+        G = c; c += NMAX * NMAX;
+        U = c; c += NMAX * NMAX;
+        W1 = c; c += NMAX * NMAX;
+        W2 = c; c += NMAX * NMAX;
+        tau = c; c += NMAX;
+        col[0] = c; c += NMAX;
+        col[1] = c; c += NMAX;
+        row[0] = c; c += NMAX;
+        row[1] = c; c += NMAX;
+        delta = c; c += NMAX;
+        eao = c; c += NMAX;
+        ean = c; c += NMAX;
+        ebo = c; c += NMAX;
+        ebn = c; c += NMAX;
+        c += NMAX;  // spare
+        coef = c; c += 2;
+        cbc = c; c += 4;
+        double* dd = reinterpret_cast<double*>(c);
+        rg = dd; dd += NMAX;
+        u2 = dd; dd += NMAX;
+        phin = dd; dd += NMAX;
+        vn1 = dd; dd += NMAX;
+        vn2 = dd; dd += NMAX;
+        d = dd; dd += NMAX;
+        red = dd; dd += kRed;
+        obs = dd; dd += kObsScalars + NMAX;
+        int* ii = reinterpret_cast<int*>(dd);
+        piv = ii; ii += NMAX;
+        ipiv = ii; ii += NMAX;
+        accf = ii; ii += NMAX;
+        ibc = ii; ii += 4;
+        seed = reinterpret_cast<uint32_t*>(ii);
+    }
+    DEVI QRScratch qr() const { return QRScratch{tau, piv, ipiv, vn1, vn2, d, const_cast<cplx*>(cbc), ibc}; }
+};
+
+template <int NMAX>
+struct Ctx {
+    Smem<NMAX> s;
+    PointDev P;
+    Arena A;
+    double* phi;
+    ChainScalars* sc;
+    int n;
+};
+
+// ---------------------------------------------------------------------------
+// small CTA helpers
+DEVI void gcopy(cplx* dst, const cplx* src, int count) {
+    for (int e = threadIdx.x; e < count; e += blockDim.x) dst[e] = src[e];
+}
+DEVI void set_identity(int n, cplx* A) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) A[e] = cmk((e / n) == (e % n) ? 1.0 : 0.0, 0.0);
+}
+
+template <int NMAX>
+DEVI void load_expT(Ctx<NMAX>& x) {
+    const int nn = x.n * x.n;
+    gcopy(x.s.W1, x.P.expP, nn);
+    gcopy(x.s.W2, x.P.expM, nn);
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// local update of one channel over all sites of one slice, fused with the
+// V-wrap of G (LocalU_prop_L / LocalU_prop_R, localU.f90:79-113, and
+// LocalU_metro, localU.f90:31-77).  Sites are strictly sequential; each site
+// costs one barrier: the owner of the next diagonal element makes the next
+// Metropolis decision right after its own update, and the owners of the next
+// row/column stage them, so the rank-1 update of site i and the staging for
+// site i+1 share one pass.  G lives in registers for the whole loop.
+template <int NMAX, bool LEFT>
+DEVI void prop_channel(Ctx<NMAX>& x, int ch, int slice) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n, tid = threadIdx.x;
+    const double ar = x.P.alpha_re[ch], ai = x.P.alpha_im[ch];
+    const double shift = fabs(x.P.shiftLoc);
+    const uint32_t s0 = *s.seed;
+    double* phis = x.phi + (long)slice * n * 2;
+
+    // per-site proposals; draw order follows the visiting order of the sites
+    for (int i = tid; i < n; i += blockDim.x) {
+        const int m = LEFT ? (n - 1 - i) : i;
+        const double xflip = lcg_u(lcg_mul(c_apow[2 * m + 1], s0));
+        const double rnd = lcg_u(lcg_mul(c_apow[2 * m + 2], s0));
+        const double po = phis[i * 2 + ch];
+        const double xdif = (xflip - 0.5) * shift;
+        const double pn = po + xdif;
+        const double go = exp(-0.5 * po * po), gn = exp(-0.5 * pn * pn);
+        const cplx eo = cexpz(cmk(ar * po, ai * po)), en = cexpz(cmk(ar * pn, ai * pn));
+        s.eao[i] = eo;
+        s.ean[i] = en;
+        s.ebo[i] = cexpz(cmk(-(ar * po), -(ai * po)));
+        s.ebn[i] = cexpz(cmk(-(ar * pn), -(ai * pn)));
+        s.delta[i] = csub(cdiv(en, eo), cmk(1.0, 0.0));
+        s.rg[i] = gn / go;
+        s.u2[i] = rnd;
+        s.phin[i] = pn;
+        s.accf[i] = 0;
+    }
+    __syncthreads();
+
+    const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
+    const bool act = tid < ncg * nrg;
+    const int r0 = act ? (tid / ncg) * TR : 0, c0 = act ? (tid % ncg) * TC : 0;
+    cplx g[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+            const int r = r0 + a, c = c0 + b;
+            g[a][b] = (act && r < n && c < n) ? s.G[r * n + c] : cmk(0.0, 0.0);
+        }
+
+    auto decide = [&](int j, cplx gjj, int par) {
+        // ratio_det = 1/(1 + Delta (1 - G_jj)); p = |r_gauss * ratio_det * conj(ratio_det)|
+        const cplx w = cadd(cmk(1.0, 0.0), cmul(s.delta[j], csub(cmk(1.0, 0.0), gjj)));
+        const cplx rdet = cdiv(cmk(1.0, 0.0), w);
+        const cplx prod = cmul(cmul(cmk(s.rg[j], 0.0), rdet), cconj(rdet));
+        const double ratio_abs = hypot(prod.x, prod.y);
+        const bool accept = ratio_abs > s.u2[j];
+        const cplx ta = cmul(rdet, s.delta[j]);
+        s.coef[par] = accept ? cmk(-ta.x, -ta.y) : cmk(0.0, 0.0);
+        s.accf[j] = accept ? 1 : 0;
+    };
+    // stage row/column of the next site j (and decide on it) from the current registers
+    auto stage = [&](int j, int par) {
+        if (!act) return;
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+            for (int b = 0; b < TC; ++b) {
+                const int r = r0 + a, c = c0 + b;
+                if (r >= n || c >= n) continue;
+                if (r != j && c != j) continue;
+                cplx v = g[a][b];
+                if (!LEFT) {   // right sweep wraps site j with its current field before the update
+                    if (r == j) v = cmul(v, s.eao[j]);
+                    if (c == j) v = cmul(v, s.ebo[j]);
+                }
+                if (c == j) s.col[par][r] = v;
+                if (r == j) s.row[par][c] = v;
+                if (r == j && c == j) decide(j, v, par);
+            }
+    };
+
+    stage(LEFT ? n - 1 : 0, 0);
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const int i = LEFT ? n - 1 - k : k;
+        const int par = k & 1;
+        if (act) {
+            const cplx coef = s.coef[par];
+            const int acc = s.accf[i];
+            cplx cr[TR];
+#pragma unroll
+            for (int a = 0; a < TR; ++a) {
+                const int r = r0 + a;
+                cr[a] = (r < n) ? cmul(coef, s.col[par][r]) : cmk(0.0, 0.0);
+            }
+#pragma unroll
+            for (int b = 0; b < TC; ++b) {
+                const int c = c0 + b;
+                if (c >= n) continue;
+                const cplx rv = s.row[par][c];
+                const cplx y = (c == i) ? cmk(1.0 - rv.x, -rv.y) : cmk(-rv.x, -rv.y);
+#pragma unroll
+                for (int a = 0; a < TR; ++a) {
+                    const int r = r0 + a;
+                    if (r >= n) continue;
+                    cplx v = g[a][b];
+                    if (!LEFT) {
+                        if (r == i) v = cmul(v, s.eao[i]);
+                        if (c == i) v = cmul(v, s.ebo[i]);
+                    }
+                    v = cfma(cr[a], y, v);
+                    if (LEFT) {
+                        if (c == i) v = cmul(v, acc ? s.ean[i] : s.eao[i]);
+                        if (r == i) v = cmul(v, acc ? s.ebn[i] : s.ebo[i]);
+                    }
+                    g[a][b] = v;
+                }
+            }
+        }
+        if (k + 1 < n) stage(LEFT ? n - 2 - k : k + 1, par ^ 1);
+        __syncthreads();
+    }
+    if (act) {
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+            for (int b = 0; b < TC; ++b) {
+                const int r = r0 + a, c = c0 + b;
+                if (r < n && c < n) s.G[r * n + c] = g[a][b];
+            }
+    }
+    // accepted fields, counters, seed, and the U factor wrap with the final fields
+    for (int i = tid; i < n; i += blockDim.x)
+        if (s.accf[i]) phis[i * 2 + ch] = s.phin[i];
+    if (tid == 0) {
+        long long na = 0;
+        for (int i = 0; i < n; ++i) na += s.accf[i];
+        x.sc->nacc[ch] += na;
+        x.sc->nc[ch] += n;
+        *s.seed = lcg_mul(c_apow[2 * n], s0);
+    }
+    for (int e = tid; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e % n;
+        const int site = LEFT ? c : r;
+        s.U[e] = cmul(s.U[e], s.accf[site] ? s.ean[site] : s.eao[site]);
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// equal-time estimators (Obs_equal_calc, obser_equal.f90:95-198)
+template <int NMAX>
+DEVI void measure(Ctx<NMAX>& x) {
+    auto& s = x.s;
+    const int n = x.n, tid = threadIdx.x;
+    const double lq = (double)x.P.Lq, lq2 = lq * lq;
+    const cplx* G = s.G;
+    double v[24];
+#pragma unroll
+    for (int k = 0; k < 24; ++k) v[k] = 0.0;
+    for (int e = tid; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        const cplx a = G[i * n + j];                  // Grup(i,j)
+        cplx gc = G[j * n + i];                       // Grupc(i,j) = G(j,i) - delta_ij
+        if (i == j) gc.x -= 1.0;
+        const cplx dui = cmk(G[i * n + i].x - 1.0, G[i * n + i].y);
+        const cplx duj = cmk(G[j * n + j].x - 1.0, G[j * n + j].y);
+        const cplx ddi = cconj(dui), ddj = cconj(duj);
+        const cplx tup = cadd(cmul(dui, duj), cmul(gc, a));
+        const cplx tdo = cadd(cmul(ddi, ddj), cmul(cconj(gc), cconj(a)));
+        const cplx tud = cmul(dui, ddj);
+        v[0] += tup.x;
+        v[1] += tdo.x;
+        const cplx ps = cmul(gc, cconj(gc));
+        v[2] += ps.x / lq2;
+        v[3] += ps.y / lq2;
+        v[8] += tup.x / lq;
+        v[9] += tup.y / lq;
+        v[10] += tdo.x / lq;
+        v[11] += tdo.y / lq;
+        v[12] += tud.x / lq;
+        v[13] += tud.y / lq;
+        if (x.P.hasK) {
+            const cplx ph = x.P.phaseK[i * n + j];
+            const cplx sf = cmul(ph, cadd(gc, cconj(gc)));
+            const cplx dw = cmul(ph, cadd(cadd(tup, tdo), cadd(tud, cmul(ddi, duj))));
+            v[4] += sf.x / lq2;
+            v[5] += sf.y / lq2;
+            v[6] += dw.x / lq2;
+            v[7] += dw.y / lq2;
+        }
+    }
+    for (int e = tid; e < 3 * n; e += blockDim.x) {
+        const int i = e / 3, jj = x.P.bonds[e];
+        cplx gij = G[jj * n + i], gji = G[i * n + jj];   // Grupc(i,jj), Grupc(jj,i)
+        if (i == jj) { gij.x -= 1.0; gji.x -= 1.0; }
+        v[14] += x.P.RT * (gij.x + gji.x + gij.x + gji.x) / lq;
+    }
+    for (int i = tid; i < n; i += blockDim.x) {
+        const cplx du = cmk(G[i * n + i].x - 1.0, G[i * n + i].y), dd = cconj(du);
+        const cplx ud = cmul(du, dd);
+        const double dens = du.x + dd.x;
+        v[15] += du.x / lq;
+        v[16] += dd.x / lq;
+        v[17] += ud.x / lq;
+        v[18] += (cmul(du, du).x + cmul(dd, dd).x) / lq;
+        v[19] += du.x;
+        v[20] += dd.x;
+        v[21] += dens / lq;
+        v[22] += 2.0 * cmul(du, du).x + du.x;
+        v[23] += 2.0 * cmul(dd, dd).x + dd.x;
+        s.obs[O_SITE + i] += dens;
+    }
+    block_sum<24>(v, s.red);
+    if (tid == 0) {
+        double* o = s.obs;
+        o[O_NUMSQUARE_UP] += v[0];
+        o[O_NUMSQUARE_DO] += v[1];
+        o[O_PSF_GAMMA] += v[2];
+        o[O_PSF_GAMMA + 1] += v[3];
+        o[O_SF_K] += v[4];
+        o[O_SF_K + 1] += v[5];
+        o[O_DW_K] += v[6];
+        o[O_DW_K + 1] += v[7];
+        o[O_DEN_UPUP] += v[8];
+        o[O_DEN_UPUP + 1] += v[9];
+        o[O_DEN_DODO] += v[10];
+        o[O_DEN_DODO + 1] += v[11];
+        o[O_DEN_UPDO] += v[12];
+        o[O_DEN_UPDO + 1] += v[13];
+        const double kin = v[14];
+        o[O_DENSITY_UP] += v[15];
+        o[O_DENSITY_DO] += v[16];
+        o[O_DOUBLEOCC] += v[17];
+        o[O_SQUAREOCC] += v[18];
+        o[O_NUM_UP] += v[19];
+        o[O_NUM_DO] += v[20];
+        o[O_DENSITY_TOTAL] += v[21];
+        o[O_ONSITE_N2_UP] += v[22];
+        o[O_ONSITE_N2_DO] += v[23];
+        const double inter = (x.P.U1 + x.P.U2) * (v[22] + v[23]) / lq + 2.0 * (x.P.U2 - x.P.U1) * v[17];
+        o[O_KINETIC] += kin;
+        o[O_INTERACTION] += inter;
+        o[O_ENERGY] += kin + inter;
+        x.sc->nobs += 1;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// stabilisation (stabilization.f90:69-190)
+
+// stab_UR: (U_R D_R) P = Q R;  D_R <- |diag R|;  V_R <- R P^T V_R;  U_R <- Q.
+// U_R is s.U; on exit the new V_R is in s.W2 and in A.VRc, D_R in A.DRc.
+template <int NMAX>
+DEVI void stab_UR(Ctx<NMAX>& x) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W1[e] = cmul(s.U[e], x.A.DRc[e % n]);
+    __syncthreads();
+    qrp_inplace(n, s.W1, s.qr());
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A.DRc[i] = cmk(s.d[i], 0.0);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2[e] = x.A.VRc[s.piv[e / n] * n + e % n];
+    __syncthreads();
+    gemm_rs<TR, TC>(n, s.W2, op_n(s.W1, n), op_n(s.W2, n), TRI_A_UPPER);
+    form_q(n, s.W1, s.tau, s.U, false);
+    gcopy(x.A.VRc, s.W2, n * n);
+    __syncthreads();
+}
+
+// stab_UL: (U_L^H D_L) P = Q R;  D_L <- |diag R|;  V_L <- V_L P R^H;  U_L <- Q^H.
+template <int NMAX>
+DEVI void stab_UL(Ctx<NMAX>& x) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e % n;
+        s.W1[e] = cmul(cconj(s.U[c * n + r]), x.A.DLc[c]);
+    }
+    __syncthreads();
+    qrp_inplace(n, s.W1, s.qr());
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A.DLc[i] = cmk(s.d[i], 0.0);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2[e] = x.A.VLc[(e / n) * n + s.piv[e % n]];
+    __syncthreads();
+    gemm_rs<TR, TC>(n, s.W2, op_n(s.W2, n), op_c(s.W1, n), TRI_B_LOWER_FROM_C);
+    form_q(n, s.W1, s.tau, s.U, true);
+    gcopy(x.A.VLc, s.W2, n * n);
+    __syncthreads();
+}
+
+// M = U_R^H U_L^H - D_R V_R V_L D_L is in W2 (W1 free); finish stab_green:
+// factor M (or M^H for nt > L/2) and write G = (I - B)^{-1} into W2.
+template <int NMAX>
+DEVI void green_from_M(Ctx<NMAX>& x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n, L = x.P.L;
+    if (nt > L / 2) conj_transpose_inplace(n, s.W2);
+    qrp_inplace(n, s.W2, s.qr());
+    if (nt < L / 2 + 1) {
+        copy_op(n, s.W1, URh);
+        apply_qh_left(n, s.W2, s.tau, s.W1);
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const double dd = s.d[e / n];
+            s.W1[e] = cmk(s.W1[e].x / dd, s.W1[e].y / dd);
+        }
+        __syncthreads();
+        trsm_left_upper(n, s.W2, s.W1);
+        permute_rows(n, s.W1, s.piv, s.ipiv, false);
+        gemm_rs<TR, TC>(n, s.W2, ULh, op_n(s.W1, n));
+    } else {
+        copy_op(n, s.W1, ULh);
+        apply_q_right(n, s.W2, s.tau, s.W1);
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const double dd = s.d[e % n];
+            s.W1[e] = cmk(s.W1[e].x / dd, s.W1[e].y / dd);
+        }
+        __syncthreads();
+        trsm_right_upperH(n, s.W2, s.W1);
+        permute_cols(n, s.W1, s.piv, s.ipiv, false);
+        gemm_rs<TR, TC>(n, s.W2, op_n(s.W1, n), URh);
+    }
+    if (want_logdet) {
+        double v[1] = {0.0};
+        for (int i = threadIdx.x; i < n; i += blockDim.x) v[0] += log(s.d[i]);
+        block_sum<1>(v, s.red);
+        if (threadIdx.x == 0) x.sc->logdetM = v[0];
+    }
+}
+
+// M = invULUR - D_R (V_R V_L) D_L with V_R V_L already in W1 and invULUR in W2.
+template <int NMAX>
+DEVI void form_M(Ctx<NMAX>& x) {
+    auto& s = x.s;
+    const int n = x.n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e % n;
+        const cplx t = cmul(x.A.DLc[c], s.W1[e]);
+        s.W2[e] = csub(s.W2[e], cmul(x.A.DRc[r], t));
+    }
+    __syncthreads();
+}
+
+// compare_mat + G <- G_new (stabilization.f90:256-266, 339-344)
+template <int NMAX>
+DEVI void drift_and_replace(Ctx<NMAX>& x) {
+    auto& s = x.s;
+    const int n = x.n;
+    double v[1] = {0.0};
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) v[0] += cabsv(csub(s.W2[e], s.G[e]));
+    block_sum<1>(v, s.red);
+    if (threadIdx.x == 0) {
+        const double dif = v[0];
+        if (dif > x.sc->xmax) x.sc->xmax = dif;
+        x.sc->xmean += dif;
+        if (!(dif == dif) || dif > 1.0e300) x.sc->status |= 1;
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.G[e] = s.W2[e];
+    __syncthreads();
+}
+
+// stab_green with the right side factored in shared memory (U = U_R, W2 = V_R)
+// and the left side in HBM (A.ULc, A.VLc, A.DLc).
+template <int NMAX>
+DEVI void stab_green_right_local(Ctx<NMAX>& x, int nt, bool want_logdet) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n;
+    gemm_rs<TR, TC>(n, s.W1, op_n(s.W2, n), op_n(x.A.VLc, n));        // V_R V_L
+    gemm_rs<TR, TC>(n, s.W2, op_c(s.U, n), op_c(x.A.ULc, n));         // U_R^H U_L^H
+    form_M(x);
+    green_from_M(x, nt, op_c(s.U, n), op_c(x.A.ULc, n), want_logdet);
+}
+
+// stab_green with the left side in shared memory (U = U_L, W2 = V_L) and the
+// right side in HBM.
+template <int NMAX>
+DEVI void stab_green_left_local(Ctx<NMAX>& x, int nt) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n;
+    gemm_rs<TR, TC>(n, s.W1, op_n(x.A.VRc, n), op_n(s.W2, n));
+    gemm_rs<TR, TC>(n, s.W2, op_c(x.A.URc, n), op_c(s.U, n));
+    form_M(x);
+    green_from_M(x, nt, op_c(x.A.URc, n), op_c(s.U, n), false);
+}
+
+// Wrap_L (stabilization.f90:301-331)
+template <int NMAX>
+DEVI void wrap_L(Ctx<NMAX>& x, int nt) {
+    auto& s = x.s;
+    const int n = x.n, st = nt / x.P.Nwrap;
+    gcopy(x.A.URc, x.A.URs(st), n * n);
+    gcopy(x.A.VRc, x.A.VRs(st), n * n);
+    gcopy(x.A.DRc, x.A.DRs(st), n);
+    __syncthreads();
+    if (nt != x.P.L) {
+        stab_UL(x);
+        stab_green_left_local(x, nt);
+        drift_and_replace(x);
+    }
+    gcopy(x.A.ULs(st), s.U, n * n);
+    gcopy(x.A.VLs(st), x.A.VLc, n * n);
+    gcopy(x.A.DLs(st), x.A.DLc, n);
+    __syncthreads();
+    load_expT(x);
+}
+
+// Wrap_R (stabilization.f90:333-366)
+template <int NMAX>
+DEVI void wrap_R(Ctx<NMAX>& x, int nt) {
+    auto& s = x.s;
+    const int n = x.n, st = nt / x.P.Nwrap;
+    gcopy(x.A.ULc, x.A.ULs(st), n * n);
+    gcopy(x.A.VLc, x.A.VLs(st), n * n);
+    gcopy(x.A.DLc, x.A.DLs(st), n);
+    __syncthreads();
+    if (nt != 0) {
+        stab_UR(x);
+        stab_green_right_local(x, nt, nt == x.P.L);
+        drift_and_replace(x);
+    }
+    gcopy(x.A.URs(st), s.U, n * n);
+    gcopy(x.A.VRs(st), x.A.VRc, n * n);
+    gcopy(x.A.DRs(st), x.A.DRc, n);
+    __syncthreads();
+    load_expT(x);
+}
+
+// ---------------------------------------------------------------------------
+template <int NMAX>
+DEVI bool setup_ctx(Ctx<NMAX>& x, unsigned char* smem, const KernelArgs& ka, int chain) {
+    x.s.carve(smem);
+    const ChainDev cd = ka.chains[chain];
+    x.P = ka.pts[cd.point];
+    x.n = x.P.N;
+    x.A = make_arena(ka.arena + cd.arena_off, x.n);
+    x.phi = ka.phi + cd.phi_off;
+    x.sc = ka.sc + chain;
+    return x.n <= NMAX;
+}
+
+template <int NMAX>
+DEVI void load_obs(Ctx<NMAX>& x) {
+    for (int k = threadIdx.x; k < kObsScalars + NMAX; k += blockDim.x) x.s.obs[k] = 0.0;
+}
+template <int NMAX>
+DEVI void flush_obs(Ctx<NMAX>& x, double* gobs) {
+    for (int k = threadIdx.x; k < kObsScalars + x.P.Lq; k += blockDim.x) gobs[k] += x.s.obs[k];
+}
+
+// one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
+template <int NMAX>
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS) sweep_kernel(KernelArgs ka, const int* idx, int count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    if ((int)blockIdx.x >= count) return;
+    const int chain = idx[blockIdx.x];
+    Ctx<NMAX> x;
+    if (!setup_ctx(x, smem, ka, chain)) return;
+    auto& s = x.s;
+    const int n = x.n, L = x.P.L;
+    if (threadIdx.x == 0) *s.seed = x.sc->seed;
+    load_obs(x);
+    gcopy(s.G, x.A.G, n * n);
+    gcopy(s.U, x.A.ULc, n * n);
+    __syncthreads();
+    load_expT(x);
+    // ---- left traversal
+    for (int nt = L; nt >= 1; --nt) {
+        if (nt % x.P.Nwrap == 0) wrap_L(x, nt);
+        measure(x);
+        gemm_rs<TR, TC>(n, s.G, op_n(s.G, n), op_n(s.W1, n));   // G e^{-dtau K}
+        gemm_rs<TR, TC>(n, s.G, op_n(s.W2, n), op_n(s.G, n));   // e^{+dtau K} G
+        gemm_rs<TR, TC>(n, s.U, op_n(s.U, n), op_n(s.W1, n));   // U_L e^{-dtau K}
+        if (x.P.active[1]) prop_channel<NMAX, true>(x, 1, nt - 1);
+        if (x.P.active[0]) prop_channel<NMAX, true>(x, 0, nt - 1);
+    }
+    wrap_L(x, 0);
+    gcopy(x.A.ULc, s.U, n * n);
+    __syncthreads();
+    // ---- right traversal
+    gcopy(s.U, x.A.URc, n * n);
+    __syncthreads();
+    wrap_R(x, 0);
+    for (int nt = 1; nt <= L; ++nt) {
+        if (x.P.active[0]) prop_channel<NMAX, false>(x, 0, nt - 1);
+        if (x.P.active[1]) prop_channel<NMAX, false>(x, 1, nt - 1);
+        gemm_rs<TR, TC>(n, s.G, op_n(s.W1, n), op_n(s.G, n));   // e^{-dtau K} G
+        gemm_rs<TR, TC>(n, s.G, op_n(s.G, n), op_n(s.W2, n));   // G e^{+dtau K}
+        gemm_rs<TR, TC>(n, s.U, op_n(s.W1, n), op_n(s.U, n));   // e^{-dtau K} U_R
+        if (nt % x.P.Nwrap == 0) wrap_R(x, nt);
+        measure(x);
+    }
+    gcopy(x.A.URc, s.U, n * n);
+    gcopy(x.A.G, s.G, n * n);
+    flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
+    if (threadIdx.x == 0) x.sc->seed = *s.seed;
+}
+
+// Local_sweep_pre (local_sweep.f90:80-94) with Prop_make's identities
+// (process_matrix.f90:37-47).
+template <int NMAX>
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS) pre_kernel(KernelArgs ka, const int* idx, int count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    if ((int)blockIdx.x >= count) return;
+    const int chain = idx[blockIdx.x];
+    Ctx<NMAX> x;
+    if (!setup_ctx(x, smem, ka, chain)) return;
+    auto& s = x.s;
+    const int n = x.n, L = x.P.L;
+    set_identity(n, s.U);
+    set_identity(n, s.G);
+    set_identity(n, x.A.VRc);
+    set_identity(n, x.A.ULc);
+    set_identity(n, x.A.VLc);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        x.A.DRc[i] = cmk(1.0, 0.0);
+        x.A.DLc[i] = cmk(1.0, 0.0);
+    }
+    __syncthreads();
+    gcopy(x.A.URs(0), s.U, n * n);
+    gcopy(x.A.VRs(0), x.A.VRc, n * n);
+    gcopy(x.A.DRs(0), x.A.DRc, n);
+    gcopy(s.W1, x.P.expP, n * n);
+    __syncthreads();
+    for (int nt = 1; nt <= L; ++nt) {
+        const double* ph = x.phi + (long)(nt - 1) * n * 2;
+        for (int ch = 0; ch < 2; ++ch) {
+            if (!x.P.active[ch]) continue;
+            const double ar = x.P.alpha_re[ch], ai = x.P.alpha_im[ch];
+            for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+                const double p = ph[(e / n) * 2 + ch];
+                s.U[e] = cmul(cexpz(cmk(ar * p, ai * p)), s.U[e]);
+            }
+            __syncthreads();
+        }
+        gemm_rs<TR, TC>(n, s.U, op_n(s.W1, n), op_n(s.U, n));
+        if (nt % x.P.Nwrap == 0) {
+            const int st = nt / x.P.Nwrap;
+            stab_UR(x);
+            gcopy(x.A.URs(st), s.U, n * n);
+            gcopy(x.A.VRs(st), x.A.VRc, n * n);
+            gcopy(x.A.DRs(st), x.A.DRc, n);
+            __syncthreads();
+            if (nt == L) {
+                stab_green_right_local(x, nt, true);
+                gcopy(s.G, s.W2, n * n);
+                __syncthreads();
+            }
+            gcopy(s.W1, x.P.expP, n * n);
+            __syncthreads();
+        }
+    }
+    gcopy(x.A.URc, s.U, n * n);
+    gcopy(x.A.G, s.G, n * n);
+}
+
+// LocalU_prop_therm / LocalU_metro_therm over the whole field, nwarm sweeps
+// (localU.f90:115-156, local_sweep.f90:64-78).  Each field value sees only its
+// own proposals, so fields are updated in parallel; the draw index of a
+// proposal is its position in the reference's sequential order.
+__global__ void warmup_kernel(KernelArgs ka, int nwarm) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    const ChainDev cd = ka.chains[chain];
+    const PointDev P = ka.pts[cd.point];
+    ChainScalars* sc = ka.sc + chain;
+    double* phi = ka.phi + cd.phi_off;
+    __shared__ double red[2 * 32];
+    __shared__ int chs[2];
+    __shared__ int nact;
+    if (threadIdx.x == 0) {
+        int a = 0;
+        for (int ch = 0; ch < 2; ++ch)
+            if (P.active[ch]) chs[a++] = ch;
+        nact = a;
+    }
+    __syncthreads();
+    const int A = nact, n = P.N, L = P.L;
+    const uint32_t s0 = sc->seed;
+    const unsigned long long per_sweep = (unsigned long long)L * A * n;
+    const uint32_t step = lcg_pow(2ull * per_sweep);
+    const double shift = fabs(P.shiftLoc);
+    double cnt[2] = {0.0, 0.0};
+    for (long long m = threadIdx.x; m < (long long)per_sweep; m += blockDim.x) {
+        const int i = (int)(m % n);
+        const int chpos = (int)((m / n) % A);
+        const int nt = (int)(m / ((long long)n * A));
+        const int ch = chs[chpos];
+        double p = phi[((long)nt * n + i) * 2 + ch];
+        uint32_t d1 = lcg_mul(lcg_pow(2ull * m + 1ull), s0);
+        for (int w = 0; w < nwarm; ++w) {
+            const uint32_t d2 = lcg_mul(kLcgA, d1);
+            const double xflip = lcg_u(d1), rnd = lcg_u(d2);
+            const double pn = p + (xflip - 0.5) * shift;
+            const double ratio = exp(-0.5 * pn * pn) / exp(-0.5 * p * p);
+            if (ratio > rnd) {
+                p = pn;
+                cnt[chpos] += 1.0;
+            }
+            d1 = lcg_mul(step, d1);
+        }
+        phi[((long)nt * n + i) * 2 + ch] = p;
+    }
+    double v[2] = {cnt[0], cnt[1]};
+    block_sum<2>(v, red);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < A; ++k) sc->therm_acc_sum[chs[k]] += v[k] / ((double)L * n);
+        sc->seed = lcg_mul(lcg_pow(2ull * per_sweep * (unsigned long long)nwarm), s0);
+    }
+}
+
+// Start of a bin: Local_sweep_reset (local_sweep.f90:54-62).
+__global__ void bin_reset_kernel(KernelArgs ka) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    double* o = ka.obs + (long)chain * ka.obs_stride;
+    for (int k = threadIdx.x; k < ka.obs_stride; k += blockDim.x) o[k] = 0.0;
+    if (threadIdx.x == 0) {
+        ChainScalars* sc = ka.sc + chain;
+        sc->nc[0] = sc->nc[1] = 0;
+        sc->nacc[0] = sc->nacc[1] = 0;
+        sc->nobs = 0;
+    }
+}
+
+// End of a bin: Obs_equal_ave and AccCounter%ratio (obser_equal.f90:66-93,
+// operator_Hubbard.f90:124-129).
+__global__ void bin_finish_kernel(KernelArgs ka) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    ChainScalars* sc = ka.sc + chain;
+    const int lq = ka.pts[ka.chains[chain].point].Lq;
+    const double z = 1.0 / (double)sc->nobs;
+    double* o = ka.obs + (long)chain * ka.obs_stride;
+    for (int k = threadIdx.x; k < kObsScalars + lq; k += blockDim.x) o[k] *= z;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ch = 0; ch < 2; ++ch)
+            if (sc->nc[ch] > 0) sc->acc_sum[ch] += (double)sc->nacc[ch] / (double)sc->nc[ch];
+    }
+}
+
+// Chain average per point (m_process_obs_equal, fourier_trans.f90:350-457):
+// out[p][k] = sum over chains of point p of obs[chain][k] / (chains of p).
+__global__ void point_average_kernel(KernelArgs ka, const int* point_chain_start, const int* point_chain_list,
+                                     double* out) {
+    const int p = blockIdx.x;
+    const int b = point_chain_start[p], e = point_chain_start[p + 1];
+    for (int k = threadIdx.x; k < ka.obs_stride; k += blockDim.x) {
+        double s = 0.0;
+        for (int c = b; c < e; ++c) s += ka.obs[(long)point_chain_list[c] * ka.obs_stride + k];
+        out[(long)p * ka.obs_stride + k] = (e > b) ? s / (double)(e - b) : 0.0;
+    }
+}
+
+// -0.5 * sum(phi^2) per chain (AuxConf_log_weight, fields.f90:29-33)
+__global__ void field_norm_kernel(KernelArgs ka, double* out) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    const ChainDev cd = ka.chains[chain];
+    const PointDev P = ka.pts[cd.point];
+    __shared__ double red[32];
+    const double* phi = ka.phi + cd.phi_off;
+    double v[1] = {0.0};
+    const long long tot = (long long)P.L * P.N * 2;
+    for (long long k = threadIdx.x; k < tot; k += blockDim.x) v[0] += phi[k] * phi[k];
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) out[chain] = -0.5 * v[0];
+}
+
+// ---------------------------------------------------------------------------
+template <int NMAX>
+static cudaError_t launch_cls(int which, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
+    if (count <= 0) return cudaSuccess;
+    const size_t sm = Smem<NMAX>::bytes();
+    cudaError_t e;
+    if (which == 0) {
+        e = cudaFuncSetAttribute(sweep_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        sweep_kernel<NMAX><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
+    } else {
+        e = cudaFuncSetAttribute(pre_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        pre_kernel<NMAX><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t upload_pow_table(const uint32_t* tab, int count) {
+    if (count > kMaxPow) return cudaErrorInvalidValue;
+    return cudaMemcpyToSymbol(c_apow, tab, sizeof(uint32_t) * count);
+}
+
+cudaError_t launch_sweep(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
+    return cls == 0 ? launch_cls<16>(0, ka, idx, count, st) : launch_cls<36>(0, ka, idx, count, st);
+}
+cudaError_t launch_pre(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
+    return cls == 0 ? launch_cls<16>(1, ka, idx, count, st) : launch_cls<36>(1, ka, idx, count, st);
+}
+cudaError_t launch_warmup(const KernelArgs& ka, int nwarm, cudaStream_t st) {
+    warmup_kernel<<<ka.nchains, 256, 0, st>>>(ka, nwarm);
+    return cudaGetLastError();
+}
+cudaError_t launch_bin_reset(const KernelArgs& ka, cudaStream_t st) {
+    bin_reset_kernel<<<ka.nchains, 64, 0, st>>>(ka);
+    return cudaGetLastError();
+}
+cudaError_t launch_bin_finish(const KernelArgs& ka, cudaStream_t st) {
+    bin_finish_kernel<<<ka.nchains, 64, 0, st>>>(ka);
+    return cudaGetLastError();
+}
+cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* start, const int* list, double* out,
+                                 cudaStream_t st) {
+    point_average_kernel<<<npts, 64, 0, st>>>(ka, start, list, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st) {
+    field_norm_kernel<<<ka.nchains, 256, 0, st>>>(ka, out);
+    return cudaGetLastError();
+}
+size_t smem_bytes(int cls) { return cls == 0 ? Smem<16>::bytes() : Smem<36>::bytes(); }
+int class_nmax(int cls) { return cls == 0 ? 16 : 36; }
+
+}  // namespace bq

@@ -1,0 +1,280 @@
+"""Host side of the B200 sweep: a batch of chains behind the C ABI, and the
+reference's run-directory contract on top of it.
+
+`Ensemble` holds one handle of libbafqmc_b200.so (chains of one or several
+parameter points).  `run_directory` reproduces `mpirun -np N bosonDQMC.out`
+(src/number_conserving/src/main.f90:22-85) for N chains on one GPU: it reads
+paramC_sets.txt / confin.txt / seeds.txt and appends the same per-bin files,
+info.txt and confout.txt.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from .observables import FILE_ORDER, OBS_SCALARS, decode
+from .params import NAUX, SolverParams, conf_transfer
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def point_struct(p: SolverParams) -> _lib.Point:
+    return _lib.Point(
+        sector=p.sector, Lx=p.Nlx, Ly=p.Nly, Ltrot=p.Ltrot, beta=p.Beta, U1=p.U1, U2=p.U2, mu=p.mu,
+        delta=p.delta, Nwrap=p.Nwrap, shiftLoc=p.shiftLoc, iniType=p.iniType, iniAmpl=p.iniAmpl,
+        iniBias1=p.iniBias[0], iniBias2=p.iniBias[1], LxTherm=p.NlxTherm, LyTherm=p.NlyTherm,
+        LtrotTherm=p.LtrotTherm)
+
+
+class Ensemble:
+    """Independent Markov chains (the reference's MPI ranks) on one GPU."""
+
+    def __init__(self, points: list[SolverParams], chain_point, device: int = 0):
+        self.lib = _lib.load()
+        self.points = list(points)
+        self.chain_point = np.ascontiguousarray(chain_point, dtype=np.int32)
+        self.nchains = int(self.chain_point.size)
+        arr = (_lib.Point * len(points))(*[point_struct(p) for p in points])
+        h = C.c_void_p()
+        _lib.check(self.lib.bafqmc_create(arr, len(points), _iptr(self.chain_point), self.nchains, device,
+                                          C.byref(h)))
+        self.h = h
+        self.stride = self.lib.bafqmc_obs_stride(h)
+        self.dims = []
+        for i in range(len(points)):
+            nd, lq, lt, nst = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            _lib.check(self.lib.bafqmc_point_dim(h, i, C.byref(nd), C.byref(lq), C.byref(lt), C.byref(nst)))
+            self.dims.append((nd.value, lq.value, lt.value, nst.value))
+        self.phi_sizes = [self.dims[p][2] * self.dims[p][0] * NAUX for p in self.chain_point]
+        self.phi_offsets = np.concatenate([[0], np.cumsum(self.phi_sizes)]).astype(np.int64)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bafqmc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state
+    def fields_from_seeds(self, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        assert s.size == self.nchains
+        _lib.check(self.lib.bafqmc_fields_from_seeds(self.h, _iptr(s)))
+
+    def set_state(self, seeds, phis):
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).ravel() for p in phis]))
+        assert flat.size == self.phi_offsets[-1]
+        _lib.check(self.lib.bafqmc_set_state(self.h, _iptr(s), _dptr(flat)))
+
+    def get_state(self):
+        s = np.zeros(self.nchains, dtype=np.int32)
+        flat = np.zeros(int(self.phi_offsets[-1]), dtype=np.float64)
+        _lib.check(self.lib.bafqmc_get_state(self.h, _iptr(s), _dptr(flat)))
+        phis = []
+        for c in range(self.nchains):
+            nd, _, lt, _ = self.dims[self.chain_point[c]]
+            phis.append(flat[self.phi_offsets[c]:self.phi_offsets[c + 1]].reshape(lt, nd, NAUX))
+        return s, phis
+
+    # ---- the sweep path
+    def warmup_prior(self, nwarm: int):
+        _lib.check(self.lib.bafqmc_warmup_prior(self.h, int(nwarm)))
+
+    def pre(self):
+        _lib.check(self.lib.bafqmc_pre(self.h))
+
+    def sweep(self, nsweep: int = 1):
+        _lib.check(self.lib.bafqmc_sweep(self.h, int(nsweep)))
+
+    def synchronize(self):
+        _lib.check(self.lib.bafqmc_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.bafqmc_stream(self.h) or 0)
+
+    # ---- results
+    def chain_obs_raw(self) -> np.ndarray:
+        out = np.zeros((self.nchains, self.stride))
+        _lib.check(self.lib.bafqmc_bin_chain_obs(self.h, _dptr(out)))
+        return out
+
+    def point_obs_raw(self) -> np.ndarray:
+        out = np.zeros((len(self.points), self.stride))
+        _lib.check(self.lib.bafqmc_bin_point_obs(self.h, _dptr(out)))
+        return out
+
+    def chain_obs(self) -> list[dict]:
+        raw = self.chain_obs_raw()
+        return [decode(raw[c], self.dims[self.chain_point[c]][1]) for c in range(self.nchains)]
+
+    def point_obs(self) -> list[dict]:
+        raw = self.point_obs_raw()
+        return [decode(raw[p], self.dims[p][1]) for p in range(len(self.points))]
+
+    def green(self, chain: int) -> np.ndarray:
+        nd = self.dims[self.chain_point[chain]][0]
+        out = np.zeros(2 * nd * nd)
+        _lib.check(self.lib.bafqmc_get_green(self.h, int(chain), _dptr(out)))
+        return out.view(np.complex128).reshape(nd, nd)
+
+    def log_weight(self) -> np.ndarray:
+        out = np.zeros(self.nchains)
+        _lib.check(self.lib.bafqmc_log_weight(self.h, _dptr(out)))
+        return out
+
+    def counters(self) -> np.ndarray:
+        out = np.zeros((self.nchains, _lib.COUNTERS))
+        _lib.check(self.lib.bafqmc_counters(self.h, _dptr(out)))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# per-bin diagnostics of G (pole_diagnostics.f90:91-123).  log_weight comes from
+# the device (stabilised factorisation of I - B); the eigen/singular values are
+# taken on the host from the device-computed G.
+def pole_diagnostics(G: np.ndarray, log_weight: float) -> dict:
+    small = np.finfo(float).tiny
+    ev = np.linalg.eigvals(G)
+    sv = np.linalg.svd(G, compute_uv=False)
+    z = np.where(np.abs(ev) <= small, complex(1.0 / small, 0.0), 1.0 / np.where(ev == 0, 1, ev))
+    pd = max(float(np.min(np.abs(z))), small)
+    return {"pole_z": z, "pole_distance": pd, "pole_x": -math.log10(pd),
+            "green_spectral_radius": float(np.max(np.abs(ev))), "green_smax": float(np.max(sv)),
+            "log_weight": float(log_weight)}
+
+
+# ---------------------------------------------------------------------------
+# output formats of the reference writer
+def _lst(*vals) -> str:
+    """Fortran list-directed record: blank-separated values, lossless."""
+    return " " + "  ".join(repr(float(v)) for v in vals) + "\n"
+
+
+def _es(v: float, width: int = 24, digits: int = 16, expdigits: int = 2) -> str:
+    m, e = f"{v:.{digits}E}".split("E")
+    ei = int(e)
+    s = f"{m}E{'-' if ei < 0 else '+'}{abs(ei):0{expdigits}d}"
+    return s.rjust(width)
+
+
+def append_bin(run_dir: Path, obs: dict) -> None:
+    """m_write_obs_equal (fourier_trans.f90:250-348)."""
+    for name in FILE_ORDER:
+        v = obs[name]
+        with open(run_dir / name, "a") as f:
+            if name == "density_site_total":
+                f.write("".join(_es(x) + " " for x in v) + "\n")
+            elif isinstance(v, complex):
+                f.write(_lst(v.real, v.imag))
+            else:
+                f.write(_lst(v))
+
+
+def append_pole(run_dir: Path, diags: list[dict]) -> None:
+    """PoleDiagnostics_write (pole_diagnostics.f90:126-187): one row per chain."""
+    with open(run_dir / "pole_z", "a") as f:
+        for d in diags:
+            f.write("".join(" " + _es(z.real, expdigits=3) + " " + _es(z.imag, expdigits=3) for z in d["pole_z"]))
+            f.write("\n")
+    for name in ("pole_distance", "pole_x", "green_spectral_radius", "green_smax", "log_weight"):
+        with open(run_dir / name, "a") as f:
+            for d in diags:
+                f.write(_es(d[name], expdigits=3) + "\n")
+
+
+def read_confin(path: Path, p: SolverParams, nchains: int):
+    toks = Path(path).read_text().split()
+    if int(float(toks[0].replace("D", "E"))) == 0:
+        return None
+    per = p.LtrotTherm * p.NlxTherm * p.NlyTherm * NAUX
+    out, pos = [], 0
+    for _ in range(nchains):
+        seed = int(float(toks[pos])); pos += 1
+        vals = np.array([float(t.replace("D", "E").replace("d", "e")) for t in toks[pos:pos + per]])
+        pos += per
+        out.append((seed, conf_transfer(p, vals)))
+    return out
+
+
+def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print) -> dict:
+    """The reference program for `mpirun -np nchains` in run_dir, on one GPU."""
+    run_dir = Path(run_dir)
+    t0 = time.time()
+    p = SolverParams.from_file(run_dir / "paramC_sets.txt")
+    info = open(run_dir / "info.txt", "w")
+    w = lambda label, v: info.write(f" {label:<47}:{v!r:>26}\n")
+    info.write(" =========================\n DQMC for boson Hubbard on triangular lattice\n")
+    w("Linear lengh Lx", p.Nlx); w("Linear lengh Ly", p.Nly); w("Hopping t", 1.0)
+    w("Hubbard U1 (relative-density, repulsive)", p.U1); w("Hubbard U2 (total-density, attractive)", p.U2)
+    w("chemical potential", p.mu); w("Local update auxiliary field magnitude Shift", p.shiftLoc)
+    if p.is_warm:
+        w("# Warm", p.Nwarm); w("Thermalize U1 relative-field magnitude", p.shiftWarm[0])
+        w("Thermalize U2 total-field magnitude", p.shiftWarm[1])
+    w("Choosing initial distribution type", p.iniType); w("Magnitude of Gaussian distribution", p.iniAmpl)
+    w("Beta", p.Beta); w("Trotter number", p.Ltrot); w("=>Dtau", p.Dtau); w("N_Ortho", p.Nwrap)
+    w("# Bins", p.Nbin); w("# Nsweep in one bin", p.Nsweep); w("# Cores", nchains)
+    ens = Ensemble([p], np.zeros(nchains, dtype=np.int32), device=device)
+    confin = read_confin(run_dir / "confin.txt", p, nchains)
+    if confin is None:
+        seeds = [int(r.split()[0]) for r in (run_dir / "seeds.txt").read_text().split("\n") if r.strip()][:nchains]
+        if len(seeds) < nchains:
+            raise ValueError("seeds.txt has fewer rows than chains")
+        ens.fields_from_seeds(seeds)
+    else:
+        ens.set_state([s for s, _ in confin], [phi for _, phi in confin])
+    if p.is_warm:
+        ens.warmup_prior(p.Nwarm)
+        cnt = ens.counters()
+        for ch, name in ((0, "Thermalize U1 Accept Ratio"), (1, "Thermalize U2 Accept Ratio")):
+            if abs((p.U1, p.U2)[ch]) > 1e-10:
+                w(name, float(cnt[:, 2 + ch].sum() / (nchains * p.Nwarm)))
+    else:
+        info.write(" Skipping Bosonic warm-up\n")
+    ens.pre()
+    for nbc in range(p.Nbin):
+        ens.sweep(p.Nsweep)
+        append_bin(run_dir, ens.point_obs()[0])
+        if pole:
+            lw = ens.log_weight()
+            append_pole(run_dir, [pole_diagnostics(ens.green(c), lw[c]) for c in range(nchains)])
+    cnt = ens.counters()
+    for ch, name in ((0, "Accept_U1_shift"), (1, "Accept_U2_shift")):
+        if abs((p.U1, p.U2)[ch]) > 1e-10:
+            w(name, float(cnt[:, ch].sum() / (nchains * p.Nbin)))
+    if np.any(cnt[:, 6] != 0):
+        info.write(" non-finite Green's function detected in chains: "
+                   + " ".join(str(i) for i in np.nonzero(cnt[:, 6])[0]) + "\n")
+    w("Max diff Matrix", float(cnt[:, 4].max()))
+    w("Mean diff Matrix", float(cnt[:, 5].sum() / (2 * nchains * p.Nbin * p.Nst * p.Nsweep)))
+    w("Tot CPU time", time.time() - t0)
+    info.close()
+    seeds, phis = ens.get_state()
+    with open(run_dir / "confout.txt", "w") as f:   # conf_out (fields.f90:236-278)
+        for c in range(nchains):
+            f.write(f" {int(seeds[c])}\n")
+            f.write("".join(f" {v!r}\n" for v in phis[c].ravel()))
+    ens.close()
+    return {"params": p, "counters": cnt}

@@ -1,0 +1,121 @@
+/*
+ * bafqmc_b200.h -- C ABI of the B200 implementation of the BAFQMC
+ * finite-temperature auxiliary-field sweep (number-conserving solver).
+ *
+ * The reference exposes this path as a process/file contract: a driver writes
+ * paramC_sets.txt, confin.txt and seeds.txt into a run directory and launches
+ * `mpirun -np N build/bosonDQMC.out` (src/number_conserving/run_paper.py:113,162),
+ * one Markov chain per MPI rank.  Each entry point below replaces one step of
+ * that program (src/number_conserving/src/main.f90:22-85); the comment names
+ * the reference routine it stands in for.  A "chain" here is one MPI rank of
+ * the reference; a "point" is one paramC_sets.txt parameter set.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative BAFQMC_E* code;
+ *     bafqmc_last_error() gives a message for the calling thread.
+ *   - Host buffers are caller-owned; device memory belongs to the handle.
+ *   - A handle owns one CUDA stream; calls are asynchronous on that stream
+ *     unless they return host data.  A handle is not thread-safe.
+ *   - Complex matrices are row-major, element (i,j) = <b_i b_j^dagger>,
+ *     stored as interleaved (re, im) doubles.
+ *   - Fields are stored per chain as phi[nt][site][aux] (aux fastest), the
+ *     order of confin.txt / confout.txt (fields.f90:81-103, 265-273).
+ */
+#ifndef BAFQMC_B200_H
+#define BAFQMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BAFQMC_OK 0
+#define BAFQMC_EARG (-1)        /* invalid argument (calc_basic.f90:61-62,103 `stop`) */
+#define BAFQMC_ECUDA (-2)       /* CUDA runtime error */
+#define BAFQMC_EUNSUPPORTED (-3)/* size or sector not built in this library */
+#define BAFQMC_ESTATE (-4)      /* call out of order (e.g. sweep before pre) */
+#define BAFQMC_ENUMERIC (-5)    /* non-finite Green's function detected */
+
+/* Number of scalar observable slots per chain before the site densities. */
+#define BAFQMC_OBS_SCALARS 26
+
+/* One parameter point: the seven lines of paramC_sets.txt
+ * (calc_basic.f90:52-59) plus the sector.  `delta` is the pairing amplitude
+ * of the Nambu solver (src/pairing/src/calc_basic.f90:51) and must be 0 for
+ * sector 0.  t is fixed to 1 as in the reference (calc_basic.f90:94). */
+typedef struct bafqmc_point {
+    int sector;              /* 0 = number-conserving (Ndim = Lx*Ly) */
+    int Lx, Ly, Ltrot;
+    double beta, U1, U2, mu, delta;
+    int Nwrap;
+    double shiftLoc;
+    int iniType;             /* 1 uniform, 2 Gaussian, 3 |Gaussian| (fields.f90:115-154) */
+    double iniAmpl, iniBias1, iniBias2;
+    int LxTherm, LyTherm, LtrotTherm;   /* size of the seeded/confin field, tiled (fields.f90:156-234) */
+} bafqmc_point;
+
+typedef struct bafqmc_handle bafqmc_handle;
+
+/* Model_init + Prop%make + WrList%make + Stabilize_init (model.f90:14-39,
+ * main.f90:28-34): lattice tables, e^{-+dtau K}, HS factors and device state
+ * for `nchains` chains, chain c using point chain_point[c]. */
+int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
+                  bafqmc_handle** out);
+void bafqmc_destroy(bafqmc_handle* h);
+const char* bafqmc_last_error(void);
+
+/* Sizes: Ndim of a point, and the per-chain observable stride. */
+int bafqmc_point_dim(const bafqmc_handle* h, int point, int* ndim, int* lq, int* ltrot, int* nst);
+int bafqmc_obs_stride(const bafqmc_handle* h);
+int bafqmc_num_chains(const bafqmc_handle* h);
+
+/* conf_set + conf_transfer (fields.f90:115-234): fields of each chain from its
+ * seed (seeds.txt row), the seed advanced past the draws as in conf_therm_in. */
+int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds);
+
+/* confin path of conf_therm_in (fields.f90:81-103): explicit seed and field
+ * (already of the full Ltrot x Ns size) per chain.  get_state is conf_out's
+ * payload (fields.f90:236-278). */
+int bafqmc_set_state(bafqmc_handle* h, const int32_t* seeds, const double* phi);
+int bafqmc_get_state(bafqmc_handle* h, int32_t* seeds, double* phi);
+
+/* Local_sweep_therm x nwarm (local_sweep.f90:64-78): prior-only warm-up. */
+int bafqmc_warmup_prior(bafqmc_handle* h, int nwarm);
+
+/* Local_sweep_pre (local_sweep.f90:80-94): right UDV slots and G(beta). */
+int bafqmc_pre(bafqmc_handle* h);
+
+/* One measurement bin: Local_sweep%sweep (local_sweep.f90:136-161) with
+ * nsweep left+right sweeps, then Obs_equal_ave and the acceptance ratio. */
+int bafqmc_sweep(bafqmc_handle* h, int nsweep);
+
+/* Observables of the last bin.  chain_obs: [nchains][stride] (per chain, the
+ * values each rank holds before MPI_REDUCE); point_obs: [npts][stride], the
+ * chain average that m_process_obs_equal writes (fourier_trans.f90:350-457).
+ * Layout: BAFQMC_OBS_SCALARS slots (see bafqmc_b200/observables.py) then Lq
+ * site densities. */
+int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs);
+int bafqmc_bin_point_obs(bafqmc_handle* h, double* point_obs);
+
+/* Prop%Gr of one chain (row-major complex). */
+int bafqmc_get_green(bafqmc_handle* h, int chain, double* G);
+
+/* log_weight = -1/2 sum phi^2 + 2 log|det G| per chain
+ * (pole_diagnostics.f90:119; log|det G| from the last stabilised
+ * (I - B(beta,0)) factorisation). */
+int bafqmc_log_weight(bafqmc_handle* h, double* out);
+
+/* Per chain, 10 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
+ * status, seed, nobs, reserved (AccCounter, Prop%Xmaxm/Xmeanm). */
+#define BAFQMC_COUNTERS 10
+int bafqmc_counters(bafqmc_handle* h, double* out);
+
+int bafqmc_synchronize(bafqmc_handle* h);
+/* The handle's cudaStream_t, for event timing by the caller. */
+void* bafqmc_stream(bafqmc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
