@@ -57,6 +57,7 @@ SIGNATURES = {
     "bafqmc_get_green": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_log_weight": (C.c_int, [_P, _DP]),
     "bafqmc_counters": (C.c_int, [_P, _DP]),
+    "bafqmc_phase_timers": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_synchronize": (C.c_int, [_P]),
     "bafqmc_stream": (_P, [_P]),
 }

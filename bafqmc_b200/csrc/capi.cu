@@ -193,6 +193,7 @@ struct bafqmc_handle {
     double* d_obs = nullptr;
     ChainScalars* d_sc = nullptr;
     bool have_fields = false, pre_done = false, bin_done = false;
+    int timers = 0;
 
     bq::KernelArgs args() const {
         bq::KernelArgs ka;
@@ -204,6 +205,7 @@ struct bafqmc_handle {
         ka.phi = d_phi;
         ka.obs = d_obs;
         ka.sc = d_sc;
+        ka.timers = timers;
         return ka;
     }
 };
@@ -626,6 +628,19 @@ int bafqmc_counters(bafqmc_handle* h, double* out) {
         o[8] = (double)sc[c].nobs;
         o[9] = 0.0;
     }
+    return BAFQMC_OK;
+}
+
+int bafqmc_phase_timers(bafqmc_handle* h, int enable, double* out) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    h->timers = enable ? 1 : 0;
+    if (!out) return BAFQMC_OK;
+    CK(cudaSetDevice(h->device));
+    std::vector<ChainScalars> sc(h->nchains);
+    CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < h->nchains; ++c)
+        for (int k = 0; k < 4; ++k) out[(size_t)c * 4 + k] = (double)sc[c].cyc[k];
     return BAFQMC_OK;
 }
 

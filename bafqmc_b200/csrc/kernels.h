@@ -19,6 +19,7 @@ struct KernelArgs {
     double* phi;
     double* obs;
     ChainScalars* sc;
+    int timers;   // nonzero: accumulate per-phase SM cycles into ChainScalars::cyc
 };
 
 // size classes of the fused sweep kernel: 0 -> N <= 16, 1 -> N <= 36

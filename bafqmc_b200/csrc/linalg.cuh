@@ -12,6 +12,10 @@
 #pragma once
 #include "cplx.cuh"
 
+// Factorisation routines are kept out of line: they run once per wrap, and
+// inlining them into the sweep kernel costs registers on the per-slice path.
+#define COLD __device__ __noinline__
+
 // Strided operand view: element (r, c) = p[r*sr + c*sc], optionally conjugated.
 // A transposed view swaps the strides.  p may point to shared or global memory.
 struct MatOp {
@@ -33,7 +37,7 @@ enum { TRI_NONE = 0, TRI_A_UPPER = 1, TRI_B_LOWER_FROM_C = 2 };
 // tri = TRI_A_UPPER zeroes A(r,k) for k < r (ZTRMM 'L','U','N');
 // tri = TRI_B_LOWER_FROM_C zeroes B(k,c) for k < c (ZTRMM 'R','U','C').
 template <int TR, int TC>
-DEVI void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
+COLD void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const int g = threadIdx.x;
     const bool active = g < ncg * nrg;
@@ -77,21 +81,72 @@ DEVI void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
     __syncthreads();
 }
 
+// C = A * B with A, B, C n x n row-major in shared memory (C may alias A or
+// B); the per-slice propagation products.
+template <int TR, int TC>
+DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
+    const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
+    const int g = threadIdx.x;
+    const bool active = g < ncg * nrg;
+    const int r0 = active ? (g / ncg) * TR : 0, c0 = active ? (g % ncg) * TC : 0;
+    cplx acc[TR][TC];
+#pragma unroll
+    for (int i = 0; i < TR; ++i)
+#pragma unroll
+        for (int j = 0; j < TC; ++j) acc[i][j] = cmk(0.0, 0.0);
+    if (active) {
+        int ra[TR], cb[TC];
+#pragma unroll
+        for (int i = 0; i < TR; ++i) ra[i] = min(r0 + i, n - 1) * n;
+#pragma unroll
+        for (int j = 0; j < TC; ++j) cb[j] = min(c0 + j, n - 1);
+        for (int k = 0; k < n; ++k) {
+            cplx a[TR], b[TC];
+#pragma unroll
+            for (int i = 0; i < TR; ++i) a[i] = A[ra[i] + k];
+#pragma unroll
+            for (int j = 0; j < TC; ++j) b[j] = B[k * n + cb[j]];
+#pragma unroll
+            for (int i = 0; i < TR; ++i)
+#pragma unroll
+                for (int j = 0; j < TC; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
+        }
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < TR; ++i)
+#pragma unroll
+            for (int j = 0; j < TC; ++j) {
+                const int r = r0 + i, c = c0 + j;
+                if (r < n && c < n) C[r * n + c] = acc[i][j];
+            }
+    }
+    __syncthreads();
+}
+
 // dst = op(src) elementwise copy for an n x n matrix (dst must not alias src
 // unless op is the identity view).
-DEVI void copy_op(int n, cplx* dst, MatOp src) {
+COLD void copy_op(int n, cplx* dst, MatOp src) {
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) dst[e] = src.at(e / n, e % n);
     __syncthreads();
 }
 
-// In-place conjugate transpose via register staging (n*n <= 8*blockDim).
-DEVI void conj_transpose_inplace(int n, cplx* A) {
-    cplx v[8];
-    int k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) v[k] = cconj(A[(e % n) * n + e / n]);
+// In-place conjugate transpose via register staging; MAXE >= ceil(n*n/blockDim).
+template <int MAXE>
+COLD void conj_transpose_inplace(int n, cplx* A) {
+    cplx v[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) v[k] = cconj(A[(e % n) * n + e / n]);
+    }
     __syncthreads();
-    k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) A[e] = v[k];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) A[e] = v[k];
+    }
     __syncthreads();
 }
 
@@ -145,7 +200,7 @@ struct QRScratch {
 // QDRP_decompose post-step (stabilization.f90:41-67): d[i] = |R_ii| and row i of
 // the upper triangle divided by d[i].  On exit A holds the scaled R in its upper
 // triangle and the Householder vectors (unit leading entry implicit) below it.
-DEVI void qrp_inplace(int n, cplx* A, QRScratch s) {
+COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int lane8 = tid & 7, seg = tid >> 3, nseg = nthr >> 3;
     const double tol3z = 1.0536712127723509e-08;   // sqrt(2^-53), LAPACK's sqrt(dlamch('E'))
@@ -261,7 +316,8 @@ DEVI void qrp_inplace(int n, cplx* A, QRScratch s) {
 
 // Q = H_0 H_1 ... H_{n-1} (ZUNGQR) from the reflectors stored below the
 // diagonal of F, written to Q (must not alias F).  conjT writes Q^H instead.
-DEVI void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
+template <int MAXE>
+COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     for (int e = tid; e < n * n; e += blockDim.x) Q[e] = cmk((e / n) == (e % n) ? 1.0 : 0.0, 0.0);
     __syncthreads();
@@ -283,11 +339,11 @@ DEVI void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
         }
         __syncthreads();
     }
-    if (conjT) conj_transpose_inplace(n, Q);
+    if (conjT) conj_transpose_inplace<MAXE>(n, Q);
 }
 
 // C <- Q^H C (ZUNMQR 'L','C'), reflectors in F.
-DEVI void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
+COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     for (int i = 0; i < n; ++i) {
         const cplx ct = cconj(tau[i]);
@@ -310,7 +366,7 @@ DEVI void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
 }
 
 // C <- C Q (ZUNMQR 'R','N'), reflectors in F.
-DEVI void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
+COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     for (int i = 0; i < n; ++i) {
         const cplx t = tau[i];
@@ -334,7 +390,7 @@ DEVI void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
 
 // C <- R^{-1} C with R the upper triangle of F (ZTRSM 'L','U','N','N').
 // Column-parallel back substitution: one 8-lane segment per column.
-DEVI void trsm_left_upper(int n, const cplx* F, cplx* C) {
+COLD void trsm_left_upper(int n, const cplx* F, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     for (int c = seg; c < n; c += nseg) {
         for (int i = n - 1; i >= 0; --i) {
@@ -351,7 +407,7 @@ DEVI void trsm_left_upper(int n, const cplx* F, cplx* C) {
 
 // C <- C R^{-H} with R the upper triangle of F (ZTRSM 'R','U','C','N').
 // Row-parallel: X R^H = C, solved for columns n-1 .. 0.
-DEVI void trsm_right_upperH(int n, const cplx* F, cplx* C) {
+COLD void trsm_right_upperH(int n, const cplx* F, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     for (int r = seg; r < n; r += nseg) {
         for (int c = n - 1; c >= 0; --c) {
@@ -368,32 +424,44 @@ DEVI void trsm_right_upperH(int n, const cplx* F, cplx* C) {
 
 // Row permutation in place.  forward: out[k][:] = in[piv[k]][:] (ZLAPMR .true.,
 // i.e. P^T X); backward: out[piv[k]][:] = in[k][:] (ZLAPMR .false., i.e. P X).
-DEVI void permute_rows(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
-    cplx v[8];
-    int k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) {
-        int r = e / n, c = e % n;
-        int src = forward ? piv[r] : ipiv[r];
-        v[k] = C[src * n + c];
+template <int MAXE>
+COLD void permute_rows(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
+    cplx v[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) {
+            const int r = e / n, c = e % n;
+            v[k] = C[(forward ? piv[r] : ipiv[r]) * n + c];
+        }
     }
     __syncthreads();
-    k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) C[e] = v[k];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) C[e] = v[k];
+    }
     __syncthreads();
 }
 
 // Column permutation in place.  forward: out[:, k] = in[:, piv[k]] (ZLAPMT
 // .true., X P); backward: out[:, piv[k]] = in[:, k] (ZLAPMT .false., X P^T).
-DEVI void permute_cols(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
-    cplx v[8];
-    int k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) {
-        int r = e / n, c = e % n;
-        int src = forward ? piv[c] : ipiv[c];
-        v[k] = C[r * n + src];
+template <int MAXE>
+COLD void permute_cols(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
+    cplx v[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) {
+            const int r = e / n, c = e % n;
+            v[k] = C[r * n + (forward ? piv[c] : ipiv[c])];
+        }
     }
     __syncthreads();
-    k = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x, ++k) C[e] = v[k];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e < n * n) C[e] = v[k];
+    }
     __syncthreads();
 }

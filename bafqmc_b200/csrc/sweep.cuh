@@ -52,6 +52,7 @@ struct ChainScalars {
     double xmax, xmean;         // stabilisation drift (Prop%Xmaxm, Prop%Xmeanm)
     double logdetM;             // sum log D of the last (I-B) factorisation at tau = beta
     double pad;
+    long long cyc[4];           // SM cycles per phase: local updates, slice products, measurement, wraps
 };
 
 struct ChainDev {

@@ -14,69 +14,74 @@ namespace bq {
 __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 
 template <int NMAX> struct Cfg;
-template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2; };
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3; };
+template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6; };
+
+// Dynamic shared memory of the sweep kernels.  Every buffer sits at a
+// compile-time offset, so device code addresses it without holding pointers.
+extern __shared__ __align__(16) unsigned char bq_smem[];
 
 template <int NMAX>
 struct Smem {
-    cplx *G, *U, *W1, *W2;
-    cplx *tau, *col[2], *row[2], *delta, *eao, *ean, *ebo, *ebn, *coef, *cbc;
-    double *rg, *u2, *phin, *vn1, *vn2, *d, *red, *obs;
-    int *piv, *ipiv, *accf, *ibc;
-    uint32_t* seed;
-
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
-    static constexpr size_t bytes() {
-        return sizeof(cplx) * (4 * NMAX * NMAX + 11 * NMAX + 2 + 4) +
-               sizeof(double) * (6 * NMAX + kRed + kObsScalars + NMAX) +
-               sizeof(int) * (3 * NMAX + 4) + 16;
-    }
-    DEVI void carve(unsigned char* base) {
-        cplx* c = reinterpret_cast<cplx*>(base);
-        G = c; c += NMAX * NMAX;
-        U = c; c += NMAX * NMAX;
-        W1 = c; c += NMAX * NMAX;
-        W2 = c; c += NMAX * NMAX;
-        tau = c; c += NMAX;
-        col[0] = c; c += NMAX;
-        col[1] = c; c += NMAX;
-        row[0] = c; c += NMAX;
-        row[1] = c; c += NMAX;
-        delta = c; c += NMAX;
-        eao = c; c += NMAX;
-        ean = c; c += NMAX;
-        ebo = c; c += NMAX;
-        ebn = c; c += NMAX;
-        c += NMAX;  // spare
-        coef = c; c += 2;
-        cbc = c; c += 4;
-        double* dd = reinterpret_cast<double*>(c);
-        rg = dd; dd += NMAX;
-        u2 = dd; dd += NMAX;
-        phin = dd; dd += NMAX;
-        vn1 = dd; dd += NMAX;
-        vn2 = dd; dd += NMAX;
-        d = dd; dd += NMAX;
-        red = dd; dd += kRed;
-        obs = dd; dd += kObsScalars + NMAX;
-        int* ii = reinterpret_cast<int*>(dd);
-        piv = ii; ii += NMAX;
-        ipiv = ii; ii += NMAX;
-        accf = ii; ii += NMAX;
-        ibc = ii; ii += 4;
-        seed = reinterpret_cast<uint32_t*>(ii);
-    }
-    DEVI QRScratch qr() const { return QRScratch{tau, piv, ipiv, vn1, vn2, d, const_cast<cplx*>(cbc), ibc}; }
+    static constexpr size_t MM = sizeof(cplx) * NMAX * NMAX, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
+    static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
+    static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + 2 * VC, oDelta = oRow + 2 * VC;
+    static constexpr size_t oEao = oDelta + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
+    static constexpr size_t oCoef = oEbn + VC, oCbc = oCoef + 2 * sizeof(cplx);
+    static constexpr size_t oP = oCbc + 4 * sizeof(cplx);
+    static constexpr size_t oRg = oP + ((sizeof(PointDev) + 15) / 16) * 16;
+    static constexpr size_t oU2 = oRg + VD, oPhin = oU2 + VD, oVn1 = oPhin + VD, oVn2 = oVn1 + VD, oD = oVn2 + VD;
+    static constexpr size_t oRed = oD + VD, oObs = oRed + sizeof(double) * kRed;
+    static constexpr size_t oPiv = oObs + sizeof(double) * (kObsScalars + NMAX);
+    static constexpr size_t oIpiv = oPiv + sizeof(int) * NMAX, oAccf = oIpiv + sizeof(int) * NMAX;
+    static constexpr size_t oIbc = oAccf + sizeof(int) * NMAX, oSeed = oIbc + 4 * sizeof(int);
+    static constexpr size_t bytes() { return oSeed + 16; }
+
+    template <class T>
+    static DEVI T* at(size_t off) { return reinterpret_cast<T*>(bq_smem + off); }
+    DEVI cplx* G() const { return at<cplx>(oG); }
+    DEVI cplx* U() const { return at<cplx>(oU); }
+    DEVI cplx* W1() const { return at<cplx>(oW1); }
+    DEVI cplx* W2() const { return at<cplx>(oW2); }
+    DEVI cplx* tau() const { return at<cplx>(oTau); }
+    DEVI cplx* col(int par) const { return at<cplx>(oCol) + par * NMAX; }
+    DEVI cplx* row(int par) const { return at<cplx>(oRow) + par * NMAX; }
+    DEVI cplx* delta() const { return at<cplx>(oDelta); }
+    DEVI cplx* eao() const { return at<cplx>(oEao); }
+    DEVI cplx* ean() const { return at<cplx>(oEan); }
+    DEVI cplx* ebo() const { return at<cplx>(oEbo); }
+    DEVI cplx* ebn() const { return at<cplx>(oEbn); }
+    DEVI cplx* coef() const { return at<cplx>(oCoef); }
+    DEVI cplx* cbc() const { return at<cplx>(oCbc); }
+    DEVI PointDev* P() const { return at<PointDev>(oP); }
+    DEVI double* rg() const { return at<double>(oRg); }
+    DEVI double* u2() const { return at<double>(oU2); }
+    DEVI double* phin() const { return at<double>(oPhin); }
+    DEVI double* vn1() const { return at<double>(oVn1); }
+    DEVI double* vn2() const { return at<double>(oVn2); }
+    DEVI double* d() const { return at<double>(oD); }
+    DEVI double* red() const { return at<double>(oRed); }
+    DEVI double* obs() const { return at<double>(oObs); }
+    DEVI int* piv() const { return at<int>(oPiv); }
+    DEVI int* ipiv() const { return at<int>(oIpiv); }
+    DEVI int* accf() const { return at<int>(oAccf); }
+    DEVI int* ibc() const { return at<int>(oIbc); }
+    DEVI uint32_t* seed() const { return at<uint32_t>(oSeed); }
+    DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
 
+// Per-chain view: the chain's arena base and fields in registers, the point
+// parameters in shared memory.
 template <int NMAX>
 struct Ctx {
     Smem<NMAX> s;
-    PointDev P;
-    Arena A;
+    cplx* abase;
     double* phi;
     ChainScalars* sc;
     int n;
+    DEVI const PointDev& P() const { return *s.P(); }
+    DEVI Arena A() const { return make_arena(abase, n); }
 };
 
 // ---------------------------------------------------------------------------
@@ -91,8 +96,8 @@ DEVI void set_identity(int n, cplx* A) {
 template <int NMAX>
 DEVI void load_expT(Ctx<NMAX>& x) {
     const int nn = x.n * x.n;
-    gcopy(x.s.W1, x.P.expP, nn);
-    gcopy(x.s.W2, x.P.expM, nn);
+    gcopy(x.s.W1(), x.P().expP, nn);
+    gcopy(x.s.W2(), x.P().expM, nn);
     __syncthreads();
 }
 
@@ -104,14 +109,55 @@ DEVI void load_expT(Ctx<NMAX>& x) {
 // Metropolis decision right after its own update, and the owners of the next
 // row/column stage them, so the rank-1 update of site i and the staging for
 // site i+1 share one pass.  G lives in registers for the whole loop.
+
+// Metropolis decision for site j from the (wrapped) diagonal element gjj:
+// ratio_det = 1/(1 + Delta (1 - G_jj)), accept if |r_gauss * |ratio_det|^2| > u;
+// on accept the rank-1 coefficient is -ratio_det * Delta (localU.f90:56-71).
+template <int NMAX>
+DEVI void metro_decide(Smem<NMAX>& s, int j, cplx gjj, int par) {
+    const cplx d = s.delta()[j];
+    const cplx w = cmk(1.0 + (d.x * (1.0 - gjj.x) + d.y * gjj.y), d.y * (1.0 - gjj.x) - d.x * gjj.y);
+    const double nw = w.x * w.x + w.y * w.y;
+    const double inv = 1.0 / nw;
+    const bool accept = s.rg()[j] * inv > s.u2()[j];
+    const cplx t = cmulcj(d, w);   // Delta * conj(w)
+    s.coef()[par] = accept ? cmk(-t.x * inv, -t.y * inv) : cmk(0.0, 0.0);
+    s.accf()[j] = accept ? 1 : 0;
+}
+
+// Stage row/column j (wrapped for the right sweep) from this thread's tile.
+template <int NMAX, bool LEFT, int TR, int TC>
+DEVI void metro_stage(Smem<NMAX>& s, const cplx (&g)[TR][TC], int r0, int c0, int n, int j, int par) {
+    const bool hasrow = (j >= r0) && (j < r0 + TR);
+    const bool hascol = (j >= c0) && (j < c0 + TC);
+    if (!hasrow && !hascol) return;
+#pragma unroll
+    for (int a = 0; a < TR; ++a) {
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+            const int r = r0 + a, c = c0 + b;
+            if (r < n && c < n && (r == j || c == j)) {
+                cplx v = g[a][b];
+                if (!LEFT) {
+                    if (r == j) v = cmul(v, s.eao()[j]);
+                    if (c == j) v = cmul(v, s.ebo()[j]);
+                }
+                if (c == j) s.col(par)[r] = v;
+                if (r == j) s.row(par)[c] = v;
+                if (r == j && c == j) metro_decide(s, j, v, par);
+            }
+        }
+    }
+}
+
 template <int NMAX, bool LEFT>
-DEVI void prop_channel(Ctx<NMAX>& x, int ch, int slice) {
+COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
     const int n = x.n, tid = threadIdx.x;
-    const double ar = x.P.alpha_re[ch], ai = x.P.alpha_im[ch];
-    const double shift = fabs(x.P.shiftLoc);
-    const uint32_t s0 = *s.seed;
+    const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
+    const double shift = fabs(x.P().shiftLoc);
+    const uint32_t s0 = *s.seed();
     double* phis = x.phi + (long)slice * n * 2;
 
     // per-site proposals; draw order follows the visiting order of the sites
@@ -124,138 +170,122 @@ DEVI void prop_channel(Ctx<NMAX>& x, int ch, int slice) {
         const double pn = po + xdif;
         const double go = exp(-0.5 * po * po), gn = exp(-0.5 * pn * pn);
         const cplx eo = cexpz(cmk(ar * po, ai * po)), en = cexpz(cmk(ar * pn, ai * pn));
-        s.eao[i] = eo;
-        s.ean[i] = en;
-        s.ebo[i] = cexpz(cmk(-(ar * po), -(ai * po)));
-        s.ebn[i] = cexpz(cmk(-(ar * pn), -(ai * pn)));
-        s.delta[i] = csub(cdiv(en, eo), cmk(1.0, 0.0));
-        s.rg[i] = gn / go;
-        s.u2[i] = rnd;
-        s.phin[i] = pn;
-        s.accf[i] = 0;
+        s.eao()[i] = eo;
+        s.ean()[i] = en;
+        s.ebo()[i] = cexpz(cmk(-(ar * po), -(ai * po)));
+        s.ebn()[i] = cexpz(cmk(-(ar * pn), -(ai * pn)));
+        s.delta()[i] = csub(cdiv(en, eo), cmk(1.0, 0.0));
+        s.rg()[i] = gn / go;
+        s.u2()[i] = rnd;
+        s.phin()[i] = pn;
+        s.accf()[i] = 0;
     }
     __syncthreads();
 
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const bool act = tid < ncg * nrg;
-    const int r0 = act ? (tid / ncg) * TR : 0, c0 = act ? (tid % ncg) * TC : 0;
+    const int r0 = act ? (tid / ncg) * TR : 4 * NMAX, c0 = act ? (tid % ncg) * TC : 4 * NMAX;
     cplx g[TR][TC];
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
         for (int b = 0; b < TC; ++b) {
             const int r = r0 + a, c = c0 + b;
-            g[a][b] = (act && r < n && c < n) ? s.G[r * n + c] : cmk(0.0, 0.0);
+            g[a][b] = (r < n && c < n) ? s.G()[r * n + c] : cmk(0.0, 0.0);
         }
 
-    auto decide = [&](int j, cplx gjj, int par) {
-        // ratio_det = 1/(1 + Delta (1 - G_jj)); p = |r_gauss * ratio_det * conj(ratio_det)|
-        const cplx w = cadd(cmk(1.0, 0.0), cmul(s.delta[j], csub(cmk(1.0, 0.0), gjj)));
-        const cplx rdet = cdiv(cmk(1.0, 0.0), w);
-        const cplx prod = cmul(cmul(cmk(s.rg[j], 0.0), rdet), cconj(rdet));
-        const double ratio_abs = hypot(prod.x, prod.y);
-        const bool accept = ratio_abs > s.u2[j];
-        const cplx ta = cmul(rdet, s.delta[j]);
-        s.coef[par] = accept ? cmk(-ta.x, -ta.y) : cmk(0.0, 0.0);
-        s.accf[j] = accept ? 1 : 0;
-    };
-    // stage row/column of the next site j (and decide on it) from the current registers
-    auto stage = [&](int j, int par) {
-        if (!act) return;
-#pragma unroll
-        for (int a = 0; a < TR; ++a)
-#pragma unroll
-            for (int b = 0; b < TC; ++b) {
-                const int r = r0 + a, c = c0 + b;
-                if (r >= n || c >= n) continue;
-                if (r != j && c != j) continue;
-                cplx v = g[a][b];
-                if (!LEFT) {   // right sweep wraps site j with its current field before the update
-                    if (r == j) v = cmul(v, s.eao[j]);
-                    if (c == j) v = cmul(v, s.ebo[j]);
-                }
-                if (c == j) s.col[par][r] = v;
-                if (r == j) s.row[par][c] = v;
-                if (r == j && c == j) decide(j, v, par);
-            }
-    };
-
-    stage(LEFT ? n - 1 : 0, 0);
+    metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, n, LEFT ? n - 1 : 0, 0);
     __syncthreads();
     for (int k = 0; k < n; ++k) {
         const int i = LEFT ? n - 1 - k : k;
         const int par = k & 1;
         if (act) {
-            const cplx coef = s.coef[par];
-            const int acc = s.accf[i];
+            const cplx coef = s.coef()[par];
+            const int acc = s.accf()[i];
             cplx cr[TR];
 #pragma unroll
             for (int a = 0; a < TR; ++a) {
                 const int r = r0 + a;
-                cr[a] = (r < n) ? cmul(coef, s.col[par][r]) : cmk(0.0, 0.0);
+                cr[a] = (r < n) ? cmul(coef, s.col(par)[r]) : cmk(0.0, 0.0);
             }
 #pragma unroll
             for (int b = 0; b < TC; ++b) {
                 const int c = c0 + b;
-                if (c >= n) continue;
-                const cplx rv = s.row[par][c];
-                const cplx y = (c == i) ? cmk(1.0 - rv.x, -rv.y) : cmk(-rv.x, -rv.y);
+                const cplx rv = (c < n) ? s.row(par)[c] : cmk(0.0, 0.0);
+                const cplx y = cmk(((c == i) ? 1.0 : 0.0) - rv.x, -rv.y);
 #pragma unroll
                 for (int a = 0; a < TR; ++a) {
                     const int r = r0 + a;
-                    if (r >= n) continue;
                     cplx v = g[a][b];
                     if (!LEFT) {
-                        if (r == i) v = cmul(v, s.eao[i]);
-                        if (c == i) v = cmul(v, s.ebo[i]);
+                        if (r == i) v = cmul(v, s.eao()[i]);
+                        if (c == i) v = cmul(v, s.ebo()[i]);
                     }
                     v = cfma(cr[a], y, v);
                     if (LEFT) {
-                        if (c == i) v = cmul(v, acc ? s.ean[i] : s.eao[i]);
-                        if (r == i) v = cmul(v, acc ? s.ebn[i] : s.ebo[i]);
+                        if (c == i) v = cmul(v, acc ? s.ean()[i] : s.eao()[i]);
+                        if (r == i) v = cmul(v, acc ? s.ebn()[i] : s.ebo()[i]);
                     }
                     g[a][b] = v;
                 }
             }
+            if (k + 1 < n) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, n, LEFT ? n - 2 - k : k + 1, par ^ 1);
         }
-        if (k + 1 < n) stage(LEFT ? n - 2 - k : k + 1, par ^ 1);
         __syncthreads();
     }
-    if (act) {
 #pragma unroll
-        for (int a = 0; a < TR; ++a)
+    for (int a = 0; a < TR; ++a)
 #pragma unroll
-            for (int b = 0; b < TC; ++b) {
-                const int r = r0 + a, c = c0 + b;
-                if (r < n && c < n) s.G[r * n + c] = g[a][b];
-            }
-    }
+        for (int b = 0; b < TC; ++b) {
+            const int r = r0 + a, c = c0 + b;
+            if (r < n && c < n) s.G()[r * n + c] = g[a][b];
+        }
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
-        if (s.accf[i]) phis[i * 2 + ch] = s.phin[i];
+        if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
     if (tid == 0) {
         long long na = 0;
-        for (int i = 0; i < n; ++i) na += s.accf[i];
+        for (int i = 0; i < n; ++i) na += s.accf()[i];
         x.sc->nacc[ch] += na;
         x.sc->nc[ch] += n;
-        *s.seed = lcg_mul(c_apow[2 * n], s0);
+        *s.seed() = lcg_mul(c_apow[2 * n], s0);
     }
     for (int e = tid; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e % n;
         const int site = LEFT ? c : r;
-        s.U[e] = cmul(s.U[e], s.accf[site] ? s.ean[site] : s.eao[site]);
+        s.U()[e] = cmul(s.U()[e], s.accf()[site] ? s.ean()[site] : s.eao()[site]);
     }
     __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
+// propT_L / propT_R (multiply.f90:72-86): G <- e^{+dK} G e^{-dK}, U_L <- U_L e^{-dK}
+// for the left traversal; G <- e^{-dK} G e^{+dK}, U_R <- e^{-dK} U_R for the
+// right.  e^{-dtau K} is in W1, e^{+dtau K} in W2.
+template <int NMAX, bool LEFT>
+COLD void slice_products(Ctx<NMAX> x) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    auto& s = x.s;
+    const int n = x.n;
+    if (LEFT) {
+        gemm_smem<TR, TC>(n, s.G(), s.G(), s.W1());
+        gemm_smem<TR, TC>(n, s.G(), s.W2(), s.G());
+        gemm_smem<TR, TC>(n, s.U(), s.U(), s.W1());
+    } else {
+        gemm_smem<TR, TC>(n, s.G(), s.W1(), s.G());
+        gemm_smem<TR, TC>(n, s.G(), s.G(), s.W2());
+        gemm_smem<TR, TC>(n, s.U(), s.W1(), s.U());
+    }
+}
+
+// ---------------------------------------------------------------------------
 // equal-time estimators (Obs_equal_calc, obser_equal.f90:95-198)
 template <int NMAX>
-DEVI void measure(Ctx<NMAX>& x) {
+COLD void measure(Ctx<NMAX> x) {
     auto& s = x.s;
     const int n = x.n, tid = threadIdx.x;
-    const double lq = (double)x.P.Lq, lq2 = lq * lq;
-    const cplx* G = s.G;
+    const double lq = (double)x.P().Lq, lq2 = lq * lq;
+    const cplx* G = s.G();
     double v[24];
 #pragma unroll
     for (int k = 0; k < 24; ++k) v[k] = 0.0;
@@ -281,8 +311,8 @@ DEVI void measure(Ctx<NMAX>& x) {
         v[11] += tdo.y / lq;
         v[12] += tud.x / lq;
         v[13] += tud.y / lq;
-        if (x.P.hasK) {
-            const cplx ph = x.P.phaseK[i * n + j];
+        if (x.P().hasK) {
+            const cplx ph = x.P().phaseK[i * n + j];
             const cplx sf = cmul(ph, cadd(gc, cconj(gc)));
             const cplx dw = cmul(ph, cadd(cadd(tup, tdo), cadd(tud, cmul(ddi, duj))));
             v[4] += sf.x / lq2;
@@ -292,10 +322,10 @@ DEVI void measure(Ctx<NMAX>& x) {
         }
     }
     for (int e = tid; e < 3 * n; e += blockDim.x) {
-        const int i = e / 3, jj = x.P.bonds[e];
+        const int i = e / 3, jj = x.P().bonds[e];
         cplx gij = G[jj * n + i], gji = G[i * n + jj];   // Grupc(i,jj), Grupc(jj,i)
         if (i == jj) { gij.x -= 1.0; gji.x -= 1.0; }
-        v[14] += x.P.RT * (gij.x + gji.x + gij.x + gji.x) / lq;
+        v[14] += x.P().RT * (gij.x + gji.x + gij.x + gji.x) / lq;
     }
     for (int i = tid; i < n; i += blockDim.x) {
         const cplx du = cmk(G[i * n + i].x - 1.0, G[i * n + i].y), dd = cconj(du);
@@ -310,11 +340,11 @@ DEVI void measure(Ctx<NMAX>& x) {
         v[21] += dens / lq;
         v[22] += 2.0 * cmul(du, du).x + du.x;
         v[23] += 2.0 * cmul(dd, dd).x + dd.x;
-        s.obs[O_SITE + i] += dens;
+        s.obs()[O_SITE + i] += dens;
     }
-    block_sum<24>(v, s.red);
+    block_sum<24>(v, s.red());
     if (tid == 0) {
-        double* o = s.obs;
+        double* o = s.obs();
         o[O_NUMSQUARE_UP] += v[0];
         o[O_NUMSQUARE_DO] += v[1];
         o[O_PSF_GAMMA] += v[2];
@@ -339,7 +369,7 @@ DEVI void measure(Ctx<NMAX>& x) {
         o[O_DENSITY_TOTAL] += v[21];
         o[O_ONSITE_N2_UP] += v[22];
         o[O_ONSITE_N2_DO] += v[23];
-        const double inter = (x.P.U1 + x.P.U2) * (v[22] + v[23]) / lq + 2.0 * (x.P.U2 - x.P.U1) * v[17];
+        const double inter = (x.P().U1 + x.P().U2) * (v[22] + v[23]) / lq + 2.0 * (x.P().U2 - x.P().U1) * v[17];
         o[O_KINETIC] += kin;
         o[O_INTERACTION] += inter;
         o[O_ENERGY] += kin + inter;
@@ -352,81 +382,81 @@ DEVI void measure(Ctx<NMAX>& x) {
 // stabilisation (stabilization.f90:69-190)
 
 // stab_UR: (U_R D_R) P = Q R;  D_R <- |diag R|;  V_R <- R P^T V_R;  U_R <- Q.
-// U_R is s.U; on exit the new V_R is in s.W2 and in A.VRc, D_R in A.DRc.
+// U_R is s.U(); on exit the new V_R is in s.W2() and in A.VRc, D_R in A.DRc.
 template <int NMAX>
-DEVI void stab_UR(Ctx<NMAX>& x) {
+COLD void stab_UR(Ctx<NMAX> x) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
     const int n = x.n;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W1[e] = cmul(s.U[e], x.A.DRc[e % n]);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W1()[e] = cmul(s.U()[e], x.A().DRc[e % n]);
     __syncthreads();
-    qrp_inplace(n, s.W1, s.qr());
-    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A.DRc[i] = cmk(s.d[i], 0.0);
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2[e] = x.A.VRc[s.piv[e / n] * n + e % n];
+    qrp_inplace(n, s.W1(), s.qr());
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DRc[i] = cmk(s.d()[i], 0.0);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VRc[s.piv()[e / n] * n + e % n];
     __syncthreads();
-    gemm_rs<TR, TC>(n, s.W2, op_n(s.W1, n), op_n(s.W2, n), TRI_A_UPPER);
-    form_q(n, s.W1, s.tau, s.U, false);
-    gcopy(x.A.VRc, s.W2, n * n);
+    gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), op_n(s.W2(), n), TRI_A_UPPER);
+    form_q<Cfg<NMAX>::MAXE>(n, s.W1(), s.tau(), s.U(), false);
+    gcopy(x.A().VRc, s.W2(), n * n);
     __syncthreads();
 }
 
 // stab_UL: (U_L^H D_L) P = Q R;  D_L <- |diag R|;  V_L <- V_L P R^H;  U_L <- Q^H.
 template <int NMAX>
-DEVI void stab_UL(Ctx<NMAX>& x) {
+COLD void stab_UL(Ctx<NMAX> x) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e % n;
-        s.W1[e] = cmul(cconj(s.U[c * n + r]), x.A.DLc[c]);
+        s.W1()[e] = cmul(cconj(s.U()[c * n + r]), x.A().DLc[c]);
     }
     __syncthreads();
-    qrp_inplace(n, s.W1, s.qr());
-    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A.DLc[i] = cmk(s.d[i], 0.0);
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2[e] = x.A.VLc[(e / n) * n + s.piv[e % n]];
+    qrp_inplace(n, s.W1(), s.qr());
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DLc[i] = cmk(s.d()[i], 0.0);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VLc[(e / n) * n + s.piv()[e % n]];
     __syncthreads();
-    gemm_rs<TR, TC>(n, s.W2, op_n(s.W2, n), op_c(s.W1, n), TRI_B_LOWER_FROM_C);
-    form_q(n, s.W1, s.tau, s.U, true);
-    gcopy(x.A.VLc, s.W2, n * n);
+    gemm_rs<TR, TC>(n, s.W2(), op_n(s.W2(), n), op_c(s.W1(), n), TRI_B_LOWER_FROM_C);
+    form_q<Cfg<NMAX>::MAXE>(n, s.W1(), s.tau(), s.U(), true);
+    gcopy(x.A().VLc, s.W2(), n * n);
     __syncthreads();
 }
 
 // M = U_R^H U_L^H - D_R V_R V_L D_L is in W2 (W1 free); finish stab_green:
 // factor M (or M^H for nt > L/2) and write G = (I - B)^{-1} into W2.
 template <int NMAX>
-DEVI void green_from_M(Ctx<NMAX>& x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
+COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
-    const int n = x.n, L = x.P.L;
-    if (nt > L / 2) conj_transpose_inplace(n, s.W2);
-    qrp_inplace(n, s.W2, s.qr());
+    const int n = x.n, L = x.P().L;
+    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, s.W2());
+    qrp_inplace(n, s.W2(), s.qr());
     if (nt < L / 2 + 1) {
-        copy_op(n, s.W1, URh);
-        apply_qh_left(n, s.W2, s.tau, s.W1);
+        copy_op(n, s.W1(), URh);
+        apply_qh_left(n, s.W2(), s.tau(), s.W1());
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const double dd = s.d[e / n];
-            s.W1[e] = cmk(s.W1[e].x / dd, s.W1[e].y / dd);
+            const double dd = s.d()[e / n];
+            s.W1()[e] = cmk(s.W1()[e].x / dd, s.W1()[e].y / dd);
         }
         __syncthreads();
-        trsm_left_upper(n, s.W2, s.W1);
-        permute_rows(n, s.W1, s.piv, s.ipiv, false);
-        gemm_rs<TR, TC>(n, s.W2, ULh, op_n(s.W1, n));
+        trsm_left_upper(n, s.W2(), s.W1());
+        permute_rows<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, s.W2(), ULh, op_n(s.W1(), n));
     } else {
-        copy_op(n, s.W1, ULh);
-        apply_q_right(n, s.W2, s.tau, s.W1);
+        copy_op(n, s.W1(), ULh);
+        apply_q_right(n, s.W2(), s.tau(), s.W1());
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const double dd = s.d[e % n];
-            s.W1[e] = cmk(s.W1[e].x / dd, s.W1[e].y / dd);
+            const double dd = s.d()[e % n];
+            s.W1()[e] = cmk(s.W1()[e].x / dd, s.W1()[e].y / dd);
         }
         __syncthreads();
-        trsm_right_upperH(n, s.W2, s.W1);
-        permute_cols(n, s.W1, s.piv, s.ipiv, false);
-        gemm_rs<TR, TC>(n, s.W2, op_n(s.W1, n), URh);
+        trsm_right_upperH(n, s.W2(), s.W1());
+        permute_cols<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), URh);
     }
     if (want_logdet) {
         double v[1] = {0.0};
-        for (int i = threadIdx.x; i < n; i += blockDim.x) v[0] += log(s.d[i]);
-        block_sum<1>(v, s.red);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) v[0] += log(s.d()[i]);
+        block_sum<1>(v, s.red());
         if (threadIdx.x == 0) x.sc->logdetM = v[0];
     }
 }
@@ -438,8 +468,8 @@ DEVI void form_M(Ctx<NMAX>& x) {
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e % n;
-        const cplx t = cmul(x.A.DLc[c], s.W1[e]);
-        s.W2[e] = csub(s.W2[e], cmul(x.A.DRc[r], t));
+        const cplx t = cmul(x.A().DLc[c], s.W1()[e]);
+        s.W2()[e] = csub(s.W2()[e], cmul(x.A().DRc[r], t));
     }
     __syncthreads();
 }
@@ -450,94 +480,94 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
     auto& s = x.s;
     const int n = x.n;
     double v[1] = {0.0};
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) v[0] += cabsv(csub(s.W2[e], s.G[e]));
-    block_sum<1>(v, s.red);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) v[0] += cabsv(csub(s.W2()[e], s.G()[e]));
+    block_sum<1>(v, s.red());
     if (threadIdx.x == 0) {
         const double dif = v[0];
         if (dif > x.sc->xmax) x.sc->xmax = dif;
         x.sc->xmean += dif;
         if (!(dif == dif) || dif > 1.0e300) x.sc->status |= 1;
     }
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.G[e] = s.W2[e];
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.G()[e] = s.W2()[e];
     __syncthreads();
 }
 
 // stab_green with the right side factored in shared memory (U = U_R, W2 = V_R)
 // and the left side in HBM (A.ULc, A.VLc, A.DLc).
 template <int NMAX>
-DEVI void stab_green_right_local(Ctx<NMAX>& x, int nt, bool want_logdet) {
+COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, s.W1, op_n(s.W2, n), op_n(x.A.VLc, n));        // V_R V_L
-    gemm_rs<TR, TC>(n, s.W2, op_c(s.U, n), op_c(x.A.ULc, n));         // U_R^H U_L^H
+    gemm_rs<TR, TC>(n, s.W1(), op_n(s.W2(), n), op_n(x.A().VLc, n));        // V_R V_L
+    gemm_rs<TR, TC>(n, s.W2(), op_c(s.U(), n), op_c(x.A().ULc, n));         // U_R^H U_L^H
     form_M(x);
-    green_from_M(x, nt, op_c(s.U, n), op_c(x.A.ULc, n), want_logdet);
+    green_from_M(x, nt, op_c(s.U(), n), op_c(x.A().ULc, n), want_logdet);
 }
 
 // stab_green with the left side in shared memory (U = U_L, W2 = V_L) and the
 // right side in HBM.
 template <int NMAX>
-DEVI void stab_green_left_local(Ctx<NMAX>& x, int nt) {
+COLD void stab_green_left_local(Ctx<NMAX> x, int nt) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, s.W1, op_n(x.A.VRc, n), op_n(s.W2, n));
-    gemm_rs<TR, TC>(n, s.W2, op_c(x.A.URc, n), op_c(s.U, n));
+    gemm_rs<TR, TC>(n, s.W1(), op_n(x.A().VRc, n), op_n(s.W2(), n));
+    gemm_rs<TR, TC>(n, s.W2(), op_c(x.A().URc, n), op_c(s.U(), n));
     form_M(x);
-    green_from_M(x, nt, op_c(x.A.URc, n), op_c(s.U, n), false);
+    green_from_M(x, nt, op_c(x.A().URc, n), op_c(s.U(), n), false);
 }
 
 // Wrap_L (stabilization.f90:301-331)
 template <int NMAX>
-DEVI void wrap_L(Ctx<NMAX>& x, int nt) {
+COLD void wrap_L(Ctx<NMAX> x, int nt) {
     auto& s = x.s;
-    const int n = x.n, st = nt / x.P.Nwrap;
-    gcopy(x.A.URc, x.A.URs(st), n * n);
-    gcopy(x.A.VRc, x.A.VRs(st), n * n);
-    gcopy(x.A.DRc, x.A.DRs(st), n);
+    const int n = x.n, st = nt / x.P().Nwrap;
+    gcopy(x.A().URc, x.A().URs(st), n * n);
+    gcopy(x.A().VRc, x.A().VRs(st), n * n);
+    gcopy(x.A().DRc, x.A().DRs(st), n);
     __syncthreads();
-    if (nt != x.P.L) {
+    if (nt != x.P().L) {
         stab_UL(x);
         stab_green_left_local(x, nt);
         drift_and_replace(x);
     }
-    gcopy(x.A.ULs(st), s.U, n * n);
-    gcopy(x.A.VLs(st), x.A.VLc, n * n);
-    gcopy(x.A.DLs(st), x.A.DLc, n);
+    gcopy(x.A().ULs(st), s.U(), n * n);
+    gcopy(x.A().VLs(st), x.A().VLc, n * n);
+    gcopy(x.A().DLs(st), x.A().DLc, n);
     __syncthreads();
     load_expT(x);
 }
 
 // Wrap_R (stabilization.f90:333-366)
 template <int NMAX>
-DEVI void wrap_R(Ctx<NMAX>& x, int nt) {
+COLD void wrap_R(Ctx<NMAX> x, int nt) {
     auto& s = x.s;
-    const int n = x.n, st = nt / x.P.Nwrap;
-    gcopy(x.A.ULc, x.A.ULs(st), n * n);
-    gcopy(x.A.VLc, x.A.VLs(st), n * n);
-    gcopy(x.A.DLc, x.A.DLs(st), n);
+    const int n = x.n, st = nt / x.P().Nwrap;
+    gcopy(x.A().ULc, x.A().ULs(st), n * n);
+    gcopy(x.A().VLc, x.A().VLs(st), n * n);
+    gcopy(x.A().DLc, x.A().DLs(st), n);
     __syncthreads();
     if (nt != 0) {
         stab_UR(x);
-        stab_green_right_local(x, nt, nt == x.P.L);
+        stab_green_right_local(x, nt, nt == x.P().L);
         drift_and_replace(x);
     }
-    gcopy(x.A.URs(st), s.U, n * n);
-    gcopy(x.A.VRs(st), x.A.VRc, n * n);
-    gcopy(x.A.DRs(st), x.A.DRc, n);
+    gcopy(x.A().URs(st), s.U(), n * n);
+    gcopy(x.A().VRs(st), x.A().VRc, n * n);
+    gcopy(x.A().DRs(st), x.A().DRc, n);
     __syncthreads();
     load_expT(x);
 }
 
 // ---------------------------------------------------------------------------
 template <int NMAX>
-DEVI bool setup_ctx(Ctx<NMAX>& x, unsigned char* smem, const KernelArgs& ka, int chain) {
-    x.s.carve(smem);
+DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     const ChainDev cd = ka.chains[chain];
-    x.P = ka.pts[cd.point];
-    x.n = x.P.N;
-    x.A = make_arena(ka.arena + cd.arena_off, x.n);
+    if (threadIdx.x == 0) *x.s.P() = ka.pts[cd.point];
+    __syncthreads();
+    x.n = x.P().N;
+    x.abase = ka.arena + cd.arena_off;
     x.phi = ka.phi + cd.phi_off;
     x.sc = ka.sc + chain;
     return x.n <= NMAX;
@@ -545,119 +575,139 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, unsigned char* smem, const KernelArgs& ka, int
 
 template <int NMAX>
 DEVI void load_obs(Ctx<NMAX>& x) {
-    for (int k = threadIdx.x; k < kObsScalars + NMAX; k += blockDim.x) x.s.obs[k] = 0.0;
+    for (int k = threadIdx.x; k < kObsScalars + NMAX; k += blockDim.x) x.s.obs()[k] = 0.0;
 }
 template <int NMAX>
 DEVI void flush_obs(Ctx<NMAX>& x, double* gobs) {
-    for (int k = threadIdx.x; k < kObsScalars + x.P.Lq; k += blockDim.x) gobs[k] += x.s.obs[k];
+    for (int k = threadIdx.x; k < kObsScalars + x.P().Lq; k += blockDim.x) gobs[k] += x.s.obs()[k];
 }
 
 // one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
 template <int NMAX>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS) sweep_kernel(KernelArgs ka, const int* idx, int count) {
-    extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
-    if (!setup_ctx(x, smem, ka, chain)) return;
+    if (!setup_ctx(x, ka, chain)) return;
     auto& s = x.s;
-    const int n = x.n, L = x.P.L;
-    if (threadIdx.x == 0) *s.seed = x.sc->seed;
+    const int n = x.n, L = x.P().L;
+    const bool tm = ka.timers && threadIdx.x == 0;
+    long long tk = tm ? clock64() : 0;
+#define lap(ph)                                      \
+    do {                                             \
+        if (tm) {                                    \
+            const long long t_ = clock64();          \
+            x.sc->cyc[ph] += t_ - tk;                \
+            tk = t_;                                 \
+        }                                            \
+    } while (0)
+    if (threadIdx.x == 0) *s.seed() = x.sc->seed;
     load_obs(x);
-    gcopy(s.G, x.A.G, n * n);
-    gcopy(s.U, x.A.ULc, n * n);
+    gcopy(s.G(), x.A().G, n * n);
+    gcopy(s.U(), x.A().ULc, n * n);
     __syncthreads();
     load_expT(x);
+    lap(3);
     // ---- left traversal
     for (int nt = L; nt >= 1; --nt) {
-        if (nt % x.P.Nwrap == 0) wrap_L(x, nt);
+        if (nt % x.P().Nwrap == 0) {
+            wrap_L(x, nt);
+            lap(3);
+        }
         measure(x);
-        gemm_rs<TR, TC>(n, s.G, op_n(s.G, n), op_n(s.W1, n));   // G e^{-dtau K}
-        gemm_rs<TR, TC>(n, s.G, op_n(s.W2, n), op_n(s.G, n));   // e^{+dtau K} G
-        gemm_rs<TR, TC>(n, s.U, op_n(s.U, n), op_n(s.W1, n));   // U_L e^{-dtau K}
-        if (x.P.active[1]) prop_channel<NMAX, true>(x, 1, nt - 1);
-        if (x.P.active[0]) prop_channel<NMAX, true>(x, 0, nt - 1);
+        lap(2);
+        slice_products<NMAX, true>(x);
+        lap(1);
+        if (x.P().active[1]) prop_channel<NMAX, true>(x, 1, nt - 1);
+        if (x.P().active[0]) prop_channel<NMAX, true>(x, 0, nt - 1);
+        lap(0);
     }
     wrap_L(x, 0);
-    gcopy(x.A.ULc, s.U, n * n);
+    gcopy(x.A().ULc, s.U(), n * n);
     __syncthreads();
     // ---- right traversal
-    gcopy(s.U, x.A.URc, n * n);
+    gcopy(s.U(), x.A().URc, n * n);
     __syncthreads();
     wrap_R(x, 0);
+    lap(3);
     for (int nt = 1; nt <= L; ++nt) {
-        if (x.P.active[0]) prop_channel<NMAX, false>(x, 0, nt - 1);
-        if (x.P.active[1]) prop_channel<NMAX, false>(x, 1, nt - 1);
-        gemm_rs<TR, TC>(n, s.G, op_n(s.W1, n), op_n(s.G, n));   // e^{-dtau K} G
-        gemm_rs<TR, TC>(n, s.G, op_n(s.G, n), op_n(s.W2, n));   // G e^{+dtau K}
-        gemm_rs<TR, TC>(n, s.U, op_n(s.W1, n), op_n(s.U, n));   // e^{-dtau K} U_R
-        if (nt % x.P.Nwrap == 0) wrap_R(x, nt);
+        if (x.P().active[0]) prop_channel<NMAX, false>(x, 0, nt - 1);
+        if (x.P().active[1]) prop_channel<NMAX, false>(x, 1, nt - 1);
+        lap(0);
+        slice_products<NMAX, false>(x);
+        lap(1);
+        if (nt % x.P().Nwrap == 0) {
+            wrap_R(x, nt);
+            lap(3);
+        }
         measure(x);
+        lap(2);
     }
-    gcopy(x.A.URc, s.U, n * n);
-    gcopy(x.A.G, s.G, n * n);
+    gcopy(x.A().URc, s.U(), n * n);
+    gcopy(x.A().G, s.G(), n * n);
     flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
-    if (threadIdx.x == 0) x.sc->seed = *s.seed;
+    if (threadIdx.x == 0) x.sc->seed = *s.seed();
+    lap(3);
+#undef lap
 }
 
 // Local_sweep_pre (local_sweep.f90:80-94) with Prop_make's identities
 // (process_matrix.f90:37-47).
 template <int NMAX>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS) pre_kernel(KernelArgs ka, const int* idx, int count) {
-    extern __shared__ __align__(16) unsigned char smem[];
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
-    if (!setup_ctx(x, smem, ka, chain)) return;
+    if (!setup_ctx(x, ka, chain)) return;
     auto& s = x.s;
-    const int n = x.n, L = x.P.L;
-    set_identity(n, s.U);
-    set_identity(n, s.G);
-    set_identity(n, x.A.VRc);
-    set_identity(n, x.A.ULc);
-    set_identity(n, x.A.VLc);
+    const int n = x.n, L = x.P().L;
+    set_identity(n, s.U());
+    set_identity(n, s.G());
+    set_identity(n, x.A().VRc);
+    set_identity(n, x.A().ULc);
+    set_identity(n, x.A().VLc);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        x.A.DRc[i] = cmk(1.0, 0.0);
-        x.A.DLc[i] = cmk(1.0, 0.0);
+        x.A().DRc[i] = cmk(1.0, 0.0);
+        x.A().DLc[i] = cmk(1.0, 0.0);
     }
     __syncthreads();
-    gcopy(x.A.URs(0), s.U, n * n);
-    gcopy(x.A.VRs(0), x.A.VRc, n * n);
-    gcopy(x.A.DRs(0), x.A.DRc, n);
-    gcopy(s.W1, x.P.expP, n * n);
+    gcopy(x.A().URs(0), s.U(), n * n);
+    gcopy(x.A().VRs(0), x.A().VRc, n * n);
+    gcopy(x.A().DRs(0), x.A().DRc, n);
+    gcopy(s.W1(), x.P().expP, n * n);
     __syncthreads();
     for (int nt = 1; nt <= L; ++nt) {
         const double* ph = x.phi + (long)(nt - 1) * n * 2;
         for (int ch = 0; ch < 2; ++ch) {
-            if (!x.P.active[ch]) continue;
-            const double ar = x.P.alpha_re[ch], ai = x.P.alpha_im[ch];
+            if (!x.P().active[ch]) continue;
+            const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
             for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
                 const double p = ph[(e / n) * 2 + ch];
-                s.U[e] = cmul(cexpz(cmk(ar * p, ai * p)), s.U[e]);
+                s.U()[e] = cmul(cexpz(cmk(ar * p, ai * p)), s.U()[e]);
             }
             __syncthreads();
         }
-        gemm_rs<TR, TC>(n, s.U, op_n(s.W1, n), op_n(s.U, n));
-        if (nt % x.P.Nwrap == 0) {
-            const int st = nt / x.P.Nwrap;
+        gemm_rs<TR, TC>(n, s.U(), op_n(s.W1(), n), op_n(s.U(), n));
+        if (nt % x.P().Nwrap == 0) {
+            const int st = nt / x.P().Nwrap;
             stab_UR(x);
-            gcopy(x.A.URs(st), s.U, n * n);
-            gcopy(x.A.VRs(st), x.A.VRc, n * n);
-            gcopy(x.A.DRs(st), x.A.DRc, n);
+            gcopy(x.A().URs(st), s.U(), n * n);
+            gcopy(x.A().VRs(st), x.A().VRc, n * n);
+            gcopy(x.A().DRs(st), x.A().DRc, n);
             __syncthreads();
             if (nt == L) {
                 stab_green_right_local(x, nt, true);
-                gcopy(s.G, s.W2, n * n);
+                gcopy(s.G(), s.W2(), n * n);
                 __syncthreads();
             }
-            gcopy(s.W1, x.P.expP, n * n);
+            gcopy(s.W1(), x.P().expP, n * n);
             __syncthreads();
         }
     }
-    gcopy(x.A.URc, s.U, n * n);
-    gcopy(x.A.G, s.G, n * n);
+    gcopy(x.A().URc, s.U(), n * n);
+    gcopy(x.A().G, s.G(), n * n);
 }
 
 // LocalU_prop_therm / LocalU_metro_therm over the whole field, nwarm sweeps

@@ -145,6 +145,12 @@ class Ensemble:
         _lib.check(self.lib.bafqmc_log_weight(self.h, _dptr(out)))
         return out
 
+    def phase_timers(self, enable: bool = True) -> np.ndarray:
+        """Enable per-phase cycle counting; returns the [nchains, 4] cycles so far."""
+        out = np.zeros((self.nchains, 4))
+        _lib.check(self.lib.bafqmc_phase_timers(self.h, 1 if enable else 0, _dptr(out)))
+        return out
+
     def counters(self) -> np.ndarray:
         out = np.zeros((self.nchains, _lib.COUNTERS))
         _lib.check(self.lib.bafqmc_counters(self.h, _dptr(out)))

@@ -111,6 +111,12 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out);
 #define BAFQMC_COUNTERS 10
 int bafqmc_counters(bafqmc_handle* h, double* out);
 
+/* Per-phase SM cycle counters of the sweep kernel (the reference has only a
+ * total wall time, main.f90:26-27,67-71).  enable switches counting for the
+ * following sweeps; out (optional) receives [nchains][4] accumulated cycles:
+ * local updates, slice products, measurement, wraps/stabilisation. */
+int bafqmc_phase_timers(bafqmc_handle* h, int enable, double* out);
+
 int bafqmc_synchronize(bafqmc_handle* h);
 /* The handle's cudaStream_t, for event timing by the caller. */
 void* bafqmc_stream(bafqmc_handle* h);
