@@ -14,7 +14,7 @@
 
 // Factorisation routines are kept out of line: they run once per wrap, and
 // inlining them into the sweep kernel costs registers on the per-slice path.
-#define COLD __device__ __noinline__
+#define COLD static __device__ __noinline__
 
 // Strided operand view: element (r, c) = p[r*sr + c*sc], optionally conjugated.
 // A transposed view swaps the strides.  p may point to shared or global memory.
