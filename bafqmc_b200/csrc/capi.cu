@@ -151,8 +151,8 @@ struct PointHost {
     bafqmc_point p;
     int N, Lq, Nst;
     double dtau;
-    zmat expP, expM, phaseK;
-    std::vector<int> bonds;
+    zmat expP, expM;
+    std::vector<double> phaseR;   // interleaved complex, Lq entries
     double alpha_re[2], alpha_im[2];
     int active[2];
 };
@@ -187,7 +187,6 @@ struct bafqmc_handle {
     PointDev* d_pts = nullptr;
     ChainDev* d_chains = nullptr;
     double2* d_mats = nullptr;
-    int* d_bonds = nullptr;
     double2* d_arena = nullptr;
     double* d_phi = nullptr;
     double* d_obs = nullptr;
@@ -241,16 +240,14 @@ int setup_point(const bafqmc_point& p, PointHost& out) {
     for (int ii = 0; ii < n; ++ii) H.re(ii, ii) -= p.mu;
     out.expP = expm_scaled(H, -out.dtau);
     out.expM = expm_scaled(H, out.dtau);
-    out.phaseK = zmat(n);
-    if (lat.hasK) {
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) {
-                const double kr = lat.k_dot_r(lat.indexK, lat.imj[(size_t)i * n + j]);
-                out.phaseK.re(i, j) = std::cos(kr);
-                out.phaseK.im(i, j) = std::sin(kr);
-            }
+    out.phaseR.assign(2 * (size_t)out.Lq, 0.0);
+    if (lat.hasK) {   // phaseK = exp(i k_dot_r(indexK, imj)) (obser_equal.f90:157)
+        for (int r = 0; r < out.Lq; ++r) {
+            const double kr = lat.k_dot_r(lat.indexK, r);
+            out.phaseR[2 * r] = std::cos(kr);
+            out.phaseR[2 * r + 1] = std::sin(kr);
+        }
     }
-    out.bonds = lat.bonds;
     const double U[2] = {p.U1, p.U2};
     for (int ch = 0; ch < 2; ++ch) {   // opU_set (operator_Hubbard.f90:36-43)
         out.alpha_re[ch] = 0.0;
@@ -271,7 +268,7 @@ int class_of(int n) {
 void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
-    void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_bonds, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
+    void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
                     h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_cls[0], h->d_cls[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -342,32 +339,24 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         v = (v * 48828125ull) & 0x7fffffffull;
     }
     if ((e = bq::upload_pow_table(apow.data(), bq::kMaxPow)) != cudaSuccess) return bail(e, "upload_pow_table");
-    // point matrices: expP, expM, phaseK per point
+    // point matrices: expP, expM (N*N each) and the K phase table (Lq) per point
     size_t mat_total = 0;
-    std::vector<size_t> mat_off(npts), bond_off(npts);
-    size_t bond_total = 0;
+    std::vector<size_t> mat_off(npts);
     for (int i = 0; i < npts; ++i) {
         mat_off[i] = mat_total;
-        mat_total += 3 * (size_t)h->pts[i].N * h->pts[i].N;
-        bond_off[i] = bond_total;
-        bond_total += 3 * (size_t)h->pts[i].N;
+        mat_total += 2 * (size_t)h->pts[i].N * h->pts[i].N + h->pts[i].Lq;
     }
     std::vector<double> mats(2 * mat_total);
-    std::vector<int> bonds(bond_total);
     for (int i = 0; i < npts; ++i) {
         const PointHost& ph = h->pts[i];
         const size_t nn = (size_t)ph.N * ph.N;
         std::memcpy(&mats[2 * mat_off[i]], ph.expP.a.data(), sizeof(double) * 2 * nn);
         std::memcpy(&mats[2 * (mat_off[i] + nn)], ph.expM.a.data(), sizeof(double) * 2 * nn);
-        std::memcpy(&mats[2 * (mat_off[i] + 2 * nn)], ph.phaseK.a.data(), sizeof(double) * 2 * nn);
-        std::memcpy(&bonds[bond_off[i]], ph.bonds.data(), sizeof(int) * 3 * ph.N);
+        std::memcpy(&mats[2 * (mat_off[i] + 2 * nn)], ph.phaseR.data(), sizeof(double) * 2 * ph.Lq);
     }
     if ((e = cudaMalloc(&h->d_mats, sizeof(double2) * mat_total)) != cudaSuccess) return bail(e, "cudaMalloc mats");
-    if ((e = cudaMalloc(&h->d_bonds, sizeof(int) * bond_total)) != cudaSuccess) return bail(e, "cudaMalloc bonds");
     if ((e = cudaMemcpy(h->d_mats, mats.data(), sizeof(double2) * mat_total, cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(e, "upload mats");
-    if ((e = cudaMemcpy(h->d_bonds, bonds.data(), sizeof(int) * bond_total, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return bail(e, "upload bonds");
     std::vector<PointDev> pd(npts);
     for (int i = 0; i < npts; ++i) {
         const PointHost& ph = h->pts[i];
@@ -379,6 +368,8 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         d.Nst = ph.Nst;
         d.Lq = ph.Lq;
         d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
+        d.Lx = ph.p.Lx;
+        d.Ly = ph.p.Ly;
         for (int ch = 0; ch < 2; ++ch) {
             d.active[ch] = ph.active[ch];
             d.alpha_re[ch] = ph.alpha_re[ch];
@@ -390,8 +381,7 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         d.RT = 1.0;
         d.expP = h->d_mats + mat_off[i];
         d.expM = h->d_mats + mat_off[i] + nn;
-        d.phaseK = h->d_mats + mat_off[i] + 2 * nn;
-        d.bonds = h->d_bonds + bond_off[i];
+        d.phaseR = h->d_mats + mat_off[i] + 2 * nn;
     }
     std::vector<ChainDev> cd(nchains);
     for (int c = 0; c < nchains; ++c) {

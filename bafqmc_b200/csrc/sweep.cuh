@@ -32,14 +32,13 @@ enum ObsIndex {
 constexpr int kObsScalars = 26;
 
 struct PointDev {
-    int N, L, Nwrap, Nst, Lq, hasK;
+    int N, L, Nwrap, Nst, Lq, hasK, Lx, Ly;
     int active[2];
     double alpha_re[2], alpha_im[2];
     double shiftLoc, U1, U2, RT;
     const cplx* expP;      // e^{-dtau K}, N*N row-major
     const cplx* expM;      // e^{+dtau K}
-    const cplx* phaseK;    // exp(i K.r_{imj(i,j)}), N*N (only if hasK)
-    const int* bonds;      // N*3: neighbour of site i along bond 1..3 (lattice.f90:98-111)
+    const cplx* phaseR;    // exp(i K.r) for the Lq lattice displacements r (only if hasK)
 };
 
 struct ChainScalars {

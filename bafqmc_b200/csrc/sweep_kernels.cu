@@ -15,7 +15,9 @@ __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 
 template <int NMAX> struct Cfg;
 template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2; };
+static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
 template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6; };
+static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 
 // Dynamic shared memory of the sweep kernels.  Every buffer sits at a
 // compile-time offset, so device code addresses it without holding pointers.
@@ -28,7 +30,7 @@ struct Smem {
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + 2 * VC, oDelta = oRow + 2 * VC;
     static constexpr size_t oEao = oDelta + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
-    static constexpr size_t oCoef = oEbn + VC, oCbc = oCoef + 2 * sizeof(cplx);
+    static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + 2 * sizeof(cplx);
     static constexpr size_t oP = oCbc + 4 * sizeof(cplx);
     static constexpr size_t oRg = oP + ((sizeof(PointDev) + 15) / 16) * 16;
     static constexpr size_t oU2 = oRg + VD, oPhin = oU2 + VD, oVn1 = oPhin + VD, oVn2 = oVn1 + VD, oD = oVn2 + VD;
@@ -52,6 +54,7 @@ struct Smem {
     DEVI cplx* ean() const { return at<cplx>(oEan); }
     DEVI cplx* ebo() const { return at<cplx>(oEbo); }
     DEVI cplx* ebn() const { return at<cplx>(oEbn); }
+    DEVI cplx* ph() const { return at<cplx>(oPh); }
     DEVI cplx* coef() const { return at<cplx>(oCoef); }
     DEVI cplx* cbc() const { return at<cplx>(oCbc); }
     DEVI PointDev* P() const { return at<PointDev>(oP); }
@@ -125,29 +128,34 @@ DEVI void metro_decide(Smem<NMAX>& s, int j, cplx gjj, int par) {
     s.accf()[j] = accept ? 1 : 0;
 }
 
-// Stage row/column j (wrapped for the right sweep) from this thread's tile.
+// Stage row/column j (wrapped with its current field for the right sweep) from
+// this thread's tile; the owner of (j,j) then decides on site j.
 template <int NMAX, bool LEFT, int TR, int TC>
-DEVI void metro_stage(Smem<NMAX>& s, const cplx (&g)[TR][TC], int r0, int c0, int n, int j, int par) {
-    const bool hasrow = (j >= r0) && (j < r0 + TR);
-    const bool hascol = (j >= c0) && (j < c0 + TC);
-    if (!hasrow && !hascol) return;
+DEVI void metro_stage(Smem<NMAX>& s, const cplx (&g)[TR][TC], int r0, int c0, int j, int par) {
+    const bool rowhit = (unsigned)(j - r0) < (unsigned)TR;
+    const bool colhit = (unsigned)(j - c0) < (unsigned)TC;
+    if (!rowhit && !colhit) return;
+    const cplx ea = LEFT ? cmk(1.0, 0.0) : s.eao()[j];
+    const cplx eb = LEFT ? cmk(1.0, 0.0) : s.ebo()[j];
+    cplx vjj = cmk(0.0, 0.0);
 #pragma unroll
     for (int a = 0; a < TR; ++a) {
 #pragma unroll
         for (int b = 0; b < TC; ++b) {
             const int r = r0 + a, c = c0 + b;
-            if (r < n && c < n && (r == j || c == j)) {
+            if (r == j || c == j) {
                 cplx v = g[a][b];
                 if (!LEFT) {
-                    if (r == j) v = cmul(v, s.eao()[j]);
-                    if (c == j) v = cmul(v, s.ebo()[j]);
+                    if (r == j) v = cmul(v, ea);
+                    if (c == j) v = cmul(v, eb);
                 }
                 if (c == j) s.col(par)[r] = v;
                 if (r == j) s.row(par)[c] = v;
-                if (r == j && c == j) metro_decide(s, j, v, par);
+                if (r == j && c == j) vjj = v;
             }
         }
     }
+    if (rowhit && colhit) metro_decide(s, j, vjj, par);
 }
 
 template <int NMAX, bool LEFT>
@@ -182,9 +190,11 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     }
     __syncthreads();
 
+    // thread tile: rows r0..r0+TR-1, columns c0..c0+TC-1 (r0, c0 < NMAX so the
+    // staging vectors are read in bounds; elements outside n x n are never stored)
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const bool act = tid < ncg * nrg;
-    const int r0 = act ? (tid / ncg) * TR : 4 * NMAX, c0 = act ? (tid % ncg) * TC : 4 * NMAX;
+    const int r0 = act ? (tid / ncg) * TR : 0, c0 = act ? (tid % ncg) * TC : 0;
     cplx g[TR][TC];
 #pragma unroll
     for (int a = 0; a < TR; ++a)
@@ -194,42 +204,50 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
             g[a][b] = (r < n && c < n) ? s.G()[r * n + c] : cmk(0.0, 0.0);
         }
 
-    metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, n, LEFT ? n - 1 : 0, 0);
+    if (act) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, LEFT ? n - 1 : 0, 0);
     __syncthreads();
     for (int k = 0; k < n; ++k) {
         const int i = LEFT ? n - 1 - k : k;
         const int par = k & 1;
         if (act) {
-            const cplx coef = s.coef()[par];
-            const int acc = s.accf()[i];
-            cplx cr[TR];
+            const bool rowhit = (unsigned)(i - r0) < (unsigned)TR;
+            const bool colhit = (unsigned)(i - c0) < (unsigned)TC;
+            if (!LEFT && (rowhit || colhit)) {   // right sweep: wrap site i first (row, then column)
+                const cplx ea = s.eao()[i], eb = s.ebo()[i];
 #pragma unroll
-            for (int a = 0; a < TR; ++a) {
-                const int r = r0 + a;
-                cr[a] = (r < n) ? cmul(coef, s.col(par)[r]) : cmk(0.0, 0.0);
+                for (int a = 0; a < TR; ++a)
+#pragma unroll
+                    for (int b = 0; b < TC; ++b) {
+                        if (r0 + a == i) g[a][b] = cmul(g[a][b], ea);
+                        if (c0 + b == i) g[a][b] = cmul(g[a][b], eb);
+                    }
             }
+            const cplx coef = s.coef()[par];
+            cplx cr[TR], y[TC];
+#pragma unroll
+            for (int a = 0; a < TR; ++a) cr[a] = cmul(coef, s.col(par)[r0 + a]);
 #pragma unroll
             for (int b = 0; b < TC; ++b) {
-                const int c = c0 + b;
-                const cplx rv = (c < n) ? s.row(par)[c] : cmk(0.0, 0.0);
-                const cplx y = cmk(((c == i) ? 1.0 : 0.0) - rv.x, -rv.y);
-#pragma unroll
-                for (int a = 0; a < TR; ++a) {
-                    const int r = r0 + a;
-                    cplx v = g[a][b];
-                    if (!LEFT) {
-                        if (r == i) v = cmul(v, s.eao()[i]);
-                        if (c == i) v = cmul(v, s.ebo()[i]);
-                    }
-                    v = cfma(cr[a], y, v);
-                    if (LEFT) {
-                        if (c == i) v = cmul(v, acc ? s.ean()[i] : s.eao()[i]);
-                        if (r == i) v = cmul(v, acc ? s.ebn()[i] : s.ebo()[i]);
-                    }
-                    g[a][b] = v;
-                }
+                const cplx rv = s.row(par)[c0 + b];
+                y[b] = cmk(((c0 + b == i) ? 1.0 : 0.0) - rv.x, -rv.y);
             }
-            if (k + 1 < n) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, n, LEFT ? n - 2 - k : k + 1, par ^ 1);
+#pragma unroll
+            for (int a = 0; a < TR; ++a)
+#pragma unroll
+                for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
+            if (LEFT && (rowhit || colhit)) {    // left sweep: wrap site i with its final field
+                const int acc = s.accf()[i];
+                const cplx ea = acc ? s.ean()[i] : s.eao()[i];
+                const cplx eb = acc ? s.ebn()[i] : s.ebo()[i];
+#pragma unroll
+                for (int a = 0; a < TR; ++a)
+#pragma unroll
+                    for (int b = 0; b < TC; ++b) {
+                        if (c0 + b == i) g[a][b] = cmul(g[a][b], ea);
+                        if (r0 + a == i) g[a][b] = cmul(g[a][b], eb);
+                    }
+            }
+            if (k + 1 < n) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, LEFT ? n - 2 - k : k + 1, par ^ 1);
         }
         __syncthreads();
     }
@@ -238,7 +256,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
 #pragma unroll
         for (int b = 0; b < TC; ++b) {
             const int r = r0 + a, c = c0 + b;
-            if (r < n && c < n) s.G()[r * n + c] = g[a][b];
+            if (act && r < n && c < n) s.G()[r * n + c] = g[a][b];
         }
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
@@ -279,100 +297,103 @@ COLD void slice_products(Ctx<NMAX> x) {
 }
 
 // ---------------------------------------------------------------------------
-// equal-time estimators (Obs_equal_calc, obser_equal.f90:95-198)
+// equal-time estimators (Obs_equal_calc, obser_equal.f90:95-198).  The c
+// flavour's Green's function is the complex conjugate of the b flavour's
+// (obser_equal.f90:112-113), so every c-flavour sum is the conjugate of the
+// b-flavour sum and is not recomputed.  The K-point phase depends only on the
+// displacement r = i - j, so it comes from an Lq-entry table in shared memory.
 template <int NMAX>
 COLD void measure(Ctx<NMAX> x) {
     auto& s = x.s;
-    const int n = x.n, tid = threadIdx.x;
-    const double lq = (double)x.P().Lq, lq2 = lq * lq;
+    const PointDev& P = x.P();
+    const int n = x.n, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
+    const double lq = (double)P.Lq, lq2 = lq * lq;
     const cplx* G = s.G();
-    double v[24];
+    const cplx* ph = s.ph();
+    const bool hasK = P.hasK;
+    // v: 0 sum Re(t_up), 1 sum |Gc|^2, 2-3 sf_K, 4-5 dw_K, 6-7 sum t_up, 8-9 sum du_i conj(du_j),
+    //    10 kinetic, 11 sum Re du, 12 sum |du|^2, 13 sum Re du^2
+    double v[14];
 #pragma unroll
-    for (int k = 0; k < 24; ++k) v[k] = 0.0;
+    for (int k = 0; k < 14; ++k) v[k] = 0.0;
     for (int e = tid; e < n * n; e += blockDim.x) {
-        const int i = e / n, j = e % n;
+        const int i = e / n, j = e - (e / n) * n;
         const cplx a = G[i * n + j];                  // Grup(i,j)
         cplx gc = G[j * n + i];                       // Grupc(i,j) = G(j,i) - delta_ij
         if (i == j) gc.x -= 1.0;
         const cplx dui = cmk(G[i * n + i].x - 1.0, G[i * n + i].y);
         const cplx duj = cmk(G[j * n + j].x - 1.0, G[j * n + j].y);
-        const cplx ddi = cconj(dui), ddj = cconj(duj);
-        const cplx tup = cadd(cmul(dui, duj), cmul(gc, a));
-        const cplx tdo = cadd(cmul(ddi, ddj), cmul(cconj(gc), cconj(a)));
-        const cplx tud = cmul(dui, ddj);
+        const cplx tup = cadd(cmul(dui, duj), cmul(gc, a));   // b-flavour density correlator
+        const cplx tud = cmulcj(dui, duj);                     // du_i * dd_j
         v[0] += tup.x;
-        v[1] += tdo.x;
-        const cplx ps = cmul(gc, cconj(gc));
-        v[2] += ps.x / lq2;
-        v[3] += ps.y / lq2;
-        v[8] += tup.x / lq;
-        v[9] += tup.y / lq;
-        v[10] += tdo.x / lq;
-        v[11] += tdo.y / lq;
-        v[12] += tud.x / lq;
-        v[13] += tud.y / lq;
-        if (x.P().hasK) {
-            const cplx ph = x.P().phaseK[i * n + j];
-            const cplx sf = cmul(ph, cadd(gc, cconj(gc)));
-            const cplx dw = cmul(ph, cadd(cadd(tup, tdo), cadd(tud, cmul(ddi, duj))));
-            v[4] += sf.x / lq2;
-            v[5] += sf.y / lq2;
-            v[6] += dw.x / lq2;
-            v[7] += dw.y / lq2;
+        v[1] += gc.x * gc.x + gc.y * gc.y;
+        v[6] += tup.x;
+        v[7] += tup.y;
+        v[8] += tud.x;
+        v[9] += tud.y;
+        if (hasK) {
+            const int ix = i % lx, iy = i / lx, jx = j % lx, jy = j / lx;
+            int dx = ix - jx, dy = iy - jy;
+            dx += (dx < 0) ? lx : 0;
+            dy += (dy < 0) ? ly : 0;
+            const cplx p = ph[dy * lx + dx];
+            const double sfr = 2.0 * gc.x;                     // Grupc + Grdoc
+            const double dwr = 2.0 * tup.x + 2.0 * tud.x;      // t_up + t_do + du_i dd_j + dd_i du_j
+            v[2] += p.x * sfr;
+            v[3] += p.y * sfr;
+            v[4] += p.x * dwr;
+            v[5] += p.y * dwr;
         }
     }
-    for (int e = tid; e < 3 * n; e += blockDim.x) {
-        const int i = e / 3, jj = x.P().bonds[e];
+    for (int e = tid; e < 3 * n; e += blockDim.x) {   // bonds (x+1,y), (x,y+1), (x-1,y+1) (lattice.f90:98-111)
+        const int i = e / 3, nb = e - (e / 3) * 3;
+        const int ix = i % lx, iy = i / lx;
+        const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
+        const int jy = (nb == 0) ? iy : (iy + 1) % ly;
+        const int jj = jy * lx + jx;
         cplx gij = G[jj * n + i], gji = G[i * n + jj];   // Grupc(i,jj), Grupc(jj,i)
         if (i == jj) { gij.x -= 1.0; gji.x -= 1.0; }
-        v[14] += x.P().RT * (gij.x + gji.x + gij.x + gji.x) / lq;
+        v[10] += 2.0 * (gij.x + gji.x);
     }
     for (int i = tid; i < n; i += blockDim.x) {
-        const cplx du = cmk(G[i * n + i].x - 1.0, G[i * n + i].y), dd = cconj(du);
-        const cplx ud = cmul(du, dd);
-        const double dens = du.x + dd.x;
-        v[15] += du.x / lq;
-        v[16] += dd.x / lq;
-        v[17] += ud.x / lq;
-        v[18] += (cmul(du, du).x + cmul(dd, dd).x) / lq;
-        v[19] += du.x;
-        v[20] += dd.x;
-        v[21] += dens / lq;
-        v[22] += 2.0 * cmul(du, du).x + du.x;
-        v[23] += 2.0 * cmul(dd, dd).x + dd.x;
-        s.obs()[O_SITE + i] += dens;
+        const cplx du = cmk(G[i * n + i].x - 1.0, G[i * n + i].y);
+        v[11] += du.x;
+        v[12] += du.x * du.x + du.y * du.y;
+        v[13] += du.x * du.x - du.y * du.y;
+        s.obs()[O_SITE + i] += 2.0 * du.x;
     }
-    block_sum<24>(v, s.red());
+    block_sum<14>(v, s.red());
     if (tid == 0) {
         double* o = s.obs();
-        o[O_NUMSQUARE_UP] += v[0];
-        o[O_NUMSQUARE_DO] += v[1];
-        o[O_PSF_GAMMA] += v[2];
-        o[O_PSF_GAMMA + 1] += v[3];
-        o[O_SF_K] += v[4];
-        o[O_SF_K + 1] += v[5];
-        o[O_DW_K] += v[6];
-        o[O_DW_K + 1] += v[7];
-        o[O_DEN_UPUP] += v[8];
-        o[O_DEN_UPUP + 1] += v[9];
-        o[O_DEN_DODO] += v[10];
-        o[O_DEN_DODO + 1] += v[11];
-        o[O_DEN_UPDO] += v[12];
-        o[O_DEN_UPDO + 1] += v[13];
-        const double kin = v[14];
-        o[O_DENSITY_UP] += v[15];
-        o[O_DENSITY_DO] += v[16];
-        o[O_DOUBLEOCC] += v[17];
-        o[O_SQUAREOCC] += v[18];
-        o[O_NUM_UP] += v[19];
-        o[O_NUM_DO] += v[20];
-        o[O_DENSITY_TOTAL] += v[21];
-        o[O_ONSITE_N2_UP] += v[22];
-        o[O_ONSITE_N2_DO] += v[23];
-        const double inter = (x.P().U1 + x.P().U2) * (v[22] + v[23]) / lq + 2.0 * (x.P().U2 - x.P().U1) * v[17];
+        const double onsite = 2.0 * v[13] + v[11];          // sum Re(2 du^2 + du)
+        const double dbl = v[12] / lq;                       // doubleOcc sample
+        const double kin = P.RT * v[10] / lq;
+        const double inter = (P.U1 + P.U2) * (2.0 * onsite) / lq + 2.0 * (P.U2 - P.U1) * dbl;
+        o[O_DENSITY_UP] += v[11] / lq;
+        o[O_DENSITY_DO] += v[11] / lq;
+        o[O_DENSITY_TOTAL] += 2.0 * v[11] / lq;
         o[O_KINETIC] += kin;
+        o[O_DOUBLEOCC] += dbl;
+        o[O_SQUAREOCC] += 2.0 * v[13] / lq;
+        o[O_NUM_UP] += v[11];
+        o[O_NUM_DO] += v[11];
+        o[O_NUMSQUARE_UP] += v[0];
+        o[O_NUMSQUARE_DO] += v[0];
+        o[O_ONSITE_N2_UP] += onsite;
+        o[O_ONSITE_N2_DO] += onsite;
         o[O_INTERACTION] += inter;
         o[O_ENERGY] += kin + inter;
+        o[O_PSF_GAMMA] += v[1] / lq2;
+        o[O_SF_K] += v[2] / lq2;
+        o[O_SF_K + 1] += v[3] / lq2;
+        o[O_DW_K] += v[4] / lq2;
+        o[O_DW_K + 1] += v[5] / lq2;
+        o[O_DEN_UPUP] += v[6] / lq;
+        o[O_DEN_UPUP + 1] += v[7] / lq;
+        o[O_DEN_DODO] += v[6] / lq;
+        o[O_DEN_DODO + 1] -= v[7] / lq;
+        o[O_DEN_UPDO] += v[8] / lq;
+        o[O_DEN_UPDO + 1] += v[9] / lq;
         x.sc->nobs += 1;
     }
     __syncthreads();
@@ -567,6 +588,8 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     if (threadIdx.x == 0) *x.s.P() = ka.pts[cd.point];
     __syncthreads();
     x.n = x.P().N;
+    if (x.P().hasK)
+        for (int r = threadIdx.x; r < x.P().Lq && r < NMAX; r += blockDim.x) x.s.ph()[r] = x.P().phaseR[r];
     x.abase = ka.arena + cd.arena_off;
     x.phi = ka.phi + cd.phi_off;
     x.sc = ka.sc + chain;
