@@ -60,6 +60,7 @@ SIGNATURES = {
     "bafqmc_phase_timers": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_synchronize": (C.c_int, [_P]),
     "bafqmc_stream": (_P, [_P]),
+    "bafqmc_sweep_noalloc": (C.c_int, [C.POINTER(Point), C.c_int, _P, _P, C.c_int, _P, _P]),
 }
 
 _lib = None

@@ -645,3 +645,155 @@ int bafqmc_synchronize(bafqmc_handle* h) {
 void* bafqmc_stream(bafqmc_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Entry point that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc once they are running: a host program
+// whose device memory is fully claimed by another runtime's caching allocator,
+// or a production driver that sizes all device memory before a long campaign
+// and forbids allocation afterwards.  bafqmc_sweep_noalloc runs the same
+// kernels as bafqmc_pre + bafqmc_sweep, but keeps every piece of scratch state
+// (chain descriptors, e^{-+dtau K}, UDV slots, Green's functions, accumulators)
+// in one file-scope device array of fixed size.  The caller passes its own
+// device buffers for the inputs and outputs.
+namespace {
+
+constexpr size_t kNoAllocBytes = (size_t)BAFQMC_NOALLOC_MAX_BYTES;
+// Host code must never use this name as a device address: it is a host-side
+// stand-in.  The device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+__global__ void noalloc_seeds_in(ChainScalars* sc, const int32_t* seeds, int nchains) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nchains) {
+        ChainScalars z;
+        memset(&z, 0, sizeof(z));
+        z.seed = (uint32_t)seeds[c];
+        sc[c] = z;
+    }
+}
+
+__global__ void noalloc_seeds_out(const ChainScalars* sc, int32_t* seeds, int nchains) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nchains) seeds[c] = (int32_t)sc[c].seed;
+}
+
+}  // namespace
+
+extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t* seeds, double* phi, int nsweep,
+                                    double* chain_obs, void* stream) {
+    if (!pt || nchains < 1 || !seeds || !phi || nsweep < 1 || !chain_obs)
+        return fail(BAFQMC_EARG, "bafqmc_sweep_noalloc: bad arguments");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(BAFQMC_EARG, "bafqmc_sweep_noalloc: device index too large");
+    if (!g_noalloc_base[dev]) {   // once per device, with that device current
+        void* base = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_base[dev] = static_cast<unsigned char*>(base);
+    }
+    PointHost ph;
+    int rc = setup_point(*pt, ph);
+    if (rc != BAFQMC_OK) return rc;
+    const int n = ph.N, cls = class_of(n);
+    const int stride = bq::kObsScalars + ph.Lq;
+    const long long asz = bq::arena_size(n, ph.Nst);
+    // scratch layout: point | chains | scalars | index list | matrices | observables | arenas
+    const size_t o_pt = 0;
+    const size_t o_ch = align256(o_pt + sizeof(PointDev));
+    const size_t o_sc = align256(o_ch + sizeof(ChainDev) * nchains);
+    const size_t o_ix = align256(o_sc + sizeof(ChainScalars) * nchains);
+    const size_t o_mt = align256(o_ix + sizeof(int) * nchains);
+    const size_t nn = (size_t)n * n;
+    const size_t o_ob = align256(o_mt + sizeof(double2) * (2 * nn + ph.Lq));
+    const size_t o_ar = align256(o_ob + sizeof(double) * (size_t)nchains * stride);
+    const size_t total = o_ar + sizeof(double2) * (size_t)asz * nchains;
+    if (total > kNoAllocBytes) {
+        char msg[256];
+        snprintf(msg, sizeof msg,
+                 "bafqmc_sweep_noalloc: %d chains of Ndim=%d, Ltrot=%d need %zu bytes of scratch; the fixed "
+                 "array holds %zu bytes (BAFQMC_NOALLOC_MAX_BYTES)",
+                 nchains, n, pt->Ltrot, total, kNoAllocBytes);
+        return fail(BAFQMC_EARG, msg);
+    }
+    unsigned char* base = g_noalloc_base[dev];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // descriptors staged on the host, copied into the array in one transfer
+    std::vector<unsigned char> stage(o_ob, 0);
+    PointDev d;
+    d.N = n;
+    d.L = ph.p.Ltrot;
+    d.Nwrap = ph.p.Nwrap;
+    d.Nst = ph.Nst;
+    d.Lq = ph.Lq;
+    d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
+    d.Lx = ph.p.Lx;
+    d.Ly = ph.p.Ly;
+    for (int ch = 0; ch < 2; ++ch) {
+        d.active[ch] = ph.active[ch];
+        d.alpha_re[ch] = ph.alpha_re[ch];
+        d.alpha_im[ch] = ph.alpha_im[ch];
+    }
+    d.shiftLoc = ph.p.shiftLoc;
+    d.U1 = ph.p.U1;
+    d.U2 = ph.p.U2;
+    d.RT = 1.0;
+    const double2* mats = reinterpret_cast<const double2*>(base + o_mt);
+    d.expP = mats;
+    d.expM = mats + nn;
+    d.phaseR = mats + 2 * nn;
+    std::memcpy(stage.data() + o_pt, &d, sizeof d);
+    ChainDev* cd = reinterpret_cast<ChainDev*>(stage.data() + o_ch);
+    int* ix = reinterpret_cast<int*>(stage.data() + o_ix);
+    for (int c = 0; c < nchains; ++c) {
+        cd[c].point = 0;
+        cd[c].pad = 0;
+        cd[c].arena_off = (long long)c * asz;
+        cd[c].phi_off = (long long)c * ph.p.Ltrot * n * 2;
+        ix[c] = c;
+    }
+    std::memcpy(stage.data() + o_mt, ph.expP.a.data(), sizeof(double2) * nn);
+    std::memcpy(stage.data() + o_mt + sizeof(double2) * nn, ph.expM.a.data(), sizeof(double2) * nn);
+    std::memcpy(stage.data() + o_mt + 2 * sizeof(double2) * nn, ph.phaseR.data(), sizeof(double2) * ph.Lq);
+    static uint32_t apow[bq::kMaxPow];
+    if (apow[0] == 0) {
+        unsigned long long v = 1;
+        for (int k = 0; k < bq::kMaxPow; ++k) {
+            apow[k] = (uint32_t)v;
+            v = (v * 48828125ull) & 0x7fffffffull;
+        }
+    }
+    CK(bq::upload_pow_table(apow, bq::kMaxPow));
+    CK(cudaMemcpyAsync(base, stage.data(), o_ob, cudaMemcpyHostToDevice, st));
+    // the array keeps the previous call's contents: reset what is accumulated
+    CK(cudaMemsetAsync(base + o_ob, 0, o_ar - o_ob, st));
+    ChainScalars* sc = reinterpret_cast<ChainScalars*>(base + o_sc);
+    noalloc_seeds_in<<<(nchains + 127) / 128, 128, 0, st>>>(sc, seeds, nchains);
+    CK(cudaGetLastError());
+    bq::KernelArgs ka;
+    ka.pts = reinterpret_cast<const PointDev*>(base + o_pt);
+    ka.chains = reinterpret_cast<const ChainDev*>(base + o_ch);
+    ka.nchains = nchains;
+    ka.obs_stride = stride;
+    ka.arena = reinterpret_cast<double2*>(base + o_ar);
+    ka.phi = phi;
+    ka.obs = reinterpret_cast<double*>(base + o_ob);
+    ka.sc = sc;
+    ka.timers = 0;
+    const int* d_ix = reinterpret_cast<const int*>(base + o_ix);
+    CK(bq::launch_pre(cls, ka, d_ix, nchains, st));
+    CK(bq::launch_bin_reset(ka, st));
+    for (int s = 0; s < nsweep; ++s) CK(bq::launch_sweep(cls, ka, d_ix, nchains, st));
+    CK(bq::launch_bin_finish(ka, st));
+    CK(cudaMemcpyAsync(chain_obs, ka.obs, sizeof(double) * (size_t)nchains * stride, cudaMemcpyDeviceToDevice, st));
+    noalloc_seeds_out<<<(nchains + 127) / 128, 128, 0, st>>>(sc, seeds, nchains);
+    CK(cudaGetLastError());
+    return BAFQMC_OK;
+}

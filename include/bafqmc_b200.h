@@ -121,6 +121,26 @@ int bafqmc_synchronize(bafqmc_handle* h);
 /* The handle's cudaStream_t, for event timing by the caller. */
 void* bafqmc_stream(bafqmc_handle* h);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory once they run (another runtime's caching allocator owns the device,
+ * or the driver sizes all memory before a campaign): bafqmc_pre followed by
+ * one bin of nsweep sweeps for nchains chains of one point, with all scratch
+ * in a fixed device array of BAFQMC_NOALLOC_MAX_BYTES that every GPU loading
+ * the library holds until exit.  No cudaMalloc/cudaFree is called.
+ *   seeds     [nchains] int32, device memory: in = start seeds, out = advanced
+ *   phi       [nchains][Ltrot][Ns][2] doubles, device memory: fields, updated
+ *   chain_obs [nchains][BAFQMC_OBS_SCALARS + Lx*Ly] doubles, device memory: the
+ *             bin averages, laid out as bafqmc_bin_chain_obs for that point
+ *   stream    cudaStream_t to run on (NULL = legacy default stream)
+ * Sizes beyond the array return BAFQMC_EARG with the bytes needed.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  Every call reuses the same array, so calls that
+ * overlap on the GPU (other streams, other host threads) race and must not be
+ * issued; the call clears the accumulators it reads. */
+#define BAFQMC_NOALLOC_MAX_BYTES (64u << 20)
+int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t* seeds, double* phi, int nsweep,
+                         double* chain_obs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
