@@ -14,9 +14,9 @@ namespace bq {
 __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 
 template <int NMAX> struct Cfg;
-template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2; };
+template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4; };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 6; };
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 
 // Dynamic shared memory of the sweep kernels.  Every buffer sits at a
@@ -28,9 +28,10 @@ struct Smem {
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
     static constexpr size_t MM = sizeof(cplx) * NMAX * NMAX, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
-    static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + 2 * VC, oDelta = oRow + 2 * VC;
+    static constexpr int KB = Cfg<NMAX>::KB;
+    static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
     static constexpr size_t oEao = oDelta + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
-    static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + 2 * sizeof(cplx);
+    static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + KB * sizeof(cplx);
     static constexpr size_t oP = oCbc + 4 * sizeof(cplx);
     static constexpr size_t oRg = oP + ((sizeof(PointDev) + 15) / 16) * 16;
     static constexpr size_t oU2 = oRg + VD, oPhin = oU2 + VD, oVn1 = oPhin + VD, oVn2 = oVn1 + VD, oD = oVn2 + VD;
@@ -47,8 +48,8 @@ struct Smem {
     DEVI cplx* W1() const { return at<cplx>(oW1); }
     DEVI cplx* W2() const { return at<cplx>(oW2); }
     DEVI cplx* tau() const { return at<cplx>(oTau); }
-    DEVI cplx* col(int par) const { return at<cplx>(oCol) + par * NMAX; }
-    DEVI cplx* row(int par) const { return at<cplx>(oRow) + par * NMAX; }
+    DEVI cplx* col(int m) const { return at<cplx>(oCol) + m * NMAX; }   // column of the m-th site of a block
+    DEVI cplx* row(int m) const { return at<cplx>(oRow) + m * NMAX; }   // row of the m-th site of a block
     DEVI cplx* delta() const { return at<cplx>(oDelta); }
     DEVI cplx* eao() const { return at<cplx>(oEao); }
     DEVI cplx* ean() const { return at<cplx>(oEan); }
@@ -107,66 +108,40 @@ DEVI void load_expT(Ctx<NMAX>& x) {
 // ---------------------------------------------------------------------------
 // local update of one channel over all sites of one slice, fused with the
 // V-wrap of G (LocalU_prop_L / LocalU_prop_R, localU.f90:79-113, and
-// LocalU_metro, localU.f90:31-77).  Sites are strictly sequential; each site
-// costs one barrier: the owner of the next diagonal element makes the next
-// Metropolis decision right after its own update, and the owners of the next
-// row/column stage them, so the rank-1 update of site i and the staging for
-// site i+1 share one pass.  G lives in registers for the whole loop.
+// LocalU_metro, localU.f90:31-77).
+//
+// Sites are strictly sequential.  They are taken in blocks of KB consecutive
+// sites.  Within a block one warp runs the sites one after another, with
+// warp-level synchronisation only: for each site it wraps and records the
+// site's column and row, makes the Metropolis decision (every lane computes
+// the same one), and applies the rank-1 update to the rows and columns of the
+// block's sites -- the only elements the block's later sites read.  After the
+// block, the whole CTA adds the block's KB rank-1 terms to the remaining
+// elements, which the wraps of the block's sites do not touch.  The terms are
+// the reference's ZGERU updates; only the order of the additions changes.
 
-// Metropolis decision for site j from the (wrapped) diagonal element gjj:
-// ratio_det = 1/(1 + Delta (1 - G_jj)), accept if |r_gauss * |ratio_det|^2| > u;
-// on accept the rank-1 coefficient is -ratio_det * Delta (localU.f90:56-71).
-template <int NMAX>
-DEVI void metro_decide(Smem<NMAX>& s, int j, cplx gjj, int par) {
-    const cplx d = s.delta()[j];
+// Metropolis ratio for the (wrapped) diagonal element gjj: ratio_det = 1/w,
+// w = 1 + Delta (1 - G_jj); accept if r_gauss |ratio_det|^2 > u; on accept the
+// rank-1 coefficient is -ratio_det * Delta (localU.f90:56-71).
+DEVI bool metro_ratio(cplx d, double rg, double u, cplx gjj, cplx& coef) {
     const cplx w = cmk(1.0 + (d.x * (1.0 - gjj.x) + d.y * gjj.y), d.y * (1.0 - gjj.x) - d.x * gjj.y);
-    const double nw = w.x * w.x + w.y * w.y;
-    const double inv = 1.0 / nw;
-    const bool accept = s.rg()[j] * inv > s.u2()[j];
+    const double inv = 1.0 / (w.x * w.x + w.y * w.y);
+    const bool accept = rg * inv > u;
     const cplx t = cmulcj(d, w);   // Delta * conj(w)
-    s.coef()[par] = accept ? cmk(-t.x * inv, -t.y * inv) : cmk(0.0, 0.0);
-    s.accf()[j] = accept ? 1 : 0;
-}
-
-// Stage row/column j (wrapped with its current field for the right sweep) from
-// this thread's tile; the owner of (j,j) then decides on site j.
-template <int NMAX, bool LEFT, int TR, int TC>
-DEVI void metro_stage(Smem<NMAX>& s, const cplx (&g)[TR][TC], int r0, int c0, int j, int par) {
-    const bool rowhit = (unsigned)(j - r0) < (unsigned)TR;
-    const bool colhit = (unsigned)(j - c0) < (unsigned)TC;
-    if (!rowhit && !colhit) return;
-    const cplx ea = LEFT ? cmk(1.0, 0.0) : s.eao()[j];
-    const cplx eb = LEFT ? cmk(1.0, 0.0) : s.ebo()[j];
-    cplx vjj = cmk(0.0, 0.0);
-#pragma unroll
-    for (int a = 0; a < TR; ++a) {
-#pragma unroll
-        for (int b = 0; b < TC; ++b) {
-            const int r = r0 + a, c = c0 + b;
-            if (r == j || c == j) {
-                cplx v = g[a][b];
-                if (!LEFT) {
-                    if (r == j) v = cmul(v, ea);
-                    if (c == j) v = cmul(v, eb);
-                }
-                if (c == j) s.col(par)[r] = v;
-                if (r == j) s.row(par)[c] = v;
-                if (r == j && c == j) vjj = v;
-            }
-        }
-    }
-    if (rowhit && colhit) metro_decide(s, j, vjj, par);
+    coef = accept ? cmk(-t.x * inv, -t.y * inv) : cmk(0.0, 0.0);
+    return accept;
 }
 
 template <int NMAX, bool LEFT>
 COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB;
     auto& s = x.s;
-    const int n = x.n, tid = threadIdx.x;
+    const int n = x.n, tid = threadIdx.x, lane = tid & 31;
     const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
     const double shift = fabs(x.P().shiftLoc);
     const uint32_t s0 = *s.seed();
     double* phis = x.phi + (long)slice * n * 2;
+    cplx* G = s.G();
 
     // per-site proposals; draw order follows the visiting order of the sites
     for (int i = tid; i < n; i += blockDim.x) {
@@ -190,74 +165,147 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     }
     __syncthreads();
 
-    // thread tile: rows r0..r0+TR-1, columns c0..c0+TC-1 (r0, c0 < NMAX so the
-    // staging vectors are read in bounds; elements outside n x n are never stored)
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const bool act = tid < ncg * nrg;
     const int r0 = act ? (tid / ncg) * TR : 0, c0 = act ? (tid % ncg) * TC : 0;
-    cplx g[TR][TC];
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-        for (int b = 0; b < TC; ++b) {
-            const int r = r0 + a, c = c0 + b;
-            g[a][b] = (r < n && c < n) ? s.G()[r * n + c] : cmk(0.0, 0.0);
-        }
 
-    if (act) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, LEFT ? n - 1 : 0, 0);
-    __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        const int i = LEFT ? n - 1 - k : k;
-        const int par = k & 1;
+    // The block's sites run on the first two warps (named barrier 1) with the
+    // block's rows and columns in registers: thread t holds column t of the block
+    // rows (ra) and row t of the block columns (ca, for t outside the block).
+    // Registers are kept in visiting order (slot q = q-th site of the block), and
+    // the site loop is unrolled, so every register index is a constant.  A site
+    // costs one barrier: threads stage the site's row and column, every thread
+    // makes the same Metropolis decision, and each updates its own registers.
+    // The rank-1 term is applied as ZGERU does, temp = alpha*y(j), then
+    // A(i,j) += x(i)*temp.
+    constexpr int NB = 64;
+    for (int k0 = 0; k0 < n; k0 += KB) {
+        const int kb = min(KB, n - k0);
+        const int slo = LEFT ? n - k0 - kb : k0;   // block sites are slo .. slo+kb-1
+        if (tid < NB) {
+            const int t = tid;
+            const bool tv = t < n;
+            const bool tin = (unsigned)(t - slo) < (unsigned)kb;
+            // site of slot q
+#define SITE(q) (LEFT ? n - 1 - (k0 + (q)) : k0 + (q))
+            cplx ra[KB], ca[KB];
+#pragma unroll
+            for (int q = 0; q < KB; ++q) {
+                const int sq = SITE(q);
+                ra[q] = (tv && q < kb) ? G[sq * n + t] : cmk(0.0, 0.0);
+                ca[q] = (tv && q < kb && !tin) ? G[t * n + sq] : cmk(0.0, 0.0);
+            }
+#pragma unroll
+            for (int m = 0; m < KB; ++m) {
+                if (m < kb) {
+                    const int i = SITE(m);
+                    const bool ti = (t == i);
+                    cplx* xr = s.col(m);
+                    cplx* yr = s.row(m);
+                    const cplx ea = s.eao()[i], eb = s.ebo()[i];
+                    if (!LEFT) {   // right sweep: wrap site i first (row i by ea, then column i by eb)
+                        ra[m] = cmul(ra[m], ea);
+                        if (ti) {
+#pragma unroll
+                            for (int q = 0; q < KB; ++q) ra[q] = cmul(ra[q], eb);
+                        }
+                        if (!tin) ca[m] = cmul(ca[m], eb);
+                    }
+                    // stage: y(t) = G(i,t); x(t) = G(t,i) outside the block; thread i stages x inside it
+                    const cplx yt = ra[m], xt = ca[m];
+                    if (tv) {
+                        yr[t] = yt;
+                        if (!tin) xr[t] = xt;
+                        if (ti) {
+#pragma unroll
+                            for (int q = 0; q < KB; ++q)
+                                if (q < kb) xr[SITE(q)] = ra[q];
+                        }
+                    }
+                    asm volatile("bar.sync 1, 64;" ::: "memory");
+                    cplx coef;
+                    const bool accept = metro_ratio(s.delta()[i], s.rg()[i], s.u2()[i], yr[i], coef);
+                    if (t == 0) {
+                        s.accf()[i] = accept ? 1 : 0;
+                        s.coef()[m] = coef;
+                    }
+                    if (accept && tv) {
+                        // block rows, column t: temp = coef * (delta(t,i) - y(t))
+                        const cplx cy = cmul(coef, cmk((ti ? 1.0 : 0.0) - yt.x, -yt.y));
+#pragma unroll
+                        for (int q = 0; q < KB; ++q)
+                            if (q < kb) ra[q] = cfma(xr[SITE(q)], cy, ra[q]);
+                        // row t, block columns: temp = coef * (delta(c,i) - y(c))
+                        if (!tin) {
+#pragma unroll
+                            for (int q = 0; q < KB; ++q) {
+                                if (q < kb) {
+                                    const cplx yv = yr[SITE(q)];
+                                    const cplx tmp = cmul(coef, cmk(((q == m) ? 1.0 : 0.0) - yv.x, -yv.y));
+                                    ca[q] = cfma(xt, tmp, ca[q]);
+                                }
+                            }
+                        }
+                    }
+                    if (LEFT) {   // left sweep: wrap site i with its final field (column i, then row i)
+                        const cplx eaf = accept ? s.ean()[i] : ea;
+                        const cplx ebf = accept ? s.ebn()[i] : eb;
+                        if (ti) {
+#pragma unroll
+                            for (int q = 0; q < KB; ++q) ra[q] = cmul(ra[q], eaf);
+                        }
+                        if (!tin) ca[m] = cmul(ca[m], eaf);
+                        ra[m] = cmul(ra[m], ebf);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < KB; ++q) {
+                const int sq = SITE(q);
+                if (tv && q < kb) G[sq * n + t] = ra[q];
+                if (tv && q < kb && !tin) G[t * n + sq] = ca[q];
+            }
+#undef SITE
+        }
+        __syncthreads();
+        // the block's rank-1 terms on the elements outside its rows and columns
         if (act) {
-            const bool rowhit = (unsigned)(i - r0) < (unsigned)TR;
-            const bool colhit = (unsigned)(i - c0) < (unsigned)TC;
-            if (!LEFT && (rowhit || colhit)) {   // right sweep: wrap site i first (row, then column)
-                const cplx ea = s.eao()[i], eb = s.ebo()[i];
+            cplx g[TR][TC];
+            bool own[TR][TC];
+#pragma unroll
+            for (int a = 0; a < TR; ++a)
+#pragma unroll
+                for (int b = 0; b < TC; ++b) {
+                    const int r = r0 + a, c = c0 + b;
+                    own[a][b] = r < n && c < n && (unsigned)(r - slo) >= (unsigned)kb &&
+                                (unsigned)(c - slo) >= (unsigned)kb;
+                    g[a][b] = G[min(r, n - 1) * n + min(c, n - 1)];
+                }
+#pragma unroll
+            for (int m = 0; m < KB; ++m) {
+                if (m >= kb) break;
+                const cplx cf = s.coef()[m];
+                cplx cr[TR], y[TC];
+#pragma unroll
+                for (int a = 0; a < TR; ++a) cr[a] = cmul(cf, s.col(m)[min(r0 + a, n - 1)]);
+#pragma unroll
+                for (int b = 0; b < TC; ++b) {
+                    const cplx yv = s.row(m)[min(c0 + b, n - 1)];
+                    y[b] = cmk(-yv.x, -yv.y);
+                }
 #pragma unroll
                 for (int a = 0; a < TR; ++a)
 #pragma unroll
-                    for (int b = 0; b < TC; ++b) {
-                        if (r0 + a == i) g[a][b] = cmul(g[a][b], ea);
-                        if (c0 + b == i) g[a][b] = cmul(g[a][b], eb);
-                    }
-            }
-            const cplx coef = s.coef()[par];
-            cplx cr[TR], y[TC];
-#pragma unroll
-            for (int a = 0; a < TR; ++a) cr[a] = cmul(coef, s.col(par)[r0 + a]);
-#pragma unroll
-            for (int b = 0; b < TC; ++b) {
-                const cplx rv = s.row(par)[c0 + b];
-                y[b] = cmk(((c0 + b == i) ? 1.0 : 0.0) - rv.x, -rv.y);
+                    for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
             }
 #pragma unroll
             for (int a = 0; a < TR; ++a)
 #pragma unroll
-                for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
-            if (LEFT && (rowhit || colhit)) {    // left sweep: wrap site i with its final field
-                const int acc = s.accf()[i];
-                const cplx ea = acc ? s.ean()[i] : s.eao()[i];
-                const cplx eb = acc ? s.ebn()[i] : s.ebo()[i];
-#pragma unroll
-                for (int a = 0; a < TR; ++a)
-#pragma unroll
-                    for (int b = 0; b < TC; ++b) {
-                        if (c0 + b == i) g[a][b] = cmul(g[a][b], ea);
-                        if (r0 + a == i) g[a][b] = cmul(g[a][b], eb);
-                    }
-            }
-            if (k + 1 < n) metro_stage<NMAX, LEFT, TR, TC>(s, g, r0, c0, LEFT ? n - 2 - k : k + 1, par ^ 1);
+                for (int b = 0; b < TC; ++b)
+                    if (own[a][b]) G[(r0 + a) * n + c0 + b] = g[a][b];
         }
         __syncthreads();
     }
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-        for (int b = 0; b < TC; ++b) {
-            const int r = r0 + a, c = c0 + b;
-            if (act && r < n && c < n) s.G()[r * n + c] = g[a][b];
-        }
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
@@ -268,10 +316,24 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
         x.sc->nc[ch] += n;
         *s.seed() = lcg_mul(c_apow[2 * n], s0);
     }
-    for (int e = tid; e < n * n; e += blockDim.x) {
-        const int r = e / n, c = e % n;
-        const int site = LEFT ? c : r;
-        s.U()[e] = cmul(s.U()[e], s.accf()[site] ? s.ean()[site] : s.eao()[site]);
+    {
+        constexpr int MAXE = Cfg<NMAX>::MAXE;
+        cplx u[MAXE], f[MAXE];
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k) {
+            const int e = tid + k * blockDim.x;
+            if (e < n * n) {
+                const int r = e / n, c = e - (e / n) * n;
+                const int site = LEFT ? c : r;
+                u[k] = s.U()[e];
+                f[k] = s.accf()[site] ? s.ean()[site] : s.eao()[site];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k) {
+            const int e = tid + k * blockDim.x;
+            if (e < n * n) s.U()[e] = cmul(u[k], f[k]);
+        }
     }
     __syncthreads();
 }
