@@ -16,7 +16,7 @@ __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 template <int NMAX> struct Cfg;
 template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4; };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 6; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4; };
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 
 // Dynamic shared memory of the sweep kernels.  Every buffer sits at a
@@ -669,7 +669,7 @@ DEVI void flush_obs(Ctx<NMAX>& x, double* gobs) {
 
 // one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
 template <int NMAX>
-__global__ void __launch_bounds__(Cfg<NMAX>::THREADS) sweep_kernel(KernelArgs ka, const int* idx, int count) {
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs ka, const int* idx, int count) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS) sweep_kernel(KernelArgs ka
 // Local_sweep_pre (local_sweep.f90:80-94) with Prop_make's identities
 // (process_matrix.f90:37-47).
 template <int NMAX>
-__global__ void __launch_bounds__(Cfg<NMAX>::THREADS) pre_kernel(KernelArgs ka, const int* idx, int count) {
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs ka, const int* idx, int count) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
