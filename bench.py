@@ -277,6 +277,8 @@ def main():
     value, tau = ess_rate(chain_sweeps)
 
     # ---- end to end through the C ABI: sweep + per-bin results to host buffers
+    from bafqmc_b200.multigpu import chain_average, torch_all_reduce
+    reduce = torch_all_reduce(device=dev) if world > 1 else (lambda b: b)
     d2h = 0
     barrier()
     t0 = time.perf_counter()
@@ -285,9 +287,8 @@ def main():
         pt = ens.point_obs_raw()
         ch = ens.chain_obs_raw()
         d2h = pt.nbytes + ch.nbytes
-        if world > 1:   # chain average across GPUs (m_process_obs_equal's MPI_REDUCE)
-            tt = torch.from_numpy(pt).to(dev)
-            dist.all_reduce(tt)
+        # job-wide chain average across GPUs (m_process_obs_equal's MPI_REDUCE)
+        job_avg = chain_average(pt[0] * C, C, reduce)
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
     if world > 1:
