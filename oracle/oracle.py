@@ -1,12 +1,14 @@
-"""CPU oracle for the BAFQMC finite-temperature sweep (number-conserving solver).
+"""CPU oracle for the BAFQMC finite-temperature sweep (number-conserving and
+Nambu pairing solvers).
 
 TEST INFRASTRUCTURE ONLY.  This module is the parity checker for the CUDA
 path in ``bafqmc_b200``.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline / reference legs of ``bench.py`` may import it; the product path
 never does, and it must not be used as a fallback.
 
-It restates, call for call, the reference Fortran solver of YinkaiYu/BAFQMC
-(files cited as ``src/number_conserving/src/<file>.f90:<line>``) in NumPy,
+It restates, call for call, the reference Fortran solvers of YinkaiYu/BAFQMC
+(files cited as ``src/number_conserving/src/<file>.f90:<line>``; the Nambu
+solver's files as ``src/pairing/src/<file>.f90:<line>``) in NumPy,
 with SciPy's LAPACK wrappers (ZGEQP3, ZUNGQR, ZUNMQR, ZTRSM, ZTRMM) standing
 in for the reference's own LAPACK calls so the stabilisation follows the same
 factorisation sequence.  Fortran arrays are 1-based column-major; here every
@@ -19,6 +21,10 @@ Parity pins (checked in ``tests/test_oracle.py``):
     that file), tolerance 2e-10;
   * the Gaussian closed forms of ``tests/physics/test_gaussian_solvers.py:44-77``
     (golden vectors in ``tests/golden/gaussian.json``), tolerances 2e-9 / 2e-8.
+The pairing path is pinned by the same Gaussian closed forms at Delta = 0,
++-0.2 (pair_equal included), by its Delta = 0 agreement with the
+number-conserving path, and by a dense fixed-field reference of the Nambu
+Green's function and estimators built in ``tests/test_oracle_pairing.py``.
 Bitwise parity with the reference's LAPACK is not pinned (no Fortran, MPI or
 LAPACK toolchain exists to run the reference); the reference tests themselves
 pin the LAPACK boundary only through invariants at 2e-10.
@@ -40,6 +46,7 @@ ZERO = 1.0e-10
 PI = math.acos(-1.0)
 NAUX = 2
 NBOND = 3
+NSEC = 4            # pairing sectors b, c, b^dagger, c^dagger (src/pairing/src/calc_basic.f90:13)
 LCG_A = 48828125
 LCG_M = 2147483648
 
@@ -100,14 +107,21 @@ class Params:
     iniAmpl: float = 1.0
     iniBias: tuple = (0.0, 0.0)
     RT: float = 1.0
+    RDelta: float = 0.0
+    pairing: bool = False
 
     @property
     def Lq(self) -> int:
         return self.Nlx * self.Nly
 
     @property
-    def Ndim(self) -> int:
+    def Nsite(self) -> int:
         return self.Lq
+
+    @property
+    def Ndim(self) -> int:
+        """Ns, or Nsite*Nsec for the Nambu solver (src/pairing/src/calc_basic.f90:99-101)."""
+        return NSEC * self.Lq if self.pairing else self.Lq
 
     @property
     def Dtau(self) -> float:
@@ -120,12 +134,15 @@ class Params:
         return self.Ltrot // self.Nwrap
 
     @classmethod
-    def from_text(cls, text: str) -> "Params":
+    def from_text(cls, text: str, pairing: bool = False) -> "Params":
+        """read_input (calc_basic.f90:48-59); the pairing solver reads RDelta as the
+        fourth value of line 1 (src/pairing/src/calc_basic.f90:51-52)."""
         rows = [ln.replace(",", " ").split() for ln in text.splitlines()]
         rows = [r for r in rows][:7]
         r = [[_fortran_token(t) for t in row] for row in rows]
         p = cls(
             U1=_float(r[0][0]), U2=_float(r[0][1]), mu=_float(r[0][2]),
+            RDelta=_float(r[0][3]) if pairing else 0.0, pairing=pairing,
             Nlx=int(r[1][0]), Nly=int(r[1][1]), Ltrot=int(r[1][2]), Beta=_float(r[1][3]),
             NlxTherm=int(r[2][0]), NlyTherm=int(r[2][1]), LtrotTherm=int(r[2][2]),
             Nwrap=int(r[3][0]), Nbin=int(r[3][1]), Nsweep=int(r[3][2]), shiftLoc=_float(r[3][3]),
@@ -219,8 +236,80 @@ def ham_T(p: Params, latt: Lattice) -> np.ndarray:
     return H
 
 
+def inv_dim(latt_lq: int, site: int, sec: int) -> int:
+    """inv_dim_list(site, sec) of the Nambu lattice, 0-based: sector-major order
+    b, c, b^dagger, c^dagger (src/pairing/src/lattice.f90:26-35)."""
+    return sec * latt_lq + site
+
+
+def ham_T_pairing(p: Params, latt: Lattice) -> np.ndarray:
+    """def_hamT of the Nambu solver (src/pairing/src/non_interact.f90:33-111)."""
+    ns = p.Lq
+    n = p.Ndim
+    H = np.zeros((n, n), dtype=complex)
+    z = complex(p.RT, 0.0)
+    for i in range(ns):
+        i1, i2, i3, i4 = (inv_dim(ns, i, k) for k in range(NSEC))
+        for nb in range(1, NBOND + 1):
+            j = latt.bonds[i, nb]
+            j1, j2, j3, j4 = (inv_dim(ns, j, k) for k in range(NSEC))
+            H[i1, j1] += z
+            H[i2, j2] += z
+            H[j3, i3] -= z
+            H[j4, i4] -= z
+            H[j1, i1] += z.conjugate()
+            H[j2, i2] += z.conjugate()
+            H[i3, j3] -= z.conjugate()
+            H[i4, j4] -= z.conjugate()
+    z = complex(p.RDelta, 0.0)
+    for i in range(ns):
+        i1, i2, i3, i4 = (inv_dim(ns, i, k) for k in range(NSEC))
+        H[i1, i4] += z
+        H[i2, i3] += z
+        H[i3, i2] -= z
+        H[i4, i1] -= z
+    z = complex(-p.mu, 0.0)
+    for i in range(ns):
+        i1, i2, i3, i4 = (inv_dim(ns, i, k) for k in range(NSEC))
+        H[i1, i1] += z
+        H[i2, i2] += z
+        H[i3, i3] -= z
+        H[i4, i4] -= z
+    return H
+
+
+def inv_and_det(a: np.ndarray):
+    """ZGETRF + ZGETRI with the LU determinant (src/common/mymats.f90:52-77;
+    src/pairing/src/localU.f90:194-220)."""
+    lu, ipiv, info = lapack.zgetrf(np.asfortranarray(a))
+    if info < 0:
+        raise RuntimeError(f"zgetrf info={info}")
+    det = complex(1.0, 0.0)
+    for i in range(a.shape[0]):
+        det = det * lu[i, i]
+        if ipiv[i] != i:
+            det = -det
+    ainv, info = lapack.zgetri(lu, ipiv)
+    if info != 0:
+        raise RuntimeError(f"zgetri info={info}")
+    return np.array(ainv), det
+
+
 class OperatorKinetic:
     def __init__(self, p: Params, latt: Lattice):
+        if p.pairing:
+            # opT_set + exp_general_matrix (src/pairing/src/non_interact.f90:113-178): the
+            # Nambu matrix is not Hermitian, so ZGEEV, the inverse eigenvector matrix and
+            # exp(-+dtau w) on the eigenvalues.
+            H = ham_T_pairing(p, latt)
+            w, V = np.linalg.eig(H)
+            Vinv, _ = inv_and_det(V)
+            self.energy_min = float(np.min(w.real))
+            self.energy_max = float(np.max(w.real))
+            self.bandwidth = self.energy_max - self.energy_min
+            self.expT_P = (V * np.exp(-p.Dtau * w)[None, :]) @ Vinv
+            self.expT_M = (V * np.exp(p.Dtau * w)[None, :]) @ Vinv
+            return
         H = ham_T(p, latt)
         w, U = np.linalg.eigh(H)
         self.energy_min = float(w.min())
@@ -233,18 +322,85 @@ class OperatorKinetic:
 
 # --------------------------------------------------------------------------
 # HS operator (operator_Hubbard.f90:36-68)
+CHANNEL_RELATIVE = 1   # U1 (n_b - n_c)^2 (src/pairing/src/operator_Hubbard.f90:10-11)
+CHANNEL_TOTAL = 2      # U2 (n_b + n_c)^2
+# sign of alpha*phi in the factor of each Nambu sector b, c, b^dagger, c^dagger
+# (src/pairing/src/operator_Hubbard.f90:155-166, 186-197)
+SECTOR_SIGN = {CHANNEL_RELATIVE: (1, -1, -1, 1), CHANNEL_TOTAL: (1, 1, -1, -1)}
+
+
+class PhaseCounter:
+    """Phase statistics of the Nambu weight ratio (src/pairing/src/operator_Hubbard.f90:228-284)."""
+
+    def __init__(self):
+        self.count_proposed = 0.0
+        self.count_accepted = 0.0
+        self.sum_abs_arg_proposed = 0.0
+        self.sum_abs_arg_accepted = 0.0
+        self.branch_pi_count = 0.0
+        self.reset()
+
+    def reset(self):
+        self.nc_prop_bin = 0.0
+        self.nc_acc_bin = 0.0
+        self.sum_abs_prop_bin = 0.0
+        self.sum_abs_acc_bin = 0.0
+        self.branch_pi_count_bin = 0.0
+
+    def count(self, phase: float, accepted: bool):
+        a = abs(phase)
+        self.nc_prop_bin += 1.0
+        self.sum_abs_prop_bin += a
+        if a > 0.9 * PI:
+            self.branch_pi_count_bin += 1.0
+        if accepted:
+            self.nc_acc_bin += 1.0
+            self.sum_abs_acc_bin += a
+
+    def ratio(self):
+        self.count_proposed += self.nc_prop_bin
+        self.count_accepted += self.nc_acc_bin
+        self.sum_abs_arg_proposed += self.sum_abs_prop_bin
+        self.sum_abs_arg_accepted += self.sum_abs_acc_bin
+        self.branch_pi_count += self.branch_pi_count_bin
+
+
 class OperatorHubbard:
-    def __init__(self, U: float, dtau: float):
+    def __init__(self, U: float, dtau: float, channel: int = 0):
         self.alpha = 0j
         if U < -ZERO:
             self.alpha = complex(math.sqrt(-2.0 * U * dtau), 0.0)
         if U > ZERO:
             self.alpha = complex(0.0, math.sqrt(2.0 * U * dtau))
         self.active = abs(U) > ZERO
+        self.channel = channel
         self.acc_local = 0.0
         self.acc_therm = 0.0
         self.nc = 0
         self.nacc = 0
+        self.phase = PhaseCounter()
+
+    def get_delta_pairing(self, phi_old: float, phi_new: float):
+        """opU_get_delta of the Nambu solver (src/pairing/src/operator_Hubbard.f90:100-137).
+
+        Returns (ratio_gaussian, ratio_constant, diagonal of the 4x4 Delta)."""
+        g_old, e_old = self.get_exp(phi_old, 1)
+        g_new, e_new = self.get_exp(phi_new, 1)
+        ratio_gaussian = g_new / g_old
+        ratio_constant = complex(1.0, 0.0)
+        if self.channel == CHANNEL_TOTAL:
+            ratio_constant = e_old / e_new
+        dphi = phi_new - phi_old
+        p = cmath.exp(self.alpha * dphi * 1) - 1.0
+        m = cmath.exp(-self.alpha * dphi * 1) - 1.0
+        d = tuple(p if sg > 0 else m for sg in SECTOR_SIGN[self.channel])
+        return ratio_gaussian, ratio_constant, np.array(d, dtype=complex)
+
+    def sector_factors(self, phi: float, nflag: int) -> np.ndarray:
+        """exp(+-alpha*phi*nflag) per sector, as opU_mmult_R/L apply them."""
+        ep = cmath.exp(self.alpha * phi * nflag)
+        em = cmath.exp(-self.alpha * phi * nflag)
+        return np.array([ep if sg > 0 else em for sg in SECTOR_SIGN[self.channel]], dtype=complex)
 
     def get_exp(self, phi: float, nflag: int) -> tuple[complex, complex]:
         gaussian = complex(math.exp(-0.5 * phi * phi), 0.0)
@@ -543,6 +699,142 @@ class ObserEqual:
 
 
 # --------------------------------------------------------------------------
+# equal-time observables of the Nambu solver (src/pairing/src/obser_equal.f90)
+OBS_REAL_PAIR = ("density_up", "density_do", "density", "density_total", "kinetic", "doubleOcc", "squareOcc",
+                 "local_numsquare", "pair_equal", "num_up", "num_do", "numsquare_up", "numsquare_do",
+                 "onsite_n2_up", "onsite_n2_do", "interaction_energy_density", "pairing_energy_density",
+                 "chemical_energy_density", "grand_energy_density", "energy_density")
+
+
+class ObserEqualPairing:
+    def __init__(self, lq: int):
+        self.lq = lq
+        self.reset()
+
+    def reset(self):
+        """Obs_equal_reset (obser_equal.f90:43-74)."""
+        for k in OBS_REAL_PAIR:
+            setattr(self, k, 0.0)
+        for k in OBS_CPLX:
+            setattr(self, k, 0j)
+        self.den_corr_up = np.zeros(self.lq, dtype=complex)
+        self.den_corr_do = np.zeros(self.lq, dtype=complex)
+        self.den_corr_updo = np.zeros(self.lq, dtype=complex)
+        self.single_corr = np.zeros(self.lq, dtype=complex)
+        self.density_site_total = np.zeros(self.lq)
+
+    def ave(self, nobs: int):
+        """Obs_equal_ave (obser_equal.f90:76-110)."""
+        z = 1.0 / float(nobs)
+        for k in OBS_REAL_PAIR:
+            setattr(self, k, getattr(self, k) * z)
+        for k in OBS_CPLX:
+            setattr(self, k, getattr(self, k) * z)
+        self.den_corr_up *= z
+        self.den_corr_do *= z
+        self.den_corr_updo *= z
+        self.single_corr *= z
+        self.density_site_total *= z
+
+    def calc(self, G: np.ndarray, p: Params, latt: Lattice):
+        """Obs_equal_calc (obser_equal.f90:112-271), Norb = 1."""
+        ns = p.Lq
+        lq = float(p.Lq)
+        blk = lambda r, c: G[r * ns:(r + 1) * ns, c * ns:(c + 1) * ns]
+        # rows b, c, b^dagger, c^dagger; the reference names a block by its row
+        # operator and the conjugate of its column operator (obser_equal.f90:133-153)
+        G_b_bdag, G_b_cdag, G_b_b, G_b_c = blk(0, 0), blk(0, 1), -blk(0, 2), -blk(0, 3)
+        G_c_bdag, G_c_cdag, G_c_b, G_c_c = blk(1, 0), blk(1, 1), -blk(1, 2), -blk(1, 3)
+        G_bdag_bdag, G_bdag_cdag, G_bdag_b, G_bdag_c = blk(2, 0), blk(2, 1), -blk(2, 2), -blk(2, 3)
+        G_cdag_bdag, G_cdag_cdag, G_cdag_b, G_cdag_c = blk(3, 0), blk(3, 1), -blk(3, 2), -blk(3, 3)
+        d = np.arange(ns)
+        nb = G_bdag_b[d, d]
+        nc = G_cdag_c[d, d]
+        Dbb = nb * nb + G_bdag_b[d, d] * G_b_bdag[d, d] + G_bdag_bdag[d, d] * G_b_b[d, d]
+        Dcc = nc * nc + G_cdag_c[d, d] * G_c_cdag[d, d] + G_cdag_cdag[d, d] * G_c_c[d, d]
+        Dbc = nb * nc + G_bdag_cdag[d, d] * G_b_c[d, d] + G_bdag_c[d, d] * G_b_cdag[d, d]
+        pair = (G_b_c[d, d] + G_bdag_cdag[d, d]).real
+        s_density_total = 0.0
+        s_double = 0.0
+        s_pair = 0.0
+        s_n2_up = 0.0
+        s_n2_do = 0.0
+        for ii in range(ns):   # site loop (obser_equal.f90:168-192), in the reference's order
+            site = ii
+            self.density_up += nb[ii].real / float(ns)
+            self.density_do += nc[ii].real / float(ns)
+            self.density += (nb[ii] + nc[ii]).real / float(ns)
+            self.num_up += nb[ii].real
+            self.num_do += nc[ii].real
+            self.doubleOcc += Dbc[ii].real / float(ns)
+            self.squareOcc += (nb[ii] * nb[ii] + nc[ii] * nc[ii]).real / float(ns)
+            self.local_numsquare += (Dbb[ii] + Dcc[ii]).real / float(ns)
+            self.pair_equal += pair[ii] / float(ns)
+            self.density_site_total[site] += (nb[ii] + nc[ii]).real
+            s_density_total += (nb[ii] + nc[ii]).real / float(ns)
+            s_double += Dbc[ii].real / float(ns)
+            s_pair += pair[ii] / float(ns)
+            s_n2_up += Dbb[ii].real
+            s_n2_do += Dcc[ii].real
+        # pair loop (obser_equal.f90:194-233): i = row site ii, j = column site jj
+        i = d[:, None]
+        j = d[None, :]
+        PDbb = G_bdag_b[i, i] * G_bdag_b[j, j] + G_bdag_b * G_b_bdag + G_bdag_bdag * G_b_b
+        PDcc = G_cdag_c[i, i] * G_cdag_c[j, j] + G_cdag_c * G_c_cdag + G_cdag_cdag * G_c_c
+        PDbc = G_bdag_b[i, i] * G_cdag_c[j, j] + G_bdag_cdag * G_b_c + G_bdag_c * G_b_cdag
+        PDcb = G_cdag_c[i, i] * G_bdag_b[j, j] + G_cdag_bdag * G_c_b + G_cdag_b * G_c_bdag
+        self.numsquare_up += float(np.sum(PDbb.real))
+        self.numsquare_do += float(np.sum(PDcc.real))
+        zlq = complex(lq, 0.0)
+        np.add.at(self.den_corr_up, latt.imj.ravel(), (PDbb / zlq).ravel())
+        np.add.at(self.den_corr_do, latt.imj.ravel(), (PDcc / zlq).ravel())
+        np.add.at(self.den_corr_updo, latt.imj.ravel(), (PDbc / zlq).ravel())
+        np.add.at(self.single_corr, latt.imj.ravel(), (G_bdag_b / zlq).ravel())
+        norm_k = 1.0 / (lq * lq)
+        sfk = 0j
+        dwk = 0j
+        if latt.hasK:
+            phase = np.exp(1j * latt.k_dot_r[latt.indexK, latt.imj])
+            sfk = complex(np.sum(phase * (G_bdag_b + G_cdag_c) * norm_k))
+            dwk = complex(np.sum(phase * (PDbb + PDcc + PDbc + PDcb) * norm_k))
+        psf = complex(np.sum((G_bdag_cdag[i, i] * G_c_b[j, j] + G_bdag_c * G_cdag_b + G_bdag_b * G_cdag_c) * norm_k))
+        kin = 0.0
+        for nbd in range(1, NBOND + 1):   # obser_equal.f90:235-244
+            jj = latt.bonds[:, nbd]
+            ii = np.arange(ns)
+            terms = p.RT * (G_bdag_b[ii, jj] + G_bdag_b[jj, ii] + G_cdag_c[ii, jj] + G_cdag_c[jj, ii]).real / float(ns)
+            kin += float(np.sum(terms))
+        s_inter = (p.U1 + p.U2) * (s_n2_up + s_n2_do) / float(ns) + 2.0 * (p.U2 - p.U1) * s_double
+        s_pairing = p.RDelta * s_pair
+        s_chem = -p.mu * s_density_total
+        s_energy = kin + s_inter + s_pairing
+        self.kinetic += kin
+        self.density_total += s_density_total
+        self.onsite_n2_up += s_n2_up
+        self.onsite_n2_do += s_n2_do
+        self.interaction_energy_density += s_inter
+        self.pairing_energy_density += s_pairing
+        self.chemical_energy_density += s_chem
+        self.energy_density += s_energy
+        self.grand_energy_density += s_energy + s_chem
+        self.sf_K += sfk
+        self.dw_K += dwk
+        self.psf_Gamma += psf
+
+    def as_dict(self, latt: Lattice) -> dict:
+        """The values the pairing bin writer emits (src/pairing/src/fourier_trans.f90:276-405)."""
+        out = {k: getattr(self, k) for k in OBS_REAL_PAIR}
+        for k in OBS_CPLX:
+            out[k] = getattr(self, k)
+        out["density_site_total"] = self.density_site_total.copy()
+        lq = float(self.lq)
+        out["den_upup_sub11"] = complex(np.sum(self.den_corr_up) / lq)
+        out["den_dodo_sub11"] = complex(np.sum(self.den_corr_do) / lq)
+        out["den_updo"] = complex(np.sum(self.den_corr_updo) / lq)
+        return out
+
+
+# --------------------------------------------------------------------------
 # one Markov chain (one MPI rank of the reference)
 class Chain:
     def __init__(self, p: Params, latt: Lattice, opT: OperatorKinetic, seed: int, phi: np.ndarray):
@@ -551,10 +843,10 @@ class Chain:
         self.opT = opT
         self.seed = int(seed)
         self.phi = np.array(phi, dtype=float)           # [Ltrot, Ns, Naux]
-        self.op = [OperatorHubbard(p.U1, p.Dtau), OperatorHubbard(p.U2, p.Dtau)]
+        self.op = [OperatorHubbard(p.U1, p.Dtau, CHANNEL_RELATIVE), OperatorHubbard(p.U2, p.Dtau, CHANNEL_TOTAL)]
         self.prop = Propagator(p.Ndim)
         self.wr = WrapList(p.Ndim, p.Nst)
-        self.obs = ObserEqual(p.Lq)
+        self.obs = ObserEqualPairing(p.Lq) if p.pairing else ObserEqual(p.Lq)
         self.nobs = 0
         self.acc_sum = [0.0, 0.0]        # sum over bins of per-bin acceptance ratio (AccCounter%acc)
         self.therm_acc_sum = [0.0, 0.0]
@@ -583,11 +875,79 @@ class Chain:
         else:
             op.count(False)
 
+    # ---- Nambu local update (src/pairing/src/localU.f90:33-113)
+    def _sec(self, site: int):
+        return [inv_dim(self.p.Lq, site, k) for k in range(NSEC)]
+
+    def metro_pairing(self, nf: int, site: int, nt: int):
+        p, op, G = self.p, self.op[nf], self.prop.Gr
+        phi_old = self.phi[nt, site, nf]
+        self.seed, xflip = ranf(self.seed)
+        xdif = (xflip - 0.5) * abs(p.shiftLoc)
+        phi_new = phi_old + xdif
+        ratio_gaussian, ratio_constant, dvec = op.get_delta_pairing(phi_old, phi_new)
+        isec = self._sec(site)
+        eye = np.eye(NSEC, dtype=complex)
+        pblock = eye + dvec[:, None] * (eye - G[np.ix_(isec, isec)])
+        pinv, det = inv_and_det(pblock)
+        ratio_det = det ** (-0.5)
+        ratio_exp = ratio_gaussian * ratio_constant
+        ratio_total = ratio_exp * ratio_det
+        ratio_phase = math.atan2(ratio_total.imag, ratio_total.real)
+        ratio_abs = abs(ratio_total)
+        self.seed, rnd = ranf(self.seed)
+        if ratio_abs > rnd:
+            op.count(True)
+            op.phase.count(ratio_phase, True)
+            left = G[:, isec]
+            mid = pinv * dvec[None, :]
+            right = -G[isec, :]
+            right[np.arange(NSEC), isec] += 1.0
+            self.prop.Gr = G - (left @ mid) @ right
+            self.phi[nt, site, nf] = phi_new
+        else:
+            op.count(False)
+            op.phase.count(ratio_phase, False)
+
+    def _mmult_R(self, M, nf, site, phi, nflag):
+        """opU_mmult_R: rows of the site's sectors (src/pairing/src/operator_Hubbard.f90:139-168)."""
+        f = self.op[nf].sector_factors(phi, nflag)
+        for k, r in enumerate(self._sec(site)):
+            M[r, :] = f[k] * M[r, :]
+
+    def _mmult_L(self, M, nf, site, phi, nflag):
+        """opU_mmult_L: columns of the site's sectors (src/pairing/src/operator_Hubbard.f90:170-199)."""
+        f = self.op[nf].sector_factors(phi, nflag)
+        for k, c in enumerate(self._sec(site)):
+            M[:, c] = M[:, c] * f[k]
+
+    def prop_L_pairing(self, nf: int, nt: int):
+        """LocalU_prop_L (src/pairing/src/localU.f90:115-131)."""
+        ns = self.p.Lq
+        for ii in range(ns - 1, -1, -1):
+            self.metro_pairing(nf, ii, nt)
+            self._mmult_L(self.prop.Gr, nf, ii, self.phi[nt, ii, nf], 1)
+            self._mmult_R(self.prop.Gr, nf, ii, self.phi[nt, ii, nf], -1)
+        for ii in range(ns - 1, -1, -1):
+            self._mmult_L(self.prop.UUL, nf, ii, self.phi[nt, ii, nf], 1)
+
+    def prop_R_pairing(self, nf: int, nt: int):
+        """LocalU_prop_R (src/pairing/src/localU.f90:133-149)."""
+        ns = self.p.Lq
+        for ii in range(ns):
+            self._mmult_R(self.prop.Gr, nf, ii, self.phi[nt, ii, nf], 1)
+            self._mmult_L(self.prop.Gr, nf, ii, self.phi[nt, ii, nf], -1)
+            self.metro_pairing(nf, ii, nt)
+        for ii in range(ns):
+            self._mmult_R(self.prop.UUR, nf, ii, self.phi[nt, ii, nf], 1)
+
     def _expalpha(self, nf, phi, nflag):
         return self.op[nf].get_exp(phi, nflag)[1]
 
     def prop_L(self, nf: int, nt: int):
         """LocalU_prop_L (localU.f90:79-95)."""
+        if self.p.pairing:
+            return self.prop_L_pairing(nf, nt)
         n = self.p.Ndim
         for ii in range(n - 1, -1, -1):
             self.metro(nf, ii, nt)
@@ -599,6 +959,8 @@ class Chain:
 
     def prop_R(self, nf: int, nt: int):
         """LocalU_prop_R (localU.f90:97-113)."""
+        if self.p.pairing:
+            return self.prop_R_pairing(nf, nt)
         n = self.p.Ndim
         for ii in range(n):
             G = self.prop.Gr
@@ -618,7 +980,7 @@ class Chain:
                 o = self.op[nf]
                 if not o.active:
                     continue
-                for ii in range(p.Ndim):
+                for ii in range(p.Nsite):
                     phi_old = self.phi[nt, ii, nf]
                     self.seed, xflip = ranf(self.seed)
                     phi_new = phi_old + (xflip - 0.5) * abs(p.shiftLoc)
@@ -635,6 +997,11 @@ class Chain:
 
     # ---- slice propagation (multiply.f90:7-16, 66-86)
     def _scale_rows(self, M, nf, nt, nflag):
+        """propU_pre: opU_mmult_R on every site (multiply.f90:7-16)."""
+        if self.p.pairing:
+            for ii in range(self.p.Nsite):
+                self._mmult_R(M, nf, ii, self.phi[nt, ii, nf], nflag)
+            return
         for ii in range(self.p.Ndim):
             M[ii, :] *= self._expalpha(nf, self.phi[nt, ii, nf], nflag)
 
@@ -740,6 +1107,7 @@ class Chain:
         """Local_sweep%sweep with is_beta=.true. (local_sweep.f90:136-161)."""
         for o in self.op:
             o.reset()
+            o.phase.reset()
         self.obs.reset()
         self.nobs = 0
         for _ in range(self.p.Nsweep):
@@ -749,6 +1117,8 @@ class Chain:
         for nf in (0, 1):
             if self.op[nf].active:
                 self.acc_sum[nf] += self.op[nf].nacc / self.op[nf].nc
+                if self.p.pairing:
+                    self.op[nf].phase.ratio()   # src/pairing/src/local_sweep.f90:158-159
 
     # ---- diagnostics (fields.f90:29-33; pole_diagnostics.f90:91-123)
     def log_weight_fields(self) -> float:
@@ -818,7 +1188,7 @@ def run(p: Params, seeds=None, confin=None, want_pole=True, callback=None):
         for c in chains:
             c.sweep_bin()
         avg = chain_average(chains)
-        if want_pole:
+        if want_pole and not p.pairing:   # the pairing program has no pole diagnostics
             avg["pole"] = [c.pole_diagnostics() for c in chains]
         bins.append(avg)
         if callback is not None:
