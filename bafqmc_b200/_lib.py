@@ -13,8 +13,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libbafqmc_b200.so"
 OK = 0
 ERRORS = {-1: "BAFQMC_EARG", -2: "BAFQMC_ECUDA", -3: "BAFQMC_EUNSUPPORTED", -4: "BAFQMC_ESTATE",
           -5: "BAFQMC_ENUMERIC"}
-OBS_SCALARS = 26
-COUNTERS = 10
+OBS_SCALARS = 32
+COUNTERS = 14
 
 
 class BafqmcError(RuntimeError):

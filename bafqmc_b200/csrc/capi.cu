@@ -1,6 +1,7 @@
 // C ABI of the B200 BAFQMC sweep (include/bafqmc_b200.h): host-side model set
 // up (lattice tables, kinetic propagators, HS factors, initial fields) and the
-// device state of a batch of chains.
+// device state of a batch of chains of the number-conserving and Nambu
+// pairing solvers.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,7 +60,9 @@ zmat zmul(const zmat& A, const zmat& B) {
 
 // exp(s * H) by scaling and squaring of the Taylor series (degree 24 after
 // scaling to norm <= 1/2; truncation error < 1e-30 relative before squaring).
-// Stands in for the ZHEEV-based opT_set (non_interact.f90:74-109).
+// Stands in for the ZHEEV-based opT_set (non_interact.f90:74-109) and, for the
+// non-Hermitian Nambu block, the ZGEEV-based exp_general_matrix
+// (src/pairing/src/non_interact.f90:131-178); it needs no eigenvectors.
 zmat expm_scaled(const zmat& H, double s) {
     const int n = H.n;
     zmat A(n);
@@ -150,11 +153,13 @@ struct HostLattice {   // lattice.f90:21-125 (Norb = 1)
 struct PointHost {
     bafqmc_point p;
     int N, Lq, Nst;
+    int pairing;   // Nambu chain: N = 2 Lq, the {b, c^dagger} block
     double dtau;
     zmat expP, expM;
     std::vector<double> phaseR;   // interleaved complex, Lq entries
     double alpha_re[2], alpha_im[2];
     int active[2];
+    int flip[2];
 };
 
 double ranf(int32_t& seed) {   // src/common/random.f90:1-11
@@ -179,7 +184,7 @@ struct bafqmc_handle {
     std::vector<long long> arena_off, phi_off;
     long long arena_total = 0, phi_total = 0;
     std::vector<int> cls_list[bq::kNumClasses];
-    int* d_cls[bq::kNumClasses] = {nullptr, nullptr};
+    int* d_cls[bq::kNumClasses] = {};
     int* d_pstart = nullptr;
     int* d_plist = nullptr;
     double* d_pout = nullptr;
@@ -212,7 +217,8 @@ struct bafqmc_handle {
 namespace {
 
 int setup_point(const bafqmc_point& p, PointHost& out) {
-    if (p.sector != 0) return fail(BAFQMC_EUNSUPPORTED, "only the number-conserving sector (0) is built");
+    if (p.sector != 0 && p.sector != 1) return fail(BAFQMC_EARG, "sector must be 0 (number-conserving) or 1 (Nambu)");
+    if (p.sector == 0 && p.delta != 0.0) return fail(BAFQMC_EARG, "delta must be 0 for the number-conserving sector");
     if (p.Lx < 1 || p.Ly < 1 || p.Ltrot < 1 || p.Nwrap < 1) return fail(BAFQMC_EARG, "non-positive lattice size");
     if (p.Ltrot % p.Nwrap != 0) return fail(BAFQMC_EARG, "Ltrot is not a multiple of Nwrap");
     if (p.U1 < -bq::kZero) return fail(BAFQMC_EARG, "U1 must be non-negative (relative-density channel)");
@@ -222,22 +228,34 @@ int setup_point(const bafqmc_point& p, PointHost& out) {
         return fail(BAFQMC_EARG, "therm field size must not exceed the lattice");
     if (p.iniType < 1 || p.iniType > 3) return fail(BAFQMC_EARG, "incorrect initype input");
     out.p = p;
+    out.pairing = p.sector == 1 ? 1 : 0;
     out.Lq = p.Lx * p.Ly;
-    out.N = out.Lq;
+    out.N = out.pairing ? 2 * out.Lq : out.Lq;
     out.Nst = p.Ltrot / p.Nwrap;
     out.dtau = p.beta / (double)p.Ltrot;
-    if (out.N > bq::class_nmax(bq::kNumClasses - 1))
+    if (bq::class_of(out.N, out.pairing) < 0)
         return fail(BAFQMC_EUNSUPPORTED, "Ndim above the largest shared-memory class of this build");
     HostLattice lat(p.Lx, p.Ly);
-    const int n = out.N;
+    const int ns = out.Lq, n = out.N;
     zmat H(n);   // def_hamT (non_interact.f90:33-72), t = 1
-    for (int ii = 0; ii < n; ++ii)
+    for (int ii = 0; ii < ns; ++ii)
         for (int nb = 0; nb < 3; ++nb) {
             const int jj = lat.bonds[3 * ii + nb];
             H.re(ii, jj) += 1.0;
             H.re(jj, ii) += 1.0;
+            if (out.pairing) {   // c^dagger block: -t on the transposed bond (src/pairing/src/non_interact.f90:61-66)
+                H.re(ns + jj, ns + ii) -= 1.0;
+                H.re(ns + ii, ns + jj) -= 1.0;
+            }
         }
-    for (int ii = 0; ii < n; ++ii) H.re(ii, ii) -= p.mu;
+    for (int ii = 0; ii < ns; ++ii) {
+        H.re(ii, ii) -= p.mu;
+        if (out.pairing) {   // pairing (:70-81) and chemical potential (:83-94) of the {b, c^dagger} block
+            H.re(ii, ns + ii) += p.delta;
+            H.re(ns + ii, ii) -= p.delta;
+            H.re(ns + ii, ns + ii) += p.mu;
+        }
+    }
     out.expP = expm_scaled(H, -out.dtau);
     out.expM = expm_scaled(H, out.dtau);
     out.phaseR.assign(2 * (size_t)out.Lq, 0.0);
@@ -256,22 +274,57 @@ int setup_point(const bafqmc_point& p, PointHost& out) {
         if (U[ch] > bq::kZero) out.alpha_im[ch] = std::sqrt(2.0 * U[ch] * out.dtau);
         out.active[ch] = std::fabs(U[ch]) > bq::kZero ? 1 : 0;
     }
+    // Nambu sector factors on c^dagger: e^{+alpha phi} for U1, e^{-alpha phi} for U2
+    // (src/pairing/src/operator_Hubbard.f90:155-166)
+    out.flip[0] = 0;
+    out.flip[1] = out.pairing;
     return BAFQMC_OK;
 }
 
-int class_of(int n) {
-    for (int c = 0; c < bq::kNumClasses; ++c)
-        if (n <= bq::class_nmax(c)) return c;
-    return -1;
+int point_class(const PointHost& ph) { return bq::class_of(ph.N, ph.pairing); }
+
+// Device descriptor of a point whose expP | expM | phase table start at mats.
+PointDev point_dev(const PointHost& ph, const double2* mats) {
+    PointDev d;
+    std::memset(&d, 0, sizeof d);
+    const size_t nn = (size_t)ph.N * ph.N;
+    d.N = ph.N;
+    d.L = ph.p.Ltrot;
+    d.Nwrap = ph.p.Nwrap;
+    d.Nst = ph.Nst;
+    d.Lq = ph.Lq;
+    d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
+    d.Lx = ph.p.Lx;
+    d.Ly = ph.p.Ly;
+    d.Ns = ph.Lq;
+    d.pairing = ph.pairing;
+    for (int ch = 0; ch < 2; ++ch) {
+        d.active[ch] = ph.active[ch];
+        d.flip[ch] = ph.flip[ch];
+        d.alpha_re[ch] = ph.alpha_re[ch];
+        d.alpha_im[ch] = ph.alpha_im[ch];
+    }
+    d.shiftLoc = ph.p.shiftLoc;
+    d.U1 = ph.p.U1;
+    d.U2 = ph.p.U2;
+    d.RT = 1.0;
+    d.mu = ph.p.mu;
+    d.Delta = ph.pairing ? ph.p.delta : 0.0;
+    d.expP = mats;
+    d.expM = mats + nn;
+    d.phaseR = mats + 2 * nn;
+    return d;
 }
 
 void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
-                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_cls[0], h->d_cls[1]};
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (int c = 0; c < bq::kNumClasses; ++c)
+        if (h->d_cls[c]) cudaFree(h->d_cls[c]);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -315,8 +368,8 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         h->arena_off[c] = h->arena_total;
         h->arena_total += bq::arena_size(ph.N, ph.Nst);
         h->phi_off[c] = h->phi_total;
-        h->phi_total += (long long)ph.p.Ltrot * ph.N * 2;
-        h->cls_list[class_of(ph.N)].push_back(c);
+        h->phi_total += (long long)ph.p.Ltrot * ph.Lq * 2;
+        h->cls_list[point_class(ph)].push_back(c);
         per_point[p].push_back(c);
     }
     cudaError_t e = cudaSetDevice(device);
@@ -358,31 +411,7 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
     if ((e = cudaMemcpy(h->d_mats, mats.data(), sizeof(double2) * mat_total, cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(e, "upload mats");
     std::vector<PointDev> pd(npts);
-    for (int i = 0; i < npts; ++i) {
-        const PointHost& ph = h->pts[i];
-        PointDev& d = pd[i];
-        const size_t nn = (size_t)ph.N * ph.N;
-        d.N = ph.N;
-        d.L = ph.p.Ltrot;
-        d.Nwrap = ph.p.Nwrap;
-        d.Nst = ph.Nst;
-        d.Lq = ph.Lq;
-        d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
-        d.Lx = ph.p.Lx;
-        d.Ly = ph.p.Ly;
-        for (int ch = 0; ch < 2; ++ch) {
-            d.active[ch] = ph.active[ch];
-            d.alpha_re[ch] = ph.alpha_re[ch];
-            d.alpha_im[ch] = ph.alpha_im[ch];
-        }
-        d.shiftLoc = ph.p.shiftLoc;
-        d.U1 = ph.p.U1;
-        d.U2 = ph.p.U2;
-        d.RT = 1.0;
-        d.expP = h->d_mats + mat_off[i];
-        d.expM = h->d_mats + mat_off[i] + nn;
-        d.phaseR = h->d_mats + mat_off[i] + 2 * nn;
-    }
+    for (int i = 0; i < npts; ++i) pd[i] = point_dev(h->pts[i], h->d_mats + mat_off[i]);
     std::vector<ChainDev> cd(nchains);
     for (int c = 0; c < nchains; ++c) {
         cd[c].point = chain_point[c];
@@ -487,7 +516,7 @@ int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds) {
                 }
         adv[c] = s;
         double* out = phi.data() + h->phi_off[c];   // conf_transfer (fields.f90:156-234)
-        const int n = ph.N;
+        const int n = ph.Lq;
         for (int nt = 0; nt < p.LtrotTherm; ++nt)
             for (int ny = 1; ny <= p.Ly; ++ny)
                 for (int nx = 1; nx <= p.Lx; ++nx) {
@@ -595,7 +624,8 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out) {
     CK(cudaMemcpyAsync(fn.data(), h->d_tmp, sizeof(double) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    for (int c = 0; c < h->nchains; ++c) out[c] = fn[c] - 2.0 * sc[c].logdetM;
+    for (int c = 0; c < h->nchains; ++c)
+        out[c] = h->pts[h->chain_point[c]].pairing ? std::nan("") : fn[c] - 2.0 * sc[c].logdetM;
     return BAFQMC_OK;
 }
 
@@ -617,6 +647,10 @@ int bafqmc_counters(bafqmc_handle* h, double* out) {
         o[7] = (double)sc[c].seed;
         o[8] = (double)sc[c].nobs;
         o[9] = 0.0;
+        o[10] = sc[c].prop_tot[0];
+        o[11] = sc[c].prop_tot[1];
+        o[12] = sc[c].acc_tot[0];
+        o[13] = sc[c].acc_tot[1];
     }
     return BAFQMC_OK;
 }
@@ -702,7 +736,7 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     PointHost ph;
     int rc = setup_point(*pt, ph);
     if (rc != BAFQMC_OK) return rc;
-    const int n = ph.N, cls = class_of(n);
+    const int n = ph.N, cls = point_class(ph);
     const int stride = bq::kObsScalars + ph.Lq;
     const long long asz = bq::arena_size(n, ph.Nst);
     // scratch layout: point | chains | scalars | index list | matrices | observables | arenas
@@ -727,28 +761,7 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // descriptors staged on the host, copied into the array in one transfer
     std::vector<unsigned char> stage(o_ob, 0);
-    PointDev d;
-    d.N = n;
-    d.L = ph.p.Ltrot;
-    d.Nwrap = ph.p.Nwrap;
-    d.Nst = ph.Nst;
-    d.Lq = ph.Lq;
-    d.hasK = (ph.p.Lx % 3 == 0 && ph.p.Ly % 3 == 0) ? 1 : 0;
-    d.Lx = ph.p.Lx;
-    d.Ly = ph.p.Ly;
-    for (int ch = 0; ch < 2; ++ch) {
-        d.active[ch] = ph.active[ch];
-        d.alpha_re[ch] = ph.alpha_re[ch];
-        d.alpha_im[ch] = ph.alpha_im[ch];
-    }
-    d.shiftLoc = ph.p.shiftLoc;
-    d.U1 = ph.p.U1;
-    d.U2 = ph.p.U2;
-    d.RT = 1.0;
-    const double2* mats = reinterpret_cast<const double2*>(base + o_mt);
-    d.expP = mats;
-    d.expM = mats + nn;
-    d.phaseR = mats + 2 * nn;
+    const PointDev d = point_dev(ph, reinterpret_cast<const double2*>(base + o_mt));
     std::memcpy(stage.data() + o_pt, &d, sizeof d);
     ChainDev* cd = reinterpret_cast<ChainDev*>(stage.data() + o_ch);
     int* ix = reinterpret_cast<int*>(stage.data() + o_ix);
@@ -756,7 +769,7 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
         cd[c].point = 0;
         cd[c].pad = 0;
         cd[c].arena_off = (long long)c * asz;
-        cd[c].phi_off = (long long)c * ph.p.Ltrot * n * 2;
+        cd[c].phi_off = (long long)c * ph.p.Ltrot * ph.Lq * 2;
         ix[c] = c;
     }
     std::memcpy(stage.data() + o_mt, ph.expP.a.data(), sizeof(double2) * nn);

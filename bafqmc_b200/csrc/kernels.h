@@ -22,10 +22,12 @@ struct KernelArgs {
     int timers;   // nonzero: accumulate per-phase SM cycles into ChainScalars::cyc
 };
 
-// size classes of the fused sweep kernel: 0 -> N <= 16, 1 -> N <= 36
-constexpr int kNumClasses = 2;
+// kernel classes of the fused sweep: bit 0 selects the shared-memory size
+// (N <= 16 or N <= 36), bit 1 the sector (0 number-conserving, 1 Nambu)
+constexpr int kNumClasses = 4;
 int class_nmax(int cls);
 size_t smem_bytes(int cls);
+int class_of(int n, int pairing);   // -1 if no class holds n
 
 cudaError_t upload_pow_table(const uint32_t* tab, int count);
 cudaError_t launch_sweep(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st);

@@ -1,11 +1,20 @@
 // Device-side data layout and per-chain sweep routines for the BAFQMC
-// number-conserving solver (src/number_conserving/src/*.f90).
+// number-conserving solver (src/number_conserving/src/*.f90) and the Nambu
+// pairing solver (src/pairing/src/*.f90).
 //
 // One CTA owns one Markov chain for a whole sweep.  Shared memory holds four
 // N x N complex matrices: G, the current U factor of the propagated side, and
 // two workspaces that hold e^{-dtau K} / e^{+dtau K} while slices are
 // propagated and serve the QR stabilisation at wrap slices.  The stored UDV
 // slots, the V/D factors and the fields stay in HBM.
+//
+// Nambu chains.  The reference's 4Ns matrices (sectors b, c, b^dagger,
+// c^dagger) are block diagonal: the kinetic matrix couples only b with
+// c^dagger and c with b^dagger (src/pairing/src/non_interact.f90:44-93), the
+// HS factors are diagonal, and for real t, Delta and the reference's HS
+// constants the {c, b^dagger} block is the complex conjugate of the
+// {b, c^dagger} block.  A Nambu chain therefore propagates only the
+// {b, c^dagger} block, N = 2Ns, index i = b_i and Ns+i = c^dagger_i.
 #pragma once
 #include "linalg.cuh"
 
@@ -27,15 +36,20 @@ enum ObsIndex {
     O_DEN_UPUP = 20,    // re, im  (sum over r of den_corr_up(r)/Lq == FFT at k=0)
     O_DEN_DODO = 22,    // re, im
     O_DEN_UPDO = 24,    // re, im
-    O_SITE = 26,        // Lq values of density_site_total
+    // written by the Nambu solver only (src/pairing/src/obser_equal.f90:10-15)
+    O_DENSITY = 26, O_LOCAL_NUMSQUARE, O_PAIR_EQUAL, O_PAIRING_ENERGY, O_CHEMICAL_ENERGY, O_GRAND_ENERGY,
+    O_SITE = 32,        // Lq values of density_site_total
 };
-constexpr int kObsScalars = 26;
+constexpr int kObsScalars = 32;
 
 struct PointDev {
     int N, L, Nwrap, Nst, Lq, hasK, Lx, Ly;
+    int Ns;         // lattice sites (fields per slice and channel); N = Ns, or 2Ns for a Nambu chain
+    int pairing;    // 1: Nambu chain propagating the {b, c^dagger} block
     int active[2];
+    int flip[2];    // Nambu: the c^dagger factor of channel ch is e^{-alpha phi} (U2) rather than e^{+alpha phi} (U1)
     double alpha_re[2], alpha_im[2];
-    double shiftLoc, U1, U2, RT;
+    double shiftLoc, U1, U2, RT, mu, Delta;
     const cplx* expP;      // e^{-dtau K}, N*N row-major
     const cplx* expM;      // e^{+dtau K}
     const cplx* phaseR;    // exp(i K.r) for the Lq lattice displacements r (only if hasK)
@@ -52,6 +66,8 @@ struct ChainScalars {
     double logdetM;             // sum log D of the last (I-B) factorisation at tau = beta
     double pad;
     long long cyc[4];           // SM cycles per phase: local updates, slice products, measurement, wraps
+    double prop_tot[2];         // proposals over all bins (PhaseCounter%count_proposed)
+    double acc_tot[2];          // accepted over all bins (PhaseCounter%count_accepted)
 };
 
 struct ChainDev {

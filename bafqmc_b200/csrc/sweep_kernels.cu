@@ -1,11 +1,13 @@
-// Sweep kernels for the BAFQMC number-conserving solver on sm_100a.
+// Sweep kernels for the BAFQMC number-conserving and Nambu pairing solvers on
+// sm_100a.
 //
 // One CTA = one Markov chain.  sweep_kernel runs one full sweep (left then
 // right traversal of imaginary time, local_sweep.f90:96-134 with is_beta
 // = .true.) including every local update, slice propagation, stabilisation
 // and equal-time measurement of that chain.  pre_kernel builds the right UDV
 // slots and G(beta) (local_sweep.f90:80-94); warmup_kernel is the prior-only
-// warm-up (local_sweep.f90:64-78).
+// warm-up (local_sweep.f90:64-78).  Both sweep kernels are instantiated per
+// shared-memory size class and per sector (PAIR: Nambu chains).
 #include "sweep.cuh"
 #include "kernels.h"
 
@@ -30,7 +32,8 @@ struct Smem {
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr int KB = Cfg<NMAX>::KB;
     static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
-    static constexpr size_t oEao = oDelta + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
+    static constexpr size_t oDelta2 = oDelta + VC;
+    static constexpr size_t oEao = oDelta2 + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
     static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + KB * sizeof(cplx);
     static constexpr size_t oP = oCbc + 4 * sizeof(cplx);
     static constexpr size_t oRg = oP + ((sizeof(PointDev) + 15) / 16) * 16;
@@ -51,6 +54,7 @@ struct Smem {
     DEVI cplx* col(int m) const { return at<cplx>(oCol) + m * NMAX; }   // column of the m-th site of a block
     DEVI cplx* row(int m) const { return at<cplx>(oRow) + m * NMAX; }   // row of the m-th site of a block
     DEVI cplx* delta() const { return at<cplx>(oDelta); }
+    DEVI cplx* delta2() const { return at<cplx>(oDelta2); }   // Nambu: Delta of the c^dagger index
     DEVI cplx* eao() const { return at<cplx>(oEao); }
     DEVI cplx* ean() const { return at<cplx>(oEan); }
     DEVI cplx* ebo() const { return at<cplx>(oEbo); }
@@ -339,6 +343,173 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
 }
 
 // ---------------------------------------------------------------------------
+// Nambu local update of one channel over all sites of one slice, fused with
+// the V-wrap of G (LocalU_prop_L / LocalU_prop_R and LocalU_metro,
+// src/pairing/src/localU.f90:33-149), on the {b, c^dagger} block.
+//
+// For site i the reference forms the 4x4 P = I + Delta (I - G[isec,isec]) over
+// the sectors b, c, b^dagger, c^dagger of the site, takes
+// ratio_det = det(P)^(-1/2), and on acceptance applies the rank-4 update
+// G -= G[:,isec] P^{-1} Delta (I[isec,:] - G[isec,:]).  With the block
+// structure P splits into the 2x2 block P1 on {b_i, c^dagger_i} and its
+// complex conjugate on {c_i, b^dagger_i}, so det(P) = |det P1|^2 (real and
+// positive: ratio_det = 1/|det P1|, and the ratio's phase that PhaseCounter
+// records is zero), and the update of the block is the rank-2 term
+// G1 -= G1[:,s] P1^{-1} D1 (I[s,:] - G1[s,:]), s = (i, Ns+i).
+//
+// Sites are sequential.  Every thread keeps the same MAXE elements of G in
+// registers for the whole slice; per site the owners of rows and columns i
+// and Ns+i stage them in shared memory (double-buffered by site parity), one
+// barrier, then every thread makes the same decision from the staged 2x2 and
+// updates its own elements.
+template <int NMAX, bool LEFT>
+COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
+    constexpr int MAXE = Cfg<NMAX>::MAXE;
+    auto& s = x.s;
+    const int n = x.n, ns = x.P().Ns, tid = threadIdx.x;
+    const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
+    const double shift = fabs(x.P().shiftLoc);
+    const bool flip = x.P().flip[ch] != 0;
+    const bool total = (ch == 1);
+    const uint32_t s0 = *s.seed();
+    double* phis = x.phi + (long)slice * ns * 2;
+    cplx* G = s.G();
+
+    // per-site proposals (opU_get_delta, src/pairing/src/operator_Hubbard.f90:100-137)
+    for (int i = tid; i < ns; i += blockDim.x) {
+        const int m = LEFT ? (ns - 1 - i) : i;
+        const double xflip = lcg_u(lcg_mul(c_apow[2 * m + 1], s0));
+        const double rnd = lcg_u(lcg_mul(c_apow[2 * m + 2], s0));
+        const double po = phis[i * 2 + ch];
+        const double pn = po + (xflip - 0.5) * shift;
+        const double go = exp(-0.5 * po * po), gn = exp(-0.5 * pn * pn);
+        const cplx eo = cexpz(cmk(ar * po, ai * po)), en = cexpz(cmk(ar * pn, ai * pn));
+        const double dphi = pn - po;
+        const cplx dp = csub(cexpz(cmk(ar * dphi, ai * dphi)), cmk(1.0, 0.0));
+        const cplx dm = csub(cexpz(cmk(-(ar * dphi), -(ai * dphi))), cmk(1.0, 0.0));
+        s.eao()[i] = eo;
+        s.ean()[i] = en;
+        s.ebo()[i] = cexpz(cmk(-(ar * po), -(ai * po)));
+        s.ebn()[i] = cexpz(cmk(-(ar * pn), -(ai * pn)));
+        s.delta()[i] = dp;                  // b_i: e^{+alpha dphi} - 1 in both channels
+        s.delta2()[i] = flip ? dm : dp;     // c^dagger_i
+        // |ratio_gaussian * ratio_constant|; ratio_constant = e^{alpha(phi_old - phi_new)} for U2
+        const double rc = total ? cabsv(cdiv(eo, en)) : 1.0;
+        s.rg()[i] = (gn / go) * rc;
+        s.u2()[i] = rnd;
+        s.phin()[i] = pn;
+        s.accf()[i] = 0;
+    }
+    __syncthreads();
+
+    cplx g[MAXE];
+    int er[MAXE], ec[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = tid + k * blockDim.x;
+        er[k] = (e < n * n) ? e / n : -1;
+        ec[k] = (e < n * n) ? e - (e / n) * n : -1;
+        g[k] = (e < n * n) ? G[e] : cmk(0.0, 0.0);
+    }
+    for (int q = 0; q < ns; ++q) {
+        const int i = LEFT ? ns - 1 - q : q;
+        const int a = i, b = ns + i;
+        const int buf = (q & 1) * 2;
+        cplx* xa = s.col(buf);
+        cplx* xb = s.col(buf + 1);
+        cplx* ya = s.row(buf);
+        cplx* yb = s.row(buf + 1);
+        if (!LEFT) {   // opU_mmult_R(+1) then opU_mmult_L(-1) with the current field
+            const cplx ep = s.eao()[i], em = s.ebo()[i];
+#pragma unroll
+            for (int k = 0; k < MAXE; ++k) {
+                if (er[k] == a) g[k] = cmul(ep, g[k]);
+                else if (er[k] == b) g[k] = cmul(flip ? em : ep, g[k]);
+                if (ec[k] == a) g[k] = cmul(g[k], em);
+                else if (ec[k] == b) g[k] = cmul(g[k], flip ? ep : em);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k) {
+            if (ec[k] == a) xa[er[k]] = g[k];
+            if (ec[k] == b) xb[er[k]] = g[k];
+            if (er[k] == a) ya[ec[k]] = g[k];
+            if (er[k] == b) yb[ec[k]] = g[k];
+        }
+        __syncthreads();
+        // P1 = I + D1 (I - G1[s,s]);  accept if |rg rc| / |det P1| > u
+        const cplx d0 = s.delta()[i], d1 = s.delta2()[i];
+        const cplx gaa = ya[a], gab = ya[b], gba = yb[a], gbb = yb[b];
+        const cplx p00 = cadd(cmk(1.0, 0.0), cmul(d0, cmk(1.0 - gaa.x, -gaa.y)));
+        const cplx p01 = cmul(d0, cmk(-gab.x, -gab.y));
+        const cplx p10 = cmul(d1, cmk(-gba.x, -gba.y));
+        const cplx p11 = cadd(cmk(1.0, 0.0), cmul(d1, cmk(1.0 - gbb.x, -gbb.y)));
+        const cplx det = csub(cmul(p00, p11), cmul(p01, p10));
+        const double det2 = det.x * det.x + det.y * det.y;
+        const bool accept = s.rg()[i] / sqrt(det2) > s.u2()[i];
+        if (tid == 0) s.accf()[i] = accept ? 1 : 0;
+        if (accept) {
+            // M = P1^{-1} D1, P1^{-1} = adj(P1) conj(det) / |det|^2
+            const cplx id = cmk(det.x / det2, -det.y / det2);
+            const cplx m00 = cmul(cmul(p11, id), d0);
+            const cplx m01 = cmul(cmul(cmk(-p01.x, -p01.y), id), d1);
+            const cplx m10 = cmul(cmul(cmk(-p10.x, -p10.y), id), d0);
+            const cplx m11 = cmul(cmul(p00, id), d1);
+#pragma unroll
+            for (int k = 0; k < MAXE; ++k) {
+                if (er[k] < 0) continue;
+                const int r = er[k], c = ec[k];
+                const cplx ca = xa[r], cb = xb[r];
+                const cplx x0 = cadd(cmul(ca, m00), cmul(cb, m10));
+                const cplx x1 = cadd(cmul(ca, m01), cmul(cb, m11));
+                const cplx y0 = cmk(((c == a) ? 1.0 : 0.0) - ya[c].x, -ya[c].y);
+                const cplx y1 = cmk(((c == b) ? 1.0 : 0.0) - yb[c].x, -yb[c].y);
+                g[k] = csub(g[k], cadd(cmul(x0, y0), cmul(x1, y1)));
+            }
+        }
+        if (LEFT) {   // opU_mmult_L(+1) then opU_mmult_R(-1) with the final field
+            const cplx ep = accept ? s.ean()[i] : s.eao()[i];
+            const cplx em = accept ? s.ebn()[i] : s.ebo()[i];
+#pragma unroll
+            for (int k = 0; k < MAXE; ++k) {
+                if (ec[k] == a) g[k] = cmul(g[k], ep);
+                else if (ec[k] == b) g[k] = cmul(g[k], flip ? em : ep);
+                if (er[k] == a) g[k] = cmul(em, g[k]);
+                else if (er[k] == b) g[k] = cmul(flip ? ep : em, g[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k)
+        if (er[k] >= 0) G[tid + k * blockDim.x] = g[k];
+    __syncthreads();
+    for (int i = tid; i < ns; i += blockDim.x)
+        if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
+    if (tid == 0) {
+        long long na = 0;
+        for (int i = 0; i < ns; ++i) na += s.accf()[i];
+        x.sc->nacc[ch] += na;
+        x.sc->nc[ch] += ns;
+        *s.seed() = lcg_mul(c_apow[2 * ns], s0);
+    }
+    // U_L columns (left) or U_R rows (right) of both indices of every site, final fields
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int e = tid + k * blockDim.x;
+        if (e < n * n) {
+            const int idx = LEFT ? ec[k] : er[k];
+            const int site = idx < ns ? idx : idx - ns;
+            const bool acc = s.accf()[site] != 0;
+            const cplx ep = acc ? s.ean()[site] : s.eao()[site];
+            const cplx em = acc ? s.ebn()[site] : s.ebo()[site];
+            const cplx f = (idx >= ns && flip) ? em : ep;
+            s.U()[e] = LEFT ? cmul(s.U()[e], f) : cmul(f, s.U()[e]);
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
 // propT_L / propT_R (multiply.f90:72-86): G <- e^{+dK} G e^{-dK}, U_L <- U_L e^{-dK}
 // for the left traversal; G <- e^{-dK} G e^{+dK}, U_R <- e^{-dK} U_R for the
 // right.  e^{-dtau K} is in W1, e^{+dtau K} in W2.
@@ -456,6 +627,131 @@ COLD void measure(Ctx<NMAX> x) {
         o[O_DEN_DODO + 1] -= v[7] / lq;
         o[O_DEN_UPDO] += v[8] / lq;
         o[O_DEN_UPDO + 1] += v[9] / lq;
+        x.sc->nobs += 1;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Nambu equal-time estimators (Obs_equal_calc, src/pairing/src/obser_equal.f90:112-271)
+// from the {b, c^dagger} block.  With A = G1[b,b], B = G1[b,c^dagger],
+// C = G1[c^dagger,b], D = G1[c^dagger,c^dagger], the reference's sixteen
+// sub-blocks are A, -B, conj(A), -conj(B), conj(C), -conj(D), C, -D and zeros:
+// n_b(i) = -conj(D_ii), n_c(i) = -D_ii, and every c-flavour sum is the complex
+// conjugate of the b-flavour sum.  Pair terms:
+//   Dbb(i,j) = n_b(i) n_b(j) - conj(D_ij) A_ij,  Dbc(i,j) = n_b(i) n_c(j) - conj(C_ij) B_ij,
+//   Dcc = conj(Dbb), Dcb = conj(Dbc).
+template <int NMAX>
+COLD void measure_pair(Ctx<NMAX> x) {
+    auto& s = x.s;
+    const PointDev& P = x.P();
+    const int n = x.n, ns = P.Ns, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
+    const double lq = (double)P.Lq, lq2 = lq * lq, dns = (double)ns;
+    const cplx* G = s.G();
+    const cplx* ph = s.ph();
+    const bool hasK = P.hasK;
+    // v: 0-1 sum Dbb, 2-3 sum Dbc, 4 sum |D_ij|^2, 5-6 sf_K, 7-8 dw_K, 9 kinetic bonds,
+    //    10 sum Re n_b, 11 sum Re Dbc(i,i), 12 sum Re n_b^2, 13 sum Re Dbb(i,i),
+    //    14 sum Re(C_ii - B_ii), 15-16 tr B, 17-18 tr C
+    double v[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) v[k] = 0.0;
+    for (int e = tid; e < ns * ns; e += blockDim.x) {
+        const int i = e / ns, j = e - (e / ns) * ns;
+        const cplx A = G[i * n + j], B = G[i * n + ns + j], C = G[(ns + i) * n + j], D = G[(ns + i) * n + ns + j];
+        const cplx di = G[(ns + i) * n + ns + i], dj = G[(ns + j) * n + ns + j];
+        const cplx nbi = cmk(-di.x, di.y), nbj = cmk(-dj.x, dj.y), ncj = cmk(-dj.x, -dj.y);
+        const cplx dbb = csub(cmul(nbi, nbj), cmul(cconj(D), A));
+        const cplx dbc = csub(cmul(nbi, ncj), cmul(cconj(C), B));
+        v[0] += dbb.x;
+        v[1] += dbb.y;
+        v[2] += dbc.x;
+        v[3] += dbc.y;
+        v[4] += D.x * D.x + D.y * D.y;
+        if (hasK) {
+            const int ix = i % lx, iy = i / lx, jx = j % lx, jy = j / lx;
+            int dx = ix - jx, dy = iy - jy;
+            dx += (dx < 0) ? lx : 0;
+            dy += (dy < 0) ? ly : 0;
+            const cplx p = ph[dy * lx + dx];
+            const double sfr = -2.0 * D.x;                 // G_bdag_b + G_cdag_c
+            const double dwr = 2.0 * (dbb.x + dbc.x);      // Dbb + Dcc + Dbc + Dcb
+            v[5] += p.x * sfr;
+            v[6] += p.y * sfr;
+            v[7] += p.x * dwr;
+            v[8] += p.y * dwr;
+        }
+    }
+    for (int e = tid; e < 3 * ns; e += blockDim.x) {   // bonds (x+1,y), (x,y+1), (x-1,y+1)
+        const int i = e / 3, nb = e - (e / 3) * 3;
+        const int ix = i % lx, iy = i / lx;
+        const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
+        const int jy = (nb == 0) ? iy : (iy + 1) % ly;
+        const int jj = jy * lx + jx;
+        v[9] += -2.0 * (G[(ns + i) * n + ns + jj].x + G[(ns + jj) * n + ns + i].x);
+    }
+    for (int i = tid; i < ns; i += blockDim.x) {
+        const cplx A = G[i * n + i], B = G[i * n + ns + i], C = G[(ns + i) * n + i], D = G[(ns + i) * n + ns + i];
+        const cplx nb = cmk(-D.x, D.y);
+        const double nbnc = D.x * D.x + D.y * D.y;          // n_b n_c = |D_ii|^2
+        const cplx cb = cmul(cconj(C), B);
+        const cplx dbb = cadd(cmul(nb, nb), cmul(nb, A));
+        v[10] += nb.x;
+        v[11] += nbnc - cb.x;
+        v[12] += nb.x * nb.x - nb.y * nb.y;
+        v[13] += dbb.x;
+        v[14] += C.x - B.x;
+        v[15] += B.x;
+        v[16] += B.y;
+        v[17] += C.x;
+        v[18] += C.y;
+        s.obs()[O_SITE + i] += 2.0 * nb.x;
+    }
+    block_sum<19>(v, s.red());
+    if (tid == 0) {
+        double* o = s.obs();
+        const double dens = 2.0 * v[10] / dns;
+        const double dbl = v[11] / dns;
+        const double pair = v[14] / dns;
+        const double kin = P.RT * v[9] / dns;
+        const double inter = (P.U1 + P.U2) * (2.0 * v[13]) / dns + 2.0 * (P.U2 - P.U1) * dbl;
+        const double epair = P.Delta * pair;
+        const double chem = -P.mu * dens;
+        const double energy = kin + inter + epair;
+        // tr C tr B; psf_Gamma = (-conj(trC trB) + sum |D_ij|^2) / Lq^2
+        const double tcb_re = v[17] * v[15] - v[18] * v[16], tcb_im = v[17] * v[16] + v[18] * v[15];
+        o[O_DENSITY_UP] += v[10] / dns;
+        o[O_DENSITY_DO] += v[10] / dns;
+        o[O_DENSITY] += dens;
+        o[O_DENSITY_TOTAL] += dens;
+        o[O_NUM_UP] += v[10];
+        o[O_NUM_DO] += v[10];
+        o[O_DOUBLEOCC] += dbl;
+        o[O_SQUAREOCC] += 2.0 * v[12] / dns;
+        o[O_LOCAL_NUMSQUARE] += 2.0 * v[13] / dns;
+        o[O_PAIR_EQUAL] += pair;
+        o[O_NUMSQUARE_UP] += v[0];
+        o[O_NUMSQUARE_DO] += v[0];
+        o[O_ONSITE_N2_UP] += v[13];
+        o[O_ONSITE_N2_DO] += v[13];
+        o[O_KINETIC] += kin;
+        o[O_INTERACTION] += inter;
+        o[O_PAIRING_ENERGY] += epair;
+        o[O_CHEMICAL_ENERGY] += chem;
+        o[O_ENERGY] += energy;
+        o[O_GRAND_ENERGY] += energy + chem;
+        o[O_SF_K] += v[5] / lq2;
+        o[O_SF_K + 1] += v[6] / lq2;
+        o[O_DW_K] += v[7] / lq2;
+        o[O_DW_K + 1] += v[8] / lq2;
+        o[O_PSF_GAMMA] += (v[4] - tcb_re) / lq2;
+        o[O_PSF_GAMMA + 1] += tcb_im / lq2;
+        o[O_DEN_UPUP] += v[0] / lq;
+        o[O_DEN_UPUP + 1] += v[1] / lq;
+        o[O_DEN_DODO] += v[0] / lq;
+        o[O_DEN_DODO + 1] -= v[1] / lq;
+        o[O_DEN_UPDO] += v[2] / lq;
+        o[O_DEN_UPDO + 1] += v[3] / lq;
         x.sc->nobs += 1;
     }
     __syncthreads();
@@ -667,8 +963,19 @@ DEVI void flush_obs(Ctx<NMAX>& x, double* gobs) {
     for (int k = threadIdx.x; k < kObsScalars + x.P().Lq; k += blockDim.x) gobs[k] += x.s.obs()[k];
 }
 
+template <int NMAX, bool PAIR, bool LEFT>
+DEVI void prop_any(Ctx<NMAX>& x, int ch, int slice) {
+    if (PAIR) prop_channel_pair<NMAX, LEFT>(x, ch, slice);
+    else prop_channel<NMAX, LEFT>(x, ch, slice);
+}
+template <int NMAX, bool PAIR>
+DEVI void measure_any(Ctx<NMAX>& x) {
+    if (PAIR) measure_pair<NMAX>(x);
+    else measure<NMAX>(x);
+}
+
 // one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
-template <int NMAX>
+template <int NMAX, bool PAIR>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs ka, const int* idx, int count) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
@@ -700,12 +1007,12 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
             wrap_L(x, nt);
             lap(3);
         }
-        measure(x);
+        measure_any<NMAX, PAIR>(x);
         lap(2);
         slice_products<NMAX, true>(x);
         lap(1);
-        if (x.P().active[1]) prop_channel<NMAX, true>(x, 1, nt - 1);
-        if (x.P().active[0]) prop_channel<NMAX, true>(x, 0, nt - 1);
+        if (x.P().active[1]) prop_any<NMAX, PAIR, true>(x, 1, nt - 1);
+        if (x.P().active[0]) prop_any<NMAX, PAIR, true>(x, 0, nt - 1);
         lap(0);
     }
     wrap_L(x, 0);
@@ -717,8 +1024,8 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
     wrap_R(x, 0);
     lap(3);
     for (int nt = 1; nt <= L; ++nt) {
-        if (x.P().active[0]) prop_channel<NMAX, false>(x, 0, nt - 1);
-        if (x.P().active[1]) prop_channel<NMAX, false>(x, 1, nt - 1);
+        if (x.P().active[0]) prop_any<NMAX, PAIR, false>(x, 0, nt - 1);
+        if (x.P().active[1]) prop_any<NMAX, PAIR, false>(x, 1, nt - 1);
         lap(0);
         slice_products<NMAX, false>(x);
         lap(1);
@@ -726,7 +1033,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
             wrap_R(x, nt);
             lap(3);
         }
-        measure(x);
+        measure_any<NMAX, PAIR>(x);
         lap(2);
     }
     gcopy(x.A().URc, s.U(), n * n);
@@ -738,8 +1045,10 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
 }
 
 // Local_sweep_pre (local_sweep.f90:80-94) with Prop_make's identities
-// (process_matrix.f90:37-47).
-template <int NMAX>
+// (process_matrix.f90:37-47).  propU_pre scales the rows of U_R by the HS
+// factors (multiply.f90:7-16); for a Nambu chain row Ns+i (c^dagger_i) takes
+// e^{-alpha phi} in the U2 channel (src/pairing/src/operator_Hubbard.f90:155-166).
+template <int NMAX, bool PAIR>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs ka, const int* idx, int count) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
@@ -763,14 +1072,20 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs k
     gcopy(x.A().DRs(0), x.A().DRc, n);
     gcopy(s.W1(), x.P().expP, n * n);
     __syncthreads();
+    const int ns = x.P().Ns;
     for (int nt = 1; nt <= L; ++nt) {
-        const double* ph = x.phi + (long)(nt - 1) * n * 2;
+        const double* ph = x.phi + (long)(nt - 1) * ns * 2;
         for (int ch = 0; ch < 2; ++ch) {
             if (!x.P().active[ch]) continue;
             const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
+            const bool flip = x.P().flip[ch] != 0;
             for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-                const double p = ph[(e / n) * 2 + ch];
-                s.U()[e] = cmul(cexpz(cmk(ar * p, ai * p)), s.U()[e]);
+                const int r = e / n;
+                const int site = (PAIR && r >= ns) ? r - ns : r;
+                const double p = ph[site * 2 + ch];
+                const bool neg = PAIR && r >= ns && flip;
+                const cplx f = neg ? cexpz(cmk(-(ar * p), -(ai * p))) : cexpz(cmk(ar * p, ai * p));
+                s.U()[e] = cmul(f, s.U()[e]);
             }
             __syncthreads();
         }
@@ -816,7 +1131,7 @@ __global__ void warmup_kernel(KernelArgs ka, int nwarm) {
         nact = a;
     }
     __syncthreads();
-    const int A = nact, n = P.N, L = P.L;
+    const int A = nact, n = P.Ns, L = P.L;
     const uint32_t s0 = sc->seed;
     const unsigned long long per_sweep = (unsigned long long)L * A * n;
     const uint32_t step = lcg_pow(2ull * per_sweep);
@@ -876,8 +1191,11 @@ __global__ void bin_finish_kernel(KernelArgs ka) {
     for (int k = threadIdx.x; k < kObsScalars + lq; k += blockDim.x) o[k] *= z;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int ch = 0; ch < 2; ++ch)
+        for (int ch = 0; ch < 2; ++ch) {
             if (sc->nc[ch] > 0) sc->acc_sum[ch] += (double)sc->nacc[ch] / (double)sc->nc[ch];
+            sc->prop_tot[ch] += (double)sc->nc[ch];
+            sc->acc_tot[ch] += (double)sc->nacc[ch];
+        }
     }
 }
 
@@ -903,28 +1221,39 @@ __global__ void field_norm_kernel(KernelArgs ka, double* out) {
     __shared__ double red[32];
     const double* phi = ka.phi + cd.phi_off;
     double v[1] = {0.0};
-    const long long tot = (long long)P.L * P.N * 2;
+    const long long tot = (long long)P.L * P.Ns * 2;
     for (long long k = threadIdx.x; k < tot; k += blockDim.x) v[0] += phi[k] * phi[k];
     block_sum<1>(v, red);
     if (threadIdx.x == 0) out[chain] = -0.5 * v[0];
 }
 
 // ---------------------------------------------------------------------------
-template <int NMAX>
+template <int NMAX, bool PAIR>
 static cudaError_t launch_cls(int which, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
     if (count <= 0) return cudaSuccess;
     const size_t sm = Smem<NMAX>::bytes();
     cudaError_t e;
     if (which == 0) {
-        e = cudaFuncSetAttribute(sweep_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        e = cudaFuncSetAttribute(sweep_kernel<NMAX, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        sweep_kernel<NMAX><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
+        sweep_kernel<NMAX, PAIR><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
     } else {
-        e = cudaFuncSetAttribute(pre_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        e = cudaFuncSetAttribute(pre_kernel<NMAX, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        pre_kernel<NMAX><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
+        pre_kernel<NMAX, PAIR><<<count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
     }
     return cudaGetLastError();
+}
+
+// class index: bit 0 = size class (NMAX 16 / 36), bit 1 = Nambu sector
+static cudaError_t launch_any(int which, int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
+    switch (cls) {
+        case 0: return launch_cls<16, false>(which, ka, idx, count, st);
+        case 1: return launch_cls<36, false>(which, ka, idx, count, st);
+        case 2: return launch_cls<16, true>(which, ka, idx, count, st);
+        case 3: return launch_cls<36, true>(which, ka, idx, count, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t upload_pow_table(const uint32_t* tab, int count) {
@@ -933,10 +1262,10 @@ cudaError_t upload_pow_table(const uint32_t* tab, int count) {
 }
 
 cudaError_t launch_sweep(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
-    return cls == 0 ? launch_cls<16>(0, ka, idx, count, st) : launch_cls<36>(0, ka, idx, count, st);
+    return launch_any(0, cls, ka, idx, count, st);
 }
 cudaError_t launch_pre(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
-    return cls == 0 ? launch_cls<16>(1, ka, idx, count, st) : launch_cls<36>(1, ka, idx, count, st);
+    return launch_any(1, cls, ka, idx, count, st);
 }
 cudaError_t launch_warmup(const KernelArgs& ka, int nwarm, cudaStream_t st) {
     warmup_kernel<<<ka.nchains, 256, 0, st>>>(ka, nwarm);
@@ -959,7 +1288,12 @@ cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st
     field_norm_kernel<<<ka.nchains, 256, 0, st>>>(ka, out);
     return cudaGetLastError();
 }
-size_t smem_bytes(int cls) { return cls == 0 ? Smem<16>::bytes() : Smem<36>::bytes(); }
-int class_nmax(int cls) { return cls == 0 ? 16 : 36; }
+size_t smem_bytes(int cls) { return (cls & 1) == 0 ? Smem<16>::bytes() : Smem<36>::bytes(); }
+int class_nmax(int cls) { return (cls & 1) == 0 ? 16 : 36; }
+int class_of(int n, int pairing) {
+    for (int c = 0; c < 2; ++c)
+        if (n <= class_nmax(c)) return c + (pairing ? 2 : 0);
+    return -1;
+}
 
 }  // namespace bq

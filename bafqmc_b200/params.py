@@ -1,4 +1,6 @@
-"""paramC_sets.txt contract of the reference solver (calc_basic.f90:48-106).
+"""paramC_sets.txt contract of the reference solvers (calc_basic.f90:48-106;
+the pairing program reads RDelta as a fourth value on line 1,
+src/pairing/src/calc_basic.f90:51-52).
 
 Seven positional lines, Fortran list-directed values; anything after line 7 is
 ignored, as the reference reads exactly seven records.
@@ -64,8 +66,20 @@ class SolverParams:
         return self.Nlx * self.Nly
 
     @property
-    def Ndim(self) -> int:
+    def Nsite(self) -> int:
         return self.Lq
+
+    @property
+    def Ndim(self) -> int:
+        """The reference's matrix dimension: Ns, or 4Ns for the Nambu solver
+        (src/pairing/src/calc_basic.f90:99-101)."""
+        return 4 * self.Lq if self.sector == 1 else self.Lq
+
+    @property
+    def block_dim(self) -> int:
+        """Dimension of the Green's function the device propagates: Ns, or the
+        {b, c^dagger} block 2Ns of a Nambu chain."""
+        return 2 * self.Lq if self.sector == 1 else self.Lq
 
     @property
     def Dtau(self) -> float:

@@ -2,10 +2,11 @@
 reference's run-directory contract on top of it.
 
 `Ensemble` holds one handle of libbafqmc_b200.so (chains of one or several
-parameter points).  `run_directory` reproduces `mpirun -np N bosonDQMC.out`
-(src/number_conserving/src/main.f90:22-85) for N chains on one GPU: it reads
-paramC_sets.txt / confin.txt / seeds.txt and appends the same per-bin files,
-info.txt and confout.txt.
+parameter points, number-conserving and Nambu mixed).  `run_directory`
+reproduces `mpirun -np N bosonDQMC.out` (src/number_conserving/src/main.f90:22-85,
+or the pairing program src/pairing/src/main.f90:19-83 with pairing=True) for
+N chains on one GPU: it reads paramC_sets.txt / confin.txt / seeds.txt and
+appends the same per-bin files, info.txt and confout.txt.
 """
 from __future__ import annotations
 
@@ -17,7 +18,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _lib
-from .observables import FILE_ORDER, OBS_SCALARS, decode
+from .observables import FILE_ORDER, FILE_ORDER_PAIRING, OBS_SCALARS, decode
 from .params import NAUX, SolverParams, conf_transfer
 
 
@@ -56,7 +57,8 @@ class Ensemble:
             nd, lq, lt, nst = C.c_int(), C.c_int(), C.c_int(), C.c_int()
             _lib.check(self.lib.bafqmc_point_dim(h, i, C.byref(nd), C.byref(lq), C.byref(lt), C.byref(nst)))
             self.dims.append((nd.value, lq.value, lt.value, nst.value))
-        self.phi_sizes = [self.dims[p][2] * self.dims[p][0] * NAUX for p in self.chain_point]
+        # fields: [Ltrot][Lx*Ly][2] per chain in both sectors
+        self.phi_sizes = [self.dims[p][2] * self.dims[p][1] * NAUX for p in self.chain_point]
         self.phi_offsets = np.concatenate([[0], np.cumsum(self.phi_sizes)]).astype(np.int64)
 
     def close(self):
@@ -94,8 +96,8 @@ class Ensemble:
         _lib.check(self.lib.bafqmc_get_state(self.h, _iptr(s), _dptr(flat)))
         phis = []
         for c in range(self.nchains):
-            nd, _, lt, _ = self.dims[self.chain_point[c]]
-            phis.append(flat[self.phi_offsets[c]:self.phi_offsets[c + 1]].reshape(lt, nd, NAUX))
+            _, lq, lt, _ = self.dims[self.chain_point[c]]
+            phis.append(flat[self.phi_offsets[c]:self.phi_offsets[c + 1]].reshape(lt, lq, NAUX))
         return s, phis
 
     # ---- the sweep path
@@ -128,13 +130,18 @@ class Ensemble:
 
     def chain_obs(self) -> list[dict]:
         raw = self.chain_obs_raw()
-        return [decode(raw[c], self.dims[self.chain_point[c]][1]) for c in range(self.nchains)]
+        out = []
+        for c in range(self.nchains):
+            pt = self.chain_point[c]
+            out.append(decode(raw[c], self.dims[pt][1], self.points[pt].sector == 1))
+        return out
 
     def point_obs(self) -> list[dict]:
         raw = self.point_obs_raw()
-        return [decode(raw[p], self.dims[p][1]) for p in range(len(self.points))]
+        return [decode(raw[p], self.dims[p][1], self.points[p].sector == 1) for p in range(len(self.points))]
 
     def green(self, chain: int) -> np.ndarray:
+        """The stored Green's function: Prop%Gr, or the {b, c^dagger} block of a Nambu chain."""
         nd = self.dims[self.chain_point[chain]][0]
         out = np.zeros(2 * nd * nd)
         _lib.check(self.lib.bafqmc_get_green(self.h, int(chain), _dptr(out)))
@@ -157,6 +164,22 @@ class Ensemble:
         return out
 
 
+def nambu_green(block: np.ndarray) -> np.ndarray:
+    """The pairing program's 4Ns Prop%Gr from the {b, c^dagger} block.
+
+    Sector order b, c, b^dagger, c^dagger (src/pairing/src/lattice.f90:26-35):
+    the block sits on {b, c^dagger}, its complex conjugate on {c, b^dagger},
+    zeros elsewhere."""
+    n2 = block.shape[0]
+    ns = n2 // 2
+    g = np.zeros((4 * ns, 4 * ns), dtype=np.complex128)
+    one = list(range(ns)) + list(range(3 * ns, 4 * ns))
+    two = list(range(ns, 2 * ns)) + list(range(2 * ns, 3 * ns))
+    g[np.ix_(one, one)] = block
+    g[np.ix_(two, two)] = np.conj(block)
+    return g
+
+
 # ---------------------------------------------------------------------------
 # per-bin diagnostics of G (pole_diagnostics.f90:91-123).  log_weight comes from
 # the device (stabilised factorisation of I - B); the eigen/singular values are
@@ -174,6 +197,11 @@ def pole_diagnostics(G: np.ndarray, log_weight: float) -> dict:
 
 # ---------------------------------------------------------------------------
 # output formats of the reference writer
+def _scalar(v):
+    """A numpy scalar as the Python int/float it holds (numpy 2 reprs carry the type name)."""
+    return v.item() if isinstance(v, np.generic) else v
+
+
 def _lst(*vals) -> str:
     """Fortran list-directed record: blank-separated values, lossless."""
     return " " + "  ".join(repr(float(v)) for v in vals) + "\n"
@@ -186,12 +214,25 @@ def _es(v: float, width: int = 24, digits: int = 16, expdigits: int = 2) -> str:
     return s.rjust(width)
 
 
-def append_bin(run_dir: Path, obs: dict) -> None:
-    """m_write_obs_equal (fourier_trans.f90:250-348)."""
-    for name in FILE_ORDER:
+def _e(v: float, width: int = 24, digits: int = 16) -> str:
+    """Fortran Ew.d: 0.ddd...E+xx (mantissa in [0.1, 1))."""
+    if v == 0.0 or not math.isfinite(v):
+        s = f"0.{'0' * digits}E+00" if v == 0.0 else str(v)
+        return s.rjust(width)
+    m, e = f"{abs(v):.{digits - 1}E}".split("E")
+    ei = int(e) + 1
+    s = f"{'-' if v < 0 else ''}0.{m.replace('.', '')}E{'-' if ei < 0 else '+'}{abs(ei):02d}"
+    return s.rjust(width)
+
+
+def append_bin(run_dir: Path, obs: dict, pairing: bool = False) -> None:
+    """m_write_obs_equal (fourier_trans.f90:250-348; src/pairing/src/fourier_trans.f90:276-405)."""
+    for name in (FILE_ORDER_PAIRING if pairing else FILE_ORDER):
         v = obs[name]
         with open(run_dir / name, "a") as f:
-            if name == "density_site_total":
+            if name == "density_site_total" and pairing:   # '(1X,E24.16)' per site
+                f.write("".join(" " + _e(x) for x in v) + "\n")
+            elif name == "density_site_total":
                 f.write("".join(_es(x) + " " for x in v) + "\n")
             elif isinstance(v, complex):
                 f.write(_lst(v.real, v.imag))
@@ -225,20 +266,35 @@ def read_confin(path: Path, p: SolverParams, nchains: int):
     return out
 
 
-def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print) -> dict:
-    """The reference program for `mpirun -np nchains` in run_dir, on one GPU."""
+def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print,
+                  pairing: bool = False) -> dict:
+    """The reference program for `mpirun -np nchains` in run_dir, on one GPU.
+
+    pairing=True runs the Nambu program (src/pairing/src/main.f90): RDelta is
+    read from line 1 of paramC_sets.txt, the pairing file set is written, and
+    there are no pole diagnostics."""
     run_dir = Path(run_dir)
     t0 = time.time()
-    p = SolverParams.from_file(run_dir / "paramC_sets.txt")
+    p = SolverParams.from_file(run_dir / "paramC_sets.txt", pairing=pairing)
     info = open(run_dir / "info.txt", "w")
-    w = lambda label, v: info.write(f" {label:<47}:{v!r:>26}\n")
-    info.write(" =========================\n DQMC for boson Hubbard on triangular lattice\n")
-    w("Linear lengh Lx", p.Nlx); w("Linear lengh Ly", p.Nly); w("Hopping t", 1.0)
-    w("Hubbard U1 (relative-density, repulsive)", p.U1); w("Hubbard U2 (total-density, attractive)", p.U2)
+    w = lambda label, v: info.write(f" {label:<47}:{_scalar(v)!r:>26}\n")
+    if pairing:   # write_info (src/pairing/src/calc_basic.f90:140-180)
+        info.write(" =========================\n DQMC for pairing Bose Hubbard on triangular lattice\n")
+        w("Linear lengh Lx", p.Nlx); w("Linear lengh Ly", p.Nly); w("Hopping t", 1.0)
+        w("Relative-density U1 (>=0)", p.U1); w("Total-density U2 (<=0)", p.U2); w("pairing Delta", p.delta)
+    else:         # write_info (calc_basic.f90:137-175)
+        info.write(" =========================\n DQMC for boson Hubbard on triangular lattice\n")
+        w("Linear lengh Lx", p.Nlx); w("Linear lengh Ly", p.Nly); w("Hopping t", 1.0)
+        w("Hubbard U1 (relative-density, repulsive)", p.U1); w("Hubbard U2 (total-density, attractive)", p.U2)
     w("chemical potential", p.mu); w("Local update auxiliary field magnitude Shift", p.shiftLoc)
     if p.is_warm:
-        w("# Warm", p.Nwarm); w("Thermalize U1 relative-field magnitude", p.shiftWarm[0])
-        w("Thermalize U2 total-field magnitude", p.shiftWarm[1])
+        w("# Warm", p.Nwarm)
+        if pairing:
+            w("Thermalize auxiliary field magnitude for U1", p.shiftWarm[0])
+            w("Thermalize auxiliary field magnitude for U2", p.shiftWarm[1])
+        else:
+            w("Thermalize U1 relative-field magnitude", p.shiftWarm[0])
+            w("Thermalize U2 total-field magnitude", p.shiftWarm[1])
     w("Choosing initial distribution type", p.iniType); w("Magnitude of Gaussian distribution", p.iniAmpl)
     w("Beta", p.Beta); w("Trotter number", p.Ltrot); w("=>Dtau", p.Dtau); w("N_Ortho", p.Nwrap)
     w("# Bins", p.Nbin); w("# Nsweep in one bin", p.Nsweep); w("# Cores", nchains)
@@ -262,14 +318,23 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     ens.pre()
     for nbc in range(p.Nbin):
         ens.sweep(p.Nsweep)
-        append_bin(run_dir, ens.point_obs()[0])
-        if pole:
+        append_bin(run_dir, ens.point_obs()[0], pairing=pairing)
+        if pole and not pairing:
             lw = ens.log_weight()
             append_pole(run_dir, [pole_diagnostics(ens.green(c), lw[c]) for c in range(nchains)])
     cnt = ens.counters()
-    for ch, name in ((0, "Accept_U1_shift"), (1, "Accept_U2_shift")):
+    for ch, name in ((0, "U1"), (1, "U2")):
         if abs((p.U1, p.U2)[ch]) > 1e-10:
-            w(name, float(cnt[:, ch].sum() / (nchains * p.Nbin)))
+            w(f"Accept_{name}_shift", float(cnt[:, ch].sum() / (nchains * p.Nbin)))
+            if pairing:   # Local_control_print (src/pairing/src/local_sweep.f90:163-213)
+                nprop, nacc = float(cnt[:, 10 + ch].sum()), float(cnt[:, 12 + ch].sum())
+                if nprop > 0:
+                    w(f"Phase_{name}_mean_abs_arg_proposed", 0.0)
+                if nacc > 0:
+                    w(f"Phase_{name}_mean_abs_arg_accepted", 0.0)
+                if nprop > 0:
+                    w(f"Phase_{name}_branch_pi_fraction", 0.0)
+                w(f"Phase_{name}_local_proposals", nprop)
     if np.any(cnt[:, 6] != 0):
         info.write(" non-finite Green's function detected in chains: "
                    + " ".join(str(i) for i in np.nonzero(cnt[:, 6])[0]) + "\n")
@@ -281,6 +346,6 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     with open(run_dir / "confout.txt", "w") as f:   # conf_out (fields.f90:236-278)
         for c in range(nchains):
             f.write(f" {int(seeds[c])}\n")
-            f.write("".join(f" {v!r}\n" for v in phis[c].ravel()))
+            f.write("".join(f" {float(v)!r}\n" for v in phis[c].ravel()))
     ens.close()
     return {"params": p, "counters": cnt}

@@ -1,14 +1,17 @@
 /*
  * bafqmc_b200.h -- C ABI of the B200 implementation of the BAFQMC
- * finite-temperature auxiliary-field sweep (number-conserving solver).
+ * finite-temperature auxiliary-field sweep (number-conserving solver and
+ * Nambu pairing solver).
  *
  * The reference exposes this path as a process/file contract: a driver writes
  * paramC_sets.txt, confin.txt and seeds.txt into a run directory and launches
- * `mpirun -np N build/bosonDQMC.out` (src/number_conserving/run_paper.py:113,162),
- * one Markov chain per MPI rank.  Each entry point below replaces one step of
- * that program (src/number_conserving/src/main.f90:22-85); the comment names
- * the reference routine it stands in for.  A "chain" here is one MPI rank of
- * the reference; a "point" is one paramC_sets.txt parameter set.
+ * `mpirun -np N build/bosonDQMC.out` (src/number_conserving/run_paper.py:113,162;
+ * the pairing program src/pairing/src/main.f90 likewise), one Markov chain per
+ * MPI rank.  Each entry point below replaces one step of that program
+ * (src/number_conserving/src/main.f90:22-85, src/pairing/src/main.f90:19-83);
+ * the comment names the reference routine it stands in for.  A "chain" here is
+ * one MPI rank of the reference; a "point" is one paramC_sets.txt parameter
+ * set.  One handle may mix points of both sectors and of several sizes.
  *
  * Conventions
  *   - Every function returns 0 on success or a negative BAFQMC_E* code;
@@ -38,14 +41,14 @@ extern "C" {
 #define BAFQMC_ENUMERIC (-5)    /* non-finite Green's function detected */
 
 /* Number of scalar observable slots per chain before the site densities. */
-#define BAFQMC_OBS_SCALARS 26
+#define BAFQMC_OBS_SCALARS 32
 
 /* One parameter point: the seven lines of paramC_sets.txt
  * (calc_basic.f90:52-59) plus the sector.  `delta` is the pairing amplitude
- * of the Nambu solver (src/pairing/src/calc_basic.f90:51) and must be 0 for
- * sector 0.  t is fixed to 1 as in the reference (calc_basic.f90:94). */
+ * RDelta of the Nambu solver (src/pairing/src/calc_basic.f90:51) and must be
+ * 0 for sector 0.  t is fixed to 1 as in the reference (calc_basic.f90:94). */
 typedef struct bafqmc_point {
-    int sector;              /* 0 = number-conserving (Ndim = Lx*Ly) */
+    int sector;              /* 0 = number-conserving (Ndim = Lx*Ly); 1 = Nambu pairing (stored block 2*Lx*Ly) */
     int Lx, Ly, Ltrot;
     double beta, U1, U2, mu, delta;
     int Nwrap;
@@ -65,12 +68,14 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
 void bafqmc_destroy(bafqmc_handle* h);
 const char* bafqmc_last_error(void);
 
-/* Sizes: Ndim of a point, and the per-chain observable stride. */
+/* Sizes: dimension of a point's stored Green's function (Lx*Ly, or 2*Lx*Ly
+ * for a Nambu point), and the per-chain observable stride. */
 int bafqmc_point_dim(const bafqmc_handle* h, int point, int* ndim, int* lq, int* ltrot, int* nst);
 int bafqmc_obs_stride(const bafqmc_handle* h);
 int bafqmc_num_chains(const bafqmc_handle* h);
 
-/* conf_set + conf_transfer (fields.f90:115-234): fields of each chain from its
+/* conf_set + conf_transfer (fields.f90:115-234): fields of each chain
+ * ([Ltrot][Lx*Ly][2] doubles in both sectors) from its
  * seed (seeds.txt row), the seed advanced past the draws as in conf_therm_in. */
 int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds);
 
@@ -98,17 +103,27 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep);
 int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs);
 int bafqmc_bin_point_obs(bafqmc_handle* h, double* point_obs);
 
-/* Prop%Gr of one chain (row-major complex). */
+/* Prop%Gr of one chain (row-major complex, ndim x ndim as bafqmc_point_dim
+ * reports).  For a Nambu chain this is the {b, c^dagger} block of the
+ * reference's 4Ns Green's function, rows/columns b_1..b_Ns, c^dagger_1..
+ * c^dagger_Ns; the full matrix in the sector order b, c, b^dagger, c^dagger
+ * (src/pairing/src/lattice.f90:26-35) has this block on {b, c^dagger}, its
+ * complex conjugate on {c, b^dagger} and zeros elsewhere. */
 int bafqmc_get_green(bafqmc_handle* h, int chain, double* G);
 
 /* log_weight = -1/2 sum phi^2 + 2 log|det G| per chain
  * (pole_diagnostics.f90:119; log|det G| from the last stabilised
- * (I - B(beta,0)) factorisation). */
+ * (I - B(beta,0)) factorisation).  The pairing program has no such output:
+ * NaN for Nambu chains. */
 int bafqmc_log_weight(bafqmc_handle* h, double* out);
 
-/* Per chain, 10 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
- * status, seed, nobs, reserved (AccCounter, Prop%Xmaxm/Xmeanm). */
-#define BAFQMC_COUNTERS 10
+/* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
+ * status, seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
+ * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and
+ * %count_accepted over all bins, src/pairing/src/operator_Hubbard.f90:269-284.
+ * The Nambu weight ratio is real and positive here, so PhaseCounter's phase
+ * sums are zero). */
+#define BAFQMC_COUNTERS 14
 int bafqmc_counters(bafqmc_handle* h, double* out);
 
 /* Per-phase SM cycle counters of the sweep kernel (the reference has only a

@@ -46,7 +46,8 @@ def _handle_path(p, seeds, phis, nsweep):
         ens.sweep(nsweep)
         obs = ens.chain_obs_raw()
         s, ph = ens.get_state()
-    return obs[:, : 26 + p.Lq], s, ph
+    from bafqmc_b200 import _lib
+    return obs[:, : _lib.OBS_SCALARS + p.Lq], s, ph
 
 
 def test_noalloc_matches_handle_path_on_two_calls():
@@ -54,7 +55,7 @@ def test_noalloc_matches_handle_path_on_two_calls():
     from bafqmc_b200 import _lib
     from bafqmc_b200.solver import Ensemble, point_struct
     p = _point()
-    nchains, nsweep, stride = 6, 2, 26 + p.Lq
+    nchains, nsweep, stride = 6, 2, _lib.OBS_SCALARS + p.Lq
     with Ensemble([p], np.zeros(nchains, dtype=np.int32)) as ens:
         ens.fields_from_seeds(4099 + 31 * np.arange(nchains))
         seeds, phis = ens.get_state()
