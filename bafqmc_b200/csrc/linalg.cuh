@@ -7,8 +7,10 @@
 // src/common/mymats.f90:20-29): ZGEMM, ZTRMM, ZGEQP3 (unblocked ZLAQP2 path,
 // which LAPACK takes for the matrix sizes here), ZUNGQR, ZUNMQR, ZTRSM,
 // ZLAPMR/ZLAPMT.  They are written for the sweep's sizes (n <= 64): one CTA
-// owns one matrix, so every step is a barrier-separated pass over shared
-// memory instead of a blocked panel algorithm.
+// owns one matrix.  The reflector and triangular-solve sequences run on 8-lane
+// segments that each keep their columns (or rows) of the operand in registers
+// for the whole sequence and reduce with shuffles, so no step needs a block
+// barrier; divisions are replaced by precomputed reciprocals.
 #pragma once
 #include "cplx.cuh"
 
@@ -184,6 +186,26 @@ DEVI double seg8_colnorm(int n, const cplx* A, int j, int r0, int lane8) {
     return m * sqrt(s);
 }
 
+// Sum of squares of column j, rows r0..n-1, by one 8-lane segment.
+DEVI double seg8_sumsq_col(int n, const cplx* A, int j, int r0, int lane8) {
+    double ss = 0.0;
+    for (int r = r0 + lane8; r < n; r += 8) {
+        const cplx a = A[r * n + j];
+        ss = fma(a.x, a.x, fma(a.y, a.y, ss));
+    }
+    return seg8_sum(ss);
+}
+
+DEVI bool sumsq_unsafe(double ss) { return !(ss <= 1.0e300) || (ss != 0.0 && ss < 1.0e-290); }
+
+// 2-norm of column j rows r0..n-1 (one segment); scaled only when the plain sum
+// of squares would over- or underflow.
+DEVI double seg8_norm(int n, const cplx* A, int j, int r0, int lane8) {
+    const double ss = seg8_sumsq_col(n, A, j, r0, lane8);
+    if (!sumsq_unsafe(ss)) return sqrt(ss);
+    return seg8_colnorm(n, A, j, r0, lane8);
+}
+
 // Shared scratch for the factorisations (lives in shared memory, size ~ 6n).
 struct QRScratch {
     cplx* tau;      // n
@@ -200,225 +222,437 @@ struct QRScratch {
 // QDRP_decompose post-step (stabilization.f90:41-67): d[i] = |R_ii| and row i of
 // the upper triangle divided by d[i].  On exit A holds the scaled R in its upper
 // triangle and the Householder vectors (unit leading entry implicit) below it.
+//
+// Two barriers per column.  Every warp finds the pivot (IDAMAX of the partial
+// norms) and every 8-lane segment forms the reflector (ZLARFG) itself from the
+// pivot column, so neither needs a barrier of its own; each segment keeps its
+// target columns in registers from the read phase to the write phase.  The
+// norm downdate is ZLAQP2's, with its quotients multiplied out (no division).
+// R8 >= ceil(n/8) rows per lane, CPS >= ceil(n/segments) columns per segment.
+template <int R8, int CPS>
 COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int lane8 = tid & 7, seg = tid >> 3, nseg = nthr >> 3;
+    const int tid = threadIdx.x, lane = tid & 31, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     const double tol3z = 1.0536712127723509e-08;   // sqrt(2^-53), LAPACK's sqrt(dlamch('E'))
-    // initial column norms
     for (int j = seg; j < n; j += nseg) {
-        double v = seg8_colnorm(n, A, j, 0, lane8);
+        const double v = seg8_norm(n, A, j, 0, lane8);
         if (lane8 == 0) { s.vn1[j] = v; s.vn2[j] = v; s.piv[j] = j; }
     }
     __syncthreads();
     for (int i = 0; i < n; ++i) {
-        // pivot: first index of max vn1[i..n) (IDAMAX), by warp 0
-        if (tid < 32) {
-            double best = -1.0;
-            int bi = n;
-            for (int j = i + tid; j < n; j += 32) {
-                double v = s.vn1[j];
-                if (v > best) { best = v; bi = j; }
-            }
+        // pivot: first index of max vn1[i..n) (IDAMAX), every warp
+        double best = -1.0;
+        int bi = n;
+        for (int j = i + lane; j < n; j += 32) {
+            const double v = s.vn1[j];
+            if (v > best) { best = v; bi = j; }
+        }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        const int pvt = (bi < n) ? bi : i;   // all-NaN norms: keep column i
+        // reflector of the pivot column (ZLARFG), every segment
+        cplx v[R8];
+        double ss = 0.0;
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = lane8 + 8 * k;
+            v[k] = (r < n && r > i) ? A[r * n + pvt] : cmk(0.0, 0.0);
+            ss = fma(v[k].x, v[k].x, fma(v[k].y, v[k].y, ss));
+        }
+        ss = seg8_sum(ss);
+        const cplx alpha = A[i * n + pvt];
+        double xn = sqrt(ss);
+        if (sumsq_unsafe(ss)) xn = seg8_colnorm(n, A, pvt, i + 1, lane8);
+        cplx tau = cmk(0.0, 0.0), beta = alpha, scl = cmk(0.0, 0.0);
+        if (!(xn == 0.0 && alpha.y == 0.0)) {
+            const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn * xn);
+            const double b = (alpha.x >= 0.0) ? -nrm : nrm;
+            const double ib = 1.0 / b;
+            tau = cmk((b - alpha.x) * ib, -alpha.y * ib);
+            const cplx d = cmk(alpha.x - b, alpha.y);           // scl = 1 / d
+            const double id2 = 1.0 / (d.x * d.x + d.y * d.y);
+            scl = cmk(d.x * id2, -d.y * id2);
+            beta = cmk(b, 0.0);
+        }
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = lane8 + 8 * k;
+            v[k] = (r == i) ? cmk(1.0, 0.0) : cmul(scl, v[k]);
+        }
+        // target columns j = i+1+seg+q*nseg; logical column pvt holds the old column i
+        cplx a[CPS][R8];
+        double t1[CPS], t2[CPS];
+#pragma unroll
+        for (int q = 0; q < CPS; ++q) {
+            const int j = i + 1 + seg + q * nseg;
+            const int src = (j == pvt) ? i : j;
+            const bool ok = j < n;
+#pragma unroll
+            for (int k = 0; k < R8; ++k) {
+                const int r = lane8 + 8 * k;
+                a[q][k] = (ok && r < n && r >= i) ? A[r * n + src] : cmk(0.0, 0.0);
             }
-            if (tid == 0) s.ibcast[0] = (bi < n) ? bi : i;   // all-NaN norms: keep column i
+            t1[q] = ok ? s.vn1[src] : 0.0;
+            t2[q] = ok ? s.vn2[src] : 0.0;
+        }
+        cplx ui = cmk(0.0, 0.0), up = cmk(0.0, 0.0);   // rows < i of columns i and pvt
+        if (tid < i) {
+            ui = A[tid * n + i];
+            up = A[tid * n + pvt];
         }
         __syncthreads();
-        const int pvt = s.ibcast[0];
-        if (pvt != i) {
-            for (int r = tid; r < n; r += nthr) {
-                cplx t = A[r * n + i];
-                A[r * n + i] = A[r * n + pvt];
-                A[r * n + pvt] = t;
-            }
-            if (tid == 0) {
-                int t = s.piv[pvt]; s.piv[pvt] = s.piv[i]; s.piv[i] = t;
-                s.vn1[pvt] = s.vn1[i];
-                s.vn2[pvt] = s.vn2[i];
-            }
+        if (pvt != i && tid < i) {
+            A[tid * n + i] = up;
+            A[tid * n + pvt] = ui;
         }
-        __syncthreads();
-        // Householder reflector for A[i:, i] (ZLARFG), by segment 0
         if (seg == 0) {
-            double xn = seg8_colnorm(n, A, i, i + 1, lane8);
-            cplx alpha = A[i * n + i];
-            cplx tau = cmk(0.0, 0.0), beta = alpha;
-            cplx scl = cmk(0.0, 0.0);
-            bool doit = !(xn == 0.0 && alpha.y == 0.0);
-            if (doit) {
-                double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn * xn);
-                double b = (alpha.x >= 0.0) ? -nrm : nrm;
-                tau = cmk((b - alpha.x) / b, -alpha.y / b);
-                scl = cdiv(cmk(1.0, 0.0), cmk(alpha.x - b, alpha.y));
-                beta = cmk(b, 0.0);
+#pragma unroll
+            for (int k = 0; k < R8; ++k) {
+                const int r = lane8 + 8 * k;
+                if (r < n && r > i) A[r * n + i] = v[k];
             }
-            if (doit) {
-                for (int r = i + 1 + lane8; r < n; r += 8) A[r * n + i] = cmul(scl, A[r * n + i]);
-            }
-            if (lane8 == 0) { A[i * n + i] = beta; s.tau[i] = tau; }
-        }
-        __syncthreads();
-        // apply H^H = I - conj(tau) v v^H to A[i:, i+1:], then downdate norms
-        const cplx ctau = cconj(s.tau[i]);
-        for (int j = i + 1 + seg; j < n; j += nseg) {
-            cplx w = cmk(0.0, 0.0);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : A[r * n + i];
-                w = cfmacj(v, A[r * n + j], w);
-            }
-            w.x = seg8_sum(w.x);
-            w.y = seg8_sum(w.y);
-            cplx f = cmul(ctau, w);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : A[r * n + i];
-                A[r * n + j] = csub(A[r * n + j], cmul(v, f));
-            }
-            __syncwarp(seg8_mask());
-            // norm downdate (ZLAQP2): lane 0 of the segment owns row i
-            double v1 = s.vn1[j];
-            int recompute = 0;
-            double newv = v1;
-            if (v1 != 0.0) {
-                double t = cabsv(A[i * n + j]) / v1;
-                double temp = fmax(1.0 - t * t, 0.0);
-                double q = v1 / s.vn2[j];
-                double temp2 = temp * q * q;
-                if (temp2 <= tol3z) recompute = 1;
-                else newv = v1 * sqrt(temp);
-            }
-            double nv = newv;
-            if (recompute) nv = (i + 1 < n) ? seg8_colnorm(n, A, j, i + 1, lane8) : 0.0;
-            __syncwarp(seg8_mask());
             if (lane8 == 0) {
-                s.vn1[j] = nv;
-                if (recompute) s.vn2[j] = nv;
+                A[i * n + i] = beta;
+                s.tau[i] = tau;
             }
         }
-        __syncthreads();
-    }
-    // QDRP post-step: D = |diag R|, scale the rows of the upper triangle
-    for (int i = tid; i < n; i += nthr) s.d[i] = cabsv(A[i * n + i]);
-    __syncthreads();
-    for (int e = tid; e < n * n; e += nthr) {
-        int r = e / n, c = e % n;
-        if (c >= r) {
-            double x = s.d[r];
-            A[e] = cmk(A[e].x / x, A[e].y / x);
+        if (tid == 0 && pvt != i) {
+            const int t = s.piv[pvt];
+            s.piv[pvt] = s.piv[i];
+            s.piv[i] = t;
         }
-    }
-    for (int k = tid; k < n; k += nthr) s.ipiv[s.piv[k]] = k;
-    __syncthreads();
-}
-
-// Q = H_0 H_1 ... H_{n-1} (ZUNGQR) from the reflectors stored below the
-// diagonal of F, written to Q (must not alias F).  conjT writes Q^H instead.
-template <int MAXE>
-COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
-    const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
-    for (int e = tid; e < n * n; e += blockDim.x) Q[e] = cmk((e / n) == (e % n) ? 1.0 : 0.0, 0.0);
-    __syncthreads();
-    for (int i = n - 1; i >= 0; --i) {
-        const cplx t = tau[i];
-        for (int j = i + seg; j < n; j += nseg) {
+        const cplx ctau = cconj(tau);
+#pragma unroll
+        for (int q = 0; q < CPS; ++q) {
+            const int j = i + 1 + seg + q * nseg;
+            if (j >= n) continue;   // uniform within the segment
             cplx w = cmk(0.0, 0.0);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : F[r * n + i];
-                w = cfmacj(v, Q[r * n + j], w);
-            }
+#pragma unroll
+            for (int k = 0; k < R8; ++k) w = cfmacj(v[k], a[q][k], w);
             w.x = seg8_sum(w.x);
             w.y = seg8_sum(w.y);
-            cplx f = cmul(t, w);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : F[r * n + i];
-                Q[r * n + j] = csub(Q[r * n + j], cmul(v, f));
+            const cplx f = cmul(ctau, w);
+            double ai2 = 0.0, rest = 0.0;
+#pragma unroll
+            for (int k = 0; k < R8; ++k) {
+                const int r = lane8 + 8 * k;
+                a[q][k] = csub(a[q][k], cmul(v[k], f));
+                const double m2 = a[q][k].x * a[q][k].x + a[q][k].y * a[q][k].y;
+                if (r == i) ai2 = m2;
+                if (r > i && r < n) rest += m2;
+                if (r < n && r >= i) A[r * n + j] = a[q][k];
+            }
+            ai2 = seg8_sum(ai2);
+            rest = seg8_sum(rest);
+            // ZLAQP2 norm downdate: temp = max(1 - (|a_ij|/vn1)^2, 0),
+            // recompute if temp (vn1/vn2)^2 <= tol3z, else vn1 *= sqrt(temp);
+            // written as max(vn1^2 - |a_ij|^2, 0) against tol3z vn2^2.
+            const double v1 = t1[q];
+            double nv1 = v1, nv2 = t2[q];
+            if (v1 != 0.0) {
+                bool recompute;
+                if (v1 < 1.0e150 && t2[q] < 1.0e150) {
+                    const double rem = fmax(v1 * v1 - ai2, 0.0);   // = temp * vn1^2
+                    recompute = rem <= tol3z * t2[q] * t2[q];
+                    nv1 = sqrt(rem);
+                } else {
+                    const double tt = sqrt(ai2) / v1;
+                    const double temp = fmax(1.0 - tt * tt, 0.0);
+                    const double qq = v1 / t2[q];
+                    recompute = !(temp * qq * qq > tol3z);
+                    nv1 = v1 * sqrt(temp);
+                }
+                if (recompute) {
+                    if (sumsq_unsafe(rest)) {
+                        __syncwarp(seg8_mask());
+                        nv1 = (i + 1 < n) ? seg8_colnorm(n, A, j, i + 1, lane8) : 0.0;
+                    } else {
+                        nv1 = sqrt(rest);
+                    }
+                    nv2 = nv1;
+                }
+            }
+            if (lane8 == 0) {
+                s.vn1[j] = nv1;
+                s.vn2[j] = nv2;
             }
         }
         __syncthreads();
     }
-    if (conjT) conj_transpose_inplace<MAXE>(n, Q);
+    // D = |diag R|, rows of the upper triangle scaled by 1/D
+    for (int i = tid; i < n; i += blockDim.x) {
+        const cplx a = A[i * n + i];
+        const double d = hypot(a.x, a.y);
+        s.d[i] = d;
+        s.vn1[i] = 1.0 / d;
+    }
+    __syncthreads();
+    for (int e = tid; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        if (c >= r) {
+            const double x = s.vn1[r];
+            A[e] = cmk(A[e].x * x, A[e].y * x);
+        }
+    }
+    for (int k = tid; k < n; k += blockDim.x) s.ipiv[s.piv[k]] = k;
+    __syncthreads();
 }
 
-// C <- Q^H C (ZUNMQR 'L','C'), reflectors in F.
+// C <- Q^H C (ZUNMQR 'L','C'): each segment holds its columns in registers.
+template <int R8, int CPS>
 COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
+    cplx c[CPS][R8];
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            c[q][k] = (j < n && r < n) ? C[r * n + j] : cmk(0.0, 0.0);
+        }
     for (int i = 0; i < n; ++i) {
         const cplx ct = cconj(tau[i]);
-        for (int j = seg; j < n; j += nseg) {
+        cplx v[R8];
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = lane8 + 8 * k;
+            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * n + i] : cmk(0.0, 0.0));
+        }
+#pragma unroll
+        for (int q = 0; q < CPS; ++q) {
             cplx w = cmk(0.0, 0.0);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : F[r * n + i];
-                w = cfmacj(v, C[r * n + j], w);
-            }
+#pragma unroll
+            for (int k = 0; k < R8; ++k) w = cfmacj(v[k], c[q][k], w);
             w.x = seg8_sum(w.x);
             w.y = seg8_sum(w.y);
-            cplx f = cmul(ct, w);
-            for (int r = i + lane8; r < n; r += 8) {
-                cplx v = (r == i) ? cmk(1.0, 0.0) : F[r * n + i];
-                C[r * n + j] = csub(C[r * n + j], cmul(v, f));
-            }
+            const cplx f = cmul(ct, w);
+#pragma unroll
+            for (int k = 0; k < R8; ++k) c[q][k] = csub(c[q][k], cmul(v[k], f));
         }
-        __syncthreads();
     }
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            if (j < n && r < n) C[r * n + j] = c[q][k];
+        }
+    __syncthreads();
 }
 
-// C <- C Q (ZUNMQR 'R','N'), reflectors in F.
+// C <- C Q (ZUNMQR 'R','N'): each segment holds its rows in registers.
+template <int R8, int CPS>
 COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
+    cplx c[CPS][R8];   // c[q][k] = C[row seg+q*nseg][col lane8+8k]
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = seg + q * nseg, col = lane8 + 8 * k;
+            c[q][k] = (r < n && col < n) ? C[r * n + col] : cmk(0.0, 0.0);
+        }
     for (int i = 0; i < n; ++i) {
         const cplx t = tau[i];
-        for (int r = seg; r < n; r += nseg) {
+        cplx v[R8];
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int col = lane8 + 8 * k;
+            v[k] = (col == i) ? cmk(1.0, 0.0) : ((col > i && col < n) ? F[col * n + i] : cmk(0.0, 0.0));
+        }
+#pragma unroll
+        for (int q = 0; q < CPS; ++q) {
             cplx w = cmk(0.0, 0.0);
-            for (int k = i + lane8; k < n; k += 8) {
-                cplx v = (k == i) ? cmk(1.0, 0.0) : F[k * n + i];
-                w = cfma(C[r * n + k], v, w);
-            }
+#pragma unroll
+            for (int k = 0; k < R8; ++k) w = cfma(c[q][k], v[k], w);
             w.x = seg8_sum(w.x);
             w.y = seg8_sum(w.y);
-            cplx f = cmul(t, w);
-            for (int k = i + lane8; k < n; k += 8) {
-                cplx v = (k == i) ? cmk(1.0, 0.0) : F[k * n + i];
-                C[r * n + k] = csub(C[r * n + k], cmulcj(f, v));
-            }
+            const cplx f = cmul(t, w);
+#pragma unroll
+            for (int k = 0; k < R8; ++k) c[q][k] = csub(c[q][k], cmulcj(f, v[k]));
         }
-        __syncthreads();
     }
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = seg + q * nseg, col = lane8 + 8 * k;
+            if (r < n && col < n) C[r * n + col] = c[q][k];
+        }
+    __syncthreads();
 }
 
-// C <- R^{-1} C with R the upper triangle of F (ZTRSM 'L','U','N','N').
-// Column-parallel back substitution: one 8-lane segment per column.
-COLD void trsm_left_upper(int n, const cplx* F, cplx* C) {
+// Q = H_0 ... H_{n-1} (ZUNGQR), or Q^H with conjT, written to Q (no alias with F).
+template <int R8, int CPS>
+COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
-    for (int c = seg; c < n; c += nseg) {
-        for (int i = n - 1; i >= 0; --i) {
-            // x_i = C[i][c] / R_ii (every lane computes it), then rows k < i downdate
-            cplx xi = cdiv(C[i * n + c], F[i * n + i]);
-            __syncwarp(seg8_mask());
-            if (lane8 == 0) C[i * n + c] = xi;
-            for (int k = lane8; k < i; k += 8) C[k * n + c] = csub(C[k * n + c], cmul(F[k * n + i], xi));
-            __syncwarp(seg8_mask());
+    cplx c[CPS][R8];
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            c[q][k] = cmk((r == j) ? 1.0 : 0.0, 0.0);
         }
+    for (int i = n - 1; i >= 0; --i) {
+        const cplx t = tau[i];
+        cplx v[R8];
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = lane8 + 8 * k;
+            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * n + i] : cmk(0.0, 0.0));
+        }
+#pragma unroll
+        for (int q = 0; q < CPS; ++q) {
+            const int j = seg + q * nseg;
+            if (j < i) continue;   // columns left of i are untouched by H_i (ZUNG2R), uniform per segment
+            cplx w = cmk(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < R8; ++k) w = cfmacj(v[k], c[q][k], w);
+            w.x = seg8_sum(w.x);
+            w.y = seg8_sum(w.y);
+            const cplx f = cmul(t, w);
+#pragma unroll
+            for (int k = 0; k < R8; ++k) c[q][k] = csub(c[q][k], cmul(v[k], f));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            if (j < n && r < n) {
+                if (conjT) Q[j * n + r] = cconj(c[q][k]);
+                else Q[r * n + j] = c[q][k];
+            }
+        }
+    __syncthreads();
+}
+
+// Inverses of the diagonal of the upper triangle of F into rinv (n complex),
+// and of the positive vector d into dinv (n reals), for the triangular solves.
+COLD void diag_inverse(int n, const cplx* F, const double* d, cplx* rinv, double* dinv) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const cplx a = F[i * n + i];
+        const double id2 = 1.0 / (a.x * a.x + a.y * a.y);
+        rinv[i] = cmk(a.x * id2, -a.y * id2);
+        dinv[i] = 1.0 / d[i];
     }
     __syncthreads();
 }
 
-// C <- C R^{-H} with R the upper triangle of F (ZTRSM 'R','U','C','N').
-// Row-parallel: X R^H = C, solved for columns n-1 .. 0.
-COLD void trsm_right_upperH(int n, const cplx* F, cplx* C) {
+// C <- R^{-1} diag(rs) C (ZTRSM 'L','U','N','N' after scaling row r of C by
+// rs[r]); rinv from diag_inverse.  Each segment holds its columns in
+// registers; row i's value comes from lane i%8 by shuffle.
+template <int R8, int CPS>
+COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
-    for (int r = seg; r < n; r += nseg) {
-        for (int c = n - 1; c >= 0; --c) {
-            cplx xc = cdiv(C[r * n + c], cconj(F[c * n + c]));
-            __syncwarp(seg8_mask());
-            if (lane8 == 0) C[r * n + c] = xc;
-            // C[r][k] -= x_c * conj(R[k][c]) for k < c
-            for (int k = lane8; k < c; k += 8) C[r * n + k] = csub(C[r * n + k], cmulcj(xc, F[k * n + c]));
-            __syncwarp(seg8_mask());
+    const unsigned m = seg8_mask();
+    const int base = tid & 24;
+    cplx c[CPS][R8];
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            if (j < n && r < n) {
+                const cplx x = C[r * n + j];
+                const double f = rs[r];
+                c[q][k] = cmk(x.x * f, x.y * f);
+            } else {
+                c[q][k] = cmk(0.0, 0.0);
+            }
+        }
+#pragma unroll
+    for (int kk = R8 - 1; kk >= 0; --kk) {
+        for (int l = 7; l >= 0; --l) {
+            const int i = 8 * kk + l;
+            if (i >= n) continue;   // uniform
+            const cplx ri = rinv[i];
+            cplx fcol[R8];
+#pragma unroll
+            for (int k = 0; k < R8; ++k) {
+                const int r = lane8 + 8 * k;
+                fcol[k] = (r < i) ? F[r * n + i] : cmk(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < CPS; ++q) {
+                cplx x;
+                x.x = __shfl_sync(m, c[q][kk].x, base + l);
+                x.y = __shfl_sync(m, c[q][kk].y, base + l);
+                x = cmul(x, ri);
+                if (lane8 == l) c[q][kk] = x;
+#pragma unroll
+                for (int k = 0; k < R8; ++k) c[q][k] = csub(c[q][k], cmul(fcol[k], x));   // fcol = 0 for rows >= i
+            }
         }
     }
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int j = seg + q * nseg, r = lane8 + 8 * k;
+            if (j < n && r < n) C[r * n + j] = c[q][k];
+        }
+    __syncthreads();
+}
+
+// C <- C diag(cs) R^{-H} (ZTRSM 'R','U','C','N' after scaling column c of C by
+// cs[c]): X R^H = C diag(cs) solved for columns n-1..0.  Each segment holds
+// its rows in registers; column c's value comes from lane c%8.
+template <int R8, int CPS>
+COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
+    const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
+    const unsigned m = seg8_mask();
+    const int base = tid & 24;
+    cplx c[CPS][R8];   // c[q][k] = C[row seg+q*nseg][col lane8+8k]
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = seg + q * nseg, col = lane8 + 8 * k;
+            if (r < n && col < n) {
+                const cplx x = C[r * n + col];
+                const double f = cs[col];
+                c[q][k] = cmk(x.x * f, x.y * f);
+            } else {
+                c[q][k] = cmk(0.0, 0.0);
+            }
+        }
+#pragma unroll
+    for (int kk = R8 - 1; kk >= 0; --kk) {
+        for (int l = 7; l >= 0; --l) {
+            const int cc = 8 * kk + l;
+            if (cc >= n) continue;
+            const cplx ri = cconj(rinv[cc]);   // 1 / conj(R_cc)
+            cplx frow[R8];                      // R[k][cc] for k < cc
+#pragma unroll
+            for (int k = 0; k < R8; ++k) {
+                const int col = lane8 + 8 * k;
+                frow[k] = (col < cc) ? F[col * n + cc] : cmk(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < CPS; ++q) {
+                cplx x;
+                x.x = __shfl_sync(m, c[q][kk].x, base + l);
+                x.y = __shfl_sync(m, c[q][kk].y, base + l);
+                x = cmul(x, ri);
+                if (lane8 == l) c[q][kk] = x;
+#pragma unroll
+                for (int k = 0; k < R8; ++k) c[q][k] = csub(c[q][k], cmulcj(x, frow[k]));
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < CPS; ++q)
+#pragma unroll
+        for (int k = 0; k < R8; ++k) {
+            const int r = seg + q * nseg, col = lane8 + 8 * k;
+            if (r < n && col < n) C[r * n + col] = c[q][k];
+        }
     __syncthreads();
 }
 

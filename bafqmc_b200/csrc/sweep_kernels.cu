@@ -16,10 +16,14 @@ namespace bq {
 __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 
 template <int NMAX> struct Cfg;
-template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4; };
+// R8 rows per lane and CPS columns per 8-lane segment for the register-resident
+// factorisation routines: R8 >= NMAX/8, CPS >= NMAX/(THREADS/8).
+template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1; };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2; };
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
+static_assert(Cfg<16>::R8 * 8 >= 16 && Cfg<16>::CPS * (Cfg<16>::THREADS / 8) >= 16, "register layout must cover NMAX");
+static_assert(Cfg<36>::R8 * 8 >= 36 && Cfg<36>::CPS * (Cfg<36>::THREADS / 8) >= 36, "register layout must cover NMAX");
 
 // Dynamic shared memory of the sweep kernels.  Every buffer sits at a
 // compile-time offset, so device code addresses it without holding pointers.
@@ -78,6 +82,11 @@ struct Smem {
     DEVI uint32_t* seed() const { return at<uint32_t>(oSeed); }
     DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
+
+// green_from_M keeps n complex reciprocals in vn1 | vn2
+static_assert(Smem<16>::oVn1 % 16 == 0 && Smem<36>::oVn1 % 16 == 0 && Smem<16>::oVn2 == Smem<16>::oVn1 + 8 * 16 &&
+                  Smem<36>::oVn2 == Smem<36>::oVn1 + 8 * 36,
+              "vn1 | vn2 must hold NMAX aligned complex values");
 
 // Per-chain view: the chain's arena base and fields in registers, the point
 // parameters in shared memory.
@@ -769,12 +778,12 @@ COLD void stab_UR(Ctx<NMAX> x) {
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W1()[e] = cmul(s.U()[e], x.A().DRc[e % n]);
     __syncthreads();
-    qrp_inplace(n, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DRc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VRc[s.piv()[e / n] * n + e % n];
     __syncthreads();
     gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), op_n(s.W2(), n), TRI_A_UPPER);
-    form_q<Cfg<NMAX>::MAXE>(n, s.W1(), s.tau(), s.U(), false);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.tau(), s.U(), false);
     gcopy(x.A().VRc, s.W2(), n * n);
     __syncthreads();
 }
@@ -790,45 +799,42 @@ COLD void stab_UL(Ctx<NMAX> x) {
         s.W1()[e] = cmul(cconj(s.U()[c * n + r]), x.A().DLc[c]);
     }
     __syncthreads();
-    qrp_inplace(n, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DLc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VLc[(e / n) * n + s.piv()[e % n]];
     __syncthreads();
     gemm_rs<TR, TC>(n, s.W2(), op_n(s.W2(), n), op_c(s.W1(), n), TRI_B_LOWER_FROM_C);
-    form_q<Cfg<NMAX>::MAXE>(n, s.W1(), s.tau(), s.U(), true);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.tau(), s.U(), true);
     gcopy(x.A().VLc, s.W2(), n * n);
     __syncthreads();
 }
 
 // M = U_R^H U_L^H - D_R V_R V_L D_L is in W2 (W1 free); finish stab_green:
-// factor M (or M^H for nt > L/2) and write G = (I - B)^{-1} into W2.
+// factor M (or M^H for nt > L/2) and write G = (I - B)^{-1} into W2.  The
+// D^{-1} scaling before ZTRSM is applied as the solve loads its operand; the
+// reciprocals of R's diagonal and of D live in the QR norm vectors (free once
+// the factorisation is done) and in u2.
 template <int NMAX>
 COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, R8 = Cfg<NMAX>::R8, CPS = Cfg<NMAX>::CPS;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
+    cplx* rinv = reinterpret_cast<cplx*>(s.vn1());   // vn1 | vn2, n complex
+    double* dinv = s.u2();
     if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, s.W2());
-    qrp_inplace(n, s.W2(), s.qr());
+    qrp_inplace<R8, CPS>(n, s.W2(), s.qr());
     if (nt < L / 2 + 1) {
         copy_op(n, s.W1(), URh);
-        apply_qh_left(n, s.W2(), s.tau(), s.W1());
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const double dd = s.d()[e / n];
-            s.W1()[e] = cmk(s.W1()[e].x / dd, s.W1()[e].y / dd);
-        }
-        __syncthreads();
-        trsm_left_upper(n, s.W2(), s.W1());
+        apply_qh_left<R8, CPS>(n, s.W2(), s.tau(), s.W1());
+        diag_inverse(n, s.W2(), s.d(), rinv, dinv);
+        trsm_left_upper<R8, CPS>(n, s.W2(), rinv, dinv, s.W1());
         permute_rows<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
         gemm_rs<TR, TC>(n, s.W2(), ULh, op_n(s.W1(), n));
     } else {
         copy_op(n, s.W1(), ULh);
-        apply_q_right(n, s.W2(), s.tau(), s.W1());
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const double dd = s.d()[e % n];
-            s.W1()[e] = cmk(s.W1()[e].x / dd, s.W1()[e].y / dd);
-        }
-        __syncthreads();
-        trsm_right_upperH(n, s.W2(), s.W1());
+        apply_q_right<R8, CPS>(n, s.W2(), s.tau(), s.W1());
+        diag_inverse(n, s.W2(), s.d(), rinv, dinv);
+        trsm_right_upperH<R8, CPS>(n, s.W2(), rinv, dinv, s.W1());
         permute_cols<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
         gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), URh);
     }

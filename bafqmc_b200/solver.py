@@ -90,6 +90,19 @@ class Ensemble:
         assert flat.size == self.phi_offsets[-1]
         _lib.check(self.lib.bafqmc_set_state(self.h, _iptr(s), _dptr(flat)))
 
+    def set_state_flat(self, seeds: np.ndarray, phi_flat: np.ndarray):
+        """set_state from caller-owned contiguous buffers (int32 seeds, float64
+        fields of all chains back to back), e.g. views of pinned host memory."""
+        assert seeds.dtype == np.int32 and seeds.flags.c_contiguous and seeds.size == self.nchains
+        assert phi_flat.dtype == np.float64 and phi_flat.flags.c_contiguous and phi_flat.size == self.phi_offsets[-1]
+        _lib.check(self.lib.bafqmc_set_state(self.h, _iptr(seeds), _dptr(phi_flat)))
+
+    def get_state_flat(self, seeds: np.ndarray, phi_flat: np.ndarray):
+        """get_state into caller-owned contiguous buffers (see set_state_flat)."""
+        assert seeds.dtype == np.int32 and seeds.flags.c_contiguous and seeds.size == self.nchains
+        assert phi_flat.dtype == np.float64 and phi_flat.flags.c_contiguous and phi_flat.size == self.phi_offsets[-1]
+        _lib.check(self.lib.bafqmc_get_state(self.h, _iptr(seeds), _dptr(phi_flat)))
+
     def get_state(self):
         s = np.zeros(self.nchains, dtype=np.int32)
         flat = np.zeros(int(self.phi_offsets[-1]), dtype=np.float64)

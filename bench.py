@@ -276,17 +276,29 @@ def main():
     chain_sweeps = world * C * args.steps / dev_s
     value, tau = ess_rate(chain_sweeps)
 
-    # ---- end to end through the C ABI: sweep + per-bin results to host buffers
+    # ---- end to end through the C ABI with host buffers: every step is one
+    # checkpointed bin, as a reference run from confin.txt to confout.txt: the
+    # chains' seeds and fields go host -> device from pinned memory
+    # (bafqmc_set_state), bafqmc_pre rebuilds the UDV slots, one sweep, and the
+    # bin records, seeds and fields come back device -> host.
     from bafqmc_b200.multigpu import chain_average, torch_all_reduce
     reduce = torch_all_reduce(device=dev) if world > 1 else (lambda b: b)
+    nphi = int(ens.phi_offsets[-1])
+    h_seeds = torch.empty(C, dtype=torch.int32, pin_memory=True).numpy()
+    h_phi = torch.empty(nphi, dtype=torch.float64, pin_memory=True).numpy()
+    ens.get_state_flat(h_seeds, h_phi)
+    h2d = h_seeds.nbytes + h_phi.nbytes
     d2h = 0
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        ens.set_state_flat(h_seeds, h_phi)
+        ens.pre()
         ens.sweep(1)
         pt = ens.point_obs_raw()
         ch = ens.chain_obs_raw()
-        d2h = pt.nbytes + ch.nbytes
+        ens.get_state_flat(h_seeds, h_phi)
+        d2h = pt.nbytes + ch.nbytes + h_seeds.nbytes + h_phi.nbytes
         # job-wide chain average across GPUs (m_process_obs_equal's MPI_REDUCE)
         job_avg = chain_average(pt[0] * C, C, reduce)
     torch.cuda.synchronize(dev)
@@ -331,7 +343,8 @@ def main():
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"},
         "clocks": clk,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "step": "checkpointed bin: set_state (pinned h2d) + pre + 1 sweep + bins and state d2h"},
         "gpu_launches": 3 * args.steps,
     }
     if cpu is not None:
