@@ -39,7 +39,6 @@ struct zmat {   // row-major complex n x n
     std::vector<double> a;   // interleaved
     explicit zmat(int n_ = 0) : n(n_), a(2 * (size_t)n_ * n_, 0.0) {}
     double& re(int i, int j) { return a[2 * ((size_t)i * n + j)]; }
-    double& im(int i, int j) { return a[2 * ((size_t)i * n + j) + 1]; }
 };
 
 zmat zmul(const zmat& A, const zmat& B) {

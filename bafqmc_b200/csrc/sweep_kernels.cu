@@ -149,7 +149,7 @@ template <int NMAX, bool LEFT>
 COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB;
     auto& s = x.s;
-    const int n = x.n, tid = threadIdx.x, lane = tid & 31;
+    const int n = x.n, tid = threadIdx.x;
     const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
     const double shift = fabs(x.P().shiftLoc);
     const uint32_t s0 = *s.seed();
@@ -187,10 +187,11 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // rows (ra) and row t of the block columns (ca, for t outside the block).
     // Registers are kept in visiting order (slot q = q-th site of the block), and
     // the site loop is unrolled, so every register index is a constant.  A site
-    // costs one barrier: threads stage the site's row and column, every thread
-    // makes the same Metropolis decision, and each updates its own registers.
-    // The rank-1 term is applied as ZGERU does, temp = alpha*y(j), then
-    // A(i,j) += x(i)*temp.
+    // costs one barrier: threads stage the site's row and column, load every
+    // operand of the site into registers, make the same Metropolis decision
+    // and update their own registers.
+    // The rank-1 term is ZGERU's x(i) alpha y(j): grouped x(i) (alpha y(j)) on
+    // the block rows and (x(i) alpha) y(j) on the block columns.
     constexpr int NB = 64;
     for (int k0 = 0; k0 < n; k0 += KB) {
         const int kb = min(KB, n - k0);
@@ -236,39 +237,51 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
                         }
                     }
                     asm volatile("bar.sync 1, 64;" ::: "memory");
-                    cplx coef;
-                    const bool accept = metro_ratio(s.delta()[i], s.rg()[i], s.u2()[i], yr[i], coef);
-                    if (t == 0) {
-                        s.accf()[i] = accept ? 1 : 0;
-                        s.coef()[m] = coef;
+                    // every operand of this site in registers before any arithmetic
+                    const cplx yii = yr[i];
+                    const cplx dl = s.delta()[i];
+                    const double rgv = s.rg()[i], uv = s.u2()[i];
+                    cplx xq[KB], yq[KB];
+#pragma unroll
+                    for (int q = 0; q < KB; ++q) {
+                        xq[q] = (q < kb) ? xr[SITE(q)] : cmk(0.0, 0.0);
+                        yq[q] = (q < kb) ? yr[SITE(q)] : cmk(0.0, 0.0);
                     }
+                    cplx ean = ea, ebn = eb;
+                    if (LEFT) {
+                        ean = s.ean()[i];
+                        ebn = s.ebn()[i];
+                    }
+                    cplx coef;
+                    const bool accept = metro_ratio(dl, rgv, uv, yii, coef);
                     if (accept && tv) {
                         // block rows, column t: temp = coef * (delta(t,i) - y(t))
                         const cplx cy = cmul(coef, cmk((ti ? 1.0 : 0.0) - yt.x, -yt.y));
 #pragma unroll
                         for (int q = 0; q < KB; ++q)
-                            if (q < kb) ra[q] = cfma(xr[SITE(q)], cy, ra[q]);
-                        // row t, block columns: temp = coef * (delta(c,i) - y(c))
+                            if (q < kb) ra[q] = cfma(xq[q], cy, ra[q]);
+                        // row t, block columns: (x(t) coef) (delta(c,i) - y(c))
                         if (!tin) {
+                            const cplx xc = cmul(xt, coef);
 #pragma unroll
-                            for (int q = 0; q < KB; ++q) {
-                                if (q < kb) {
-                                    const cplx yv = yr[SITE(q)];
-                                    const cplx tmp = cmul(coef, cmk(((q == m) ? 1.0 : 0.0) - yv.x, -yv.y));
-                                    ca[q] = cfma(xt, tmp, ca[q]);
-                                }
-                            }
+                            for (int q = 0; q < KB; ++q)
+                                if (q < kb) ca[q] = cfma(xc, cmk(((q == m) ? 1.0 : 0.0) - yq[q].x, -yq[q].y), ca[q]);
                         }
                     }
                     if (LEFT) {   // left sweep: wrap site i with its final field (column i, then row i)
-                        const cplx eaf = accept ? s.ean()[i] : ea;
-                        const cplx ebf = accept ? s.ebn()[i] : eb;
+                        const cplx eaf = accept ? ean : ea;
+                        const cplx ebf = accept ? ebn : eb;
                         if (ti) {
 #pragma unroll
                             for (int q = 0; q < KB; ++q) ra[q] = cmul(ra[q], eaf);
                         }
                         if (!tin) ca[m] = cmul(ca[m], eaf);
                         ra[m] = cmul(ra[m], ebf);
+                    }
+                    // the coefficient for the deferred pass, the flag for the field write-back
+                    if (t == 0) {
+                        s.accf()[i] = accept ? 1 : 0;
+                        s.coef()[m] = coef;
                     }
                 }
             }
@@ -983,7 +996,6 @@ DEVI void measure_any(Ctx<NMAX>& x) {
 // one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
 template <int NMAX, bool PAIR>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs ka, const int* idx, int count) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
