@@ -46,7 +46,8 @@ struct Smem {
     static constexpr size_t oPiv = oObs + sizeof(double) * (kObsScalars + NMAX);
     static constexpr size_t oIpiv = oPiv + sizeof(int) * NMAX, oAccf = oIpiv + sizeof(int) * NMAX;
     static constexpr size_t oIbc = oAccf + sizeof(int) * NMAX, oSeed = oIbc + 4 * sizeof(int);
-    static constexpr size_t bytes() { return oSeed + 16; }
+    static constexpr size_t oSxy = oSeed + 16;   // site coordinates x | y << 16
+    static constexpr size_t bytes() { return oSxy + ((sizeof(int) * NMAX + 15) / 16) * 16; }
 
     template <class T>
     static DEVI T* at(size_t off) { return reinterpret_cast<T*>(bq_smem + off); }
@@ -80,6 +81,7 @@ struct Smem {
     DEVI int* accf() const { return at<int>(oAccf); }
     DEVI int* ibc() const { return at<int>(oIbc); }
     DEVI uint32_t* seed() const { return at<uint32_t>(oSeed); }
+    DEVI int* sxy() const { return at<int>(oSxy); }
     DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
 
@@ -133,6 +135,31 @@ DEVI void load_expT(Ctx<NMAX>& x) {
 // elements, which the wraps of the block's sites do not touch.  The terms are
 // the reference's ZGERU updates; only the order of the additions changes.
 
+// e^{+alpha phi} and e^{-alpha phi} for the HS coupling alpha = ar + i ai of one
+// channel, which the reference makes purely real (U2) or purely imaginary (U1)
+// (operator_Hubbard.f90:36-43): a real alpha needs only exp, an imaginary one
+// one sincos with e^{-i theta} = conj(e^{i theta}).
+DEVI void hs_factors(double ar, double ai, double p, cplx& ep, cplx& em) {
+    if (ai == 0.0) {
+        ep = cmk(exp(ar * p), 0.0);
+        em = cmk(exp(-(ar * p)), 0.0);
+    } else if (ar == 0.0) {
+        double sn, cs;
+        sincos(ai * p, &sn, &cs);
+        ep = cmk(cs, sn);
+        em = cmk(cs, -sn);
+    } else {
+        ep = cexpz(cmk(ar * p, ai * p));
+        em = cexpz(cmk(-(ar * p), -(ai * p)));
+    }
+}
+// e_new / e_old for those factors: a real quotient, or e_new conj(e_old) on the unit circle.
+DEVI cplx ratio_unit(double ar, double ai, cplx en, cplx eo) {
+    if (ai == 0.0) return cmk(en.x / eo.x, 0.0);
+    if (ar == 0.0) return cmulcj(en, eo);
+    return cdiv(en, eo);
+}
+
 // Metropolis ratio for the (wrapped) diagonal element gjj: ratio_det = 1/w,
 // w = 1 + Delta (1 - G_jj); accept if r_gauss |ratio_det|^2 > u; on accept the
 // rank-1 coefficient is -ratio_det * Delta (localU.f90:56-71).
@@ -165,12 +192,14 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
         const double xdif = (xflip - 0.5) * shift;
         const double pn = po + xdif;
         const double go = exp(-0.5 * po * po), gn = exp(-0.5 * pn * pn);
-        const cplx eo = cexpz(cmk(ar * po, ai * po)), en = cexpz(cmk(ar * pn, ai * pn));
+        cplx eo, en, ebo, ebn;
+        hs_factors(ar, ai, po, eo, ebo);
+        hs_factors(ar, ai, pn, en, ebn);
         s.eao()[i] = eo;
         s.ean()[i] = en;
-        s.ebo()[i] = cexpz(cmk(-(ar * po), -(ai * po)));
-        s.ebn()[i] = cexpz(cmk(-(ar * pn), -(ai * pn)));
-        s.delta()[i] = csub(cdiv(en, eo), cmk(1.0, 0.0));
+        s.ebo()[i] = ebo;
+        s.ebn()[i] = ebn;
+        s.delta()[i] = csub(ratio_unit(ar, ai, en, eo), cmk(1.0, 0.0));
         s.rg()[i] = gn / go;
         s.u2()[i] = rnd;
         s.phin()[i] = pn;
@@ -343,21 +372,28 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
         *s.seed() = lcg_mul(c_apow[2 * n], s0);
     }
     {
-        constexpr int MAXE = Cfg<NMAX>::MAXE;
+        constexpr int MAXE = Cfg<NMAX>::MAXE, T = Cfg<NMAX>::THREADS;
         cplx u[MAXE], f[MAXE];
+        int r = tid / n, c = tid - (tid / n) * n;
+        const int dr = T / n, dc = T - (T / n) * n;
 #pragma unroll
         for (int k = 0; k < MAXE; ++k) {
-            const int e = tid + k * blockDim.x;
+            const int e = tid + k * T;
             if (e < n * n) {
-                const int r = e / n, c = e - (e / n) * n;
                 const int site = LEFT ? c : r;
                 u[k] = s.U()[e];
                 f[k] = s.accf()[site] ? s.ean()[site] : s.eao()[site];
             }
+            c += dc;
+            r += dr;
+            if (c >= n) {
+                c -= n;
+                ++r;
+            }
         }
 #pragma unroll
         for (int k = 0; k < MAXE; ++k) {
-            const int e = tid + k * blockDim.x;
+            const int e = tid + k * T;
             if (e < n * n) s.U()[e] = cmul(u[k], f[k]);
         }
     }
@@ -571,8 +607,10 @@ COLD void measure(Ctx<NMAX> x) {
     double v[14];
 #pragma unroll
     for (int k = 0; k < 14; ++k) v[k] = 0.0;
-    for (int e = tid; e < n * n; e += blockDim.x) {
-        const int i = e / n, j = e - (e / n) * n;
+    const int* sxy = s.sxy();
+    const int T = blockDim.x, di = T / n, dj = T - (T / n) * n;
+    int i = tid / n, j = tid - (tid / n) * n;
+    for (int e = tid; e < n * n; e += T) {
         const cplx a = G[i * n + j];                  // Grup(i,j)
         cplx gc = G[j * n + i];                       // Grupc(i,j) = G(j,i) - delta_ij
         if (i == j) gc.x -= 1.0;
@@ -587,8 +625,8 @@ COLD void measure(Ctx<NMAX> x) {
         v[8] += tud.x;
         v[9] += tud.y;
         if (hasK) {
-            const int ix = i % lx, iy = i / lx, jx = j % lx, jy = j / lx;
-            int dx = ix - jx, dy = iy - jy;
+            const int pi = sxy[i], pj = sxy[j];
+            int dx = (pi & 0xffff) - (pj & 0xffff), dy = (pi >> 16) - (pj >> 16);
             dx += (dx < 0) ? lx : 0;
             dy += (dy < 0) ? ly : 0;
             const cplx p = ph[dy * lx + dx];
@@ -599,10 +637,16 @@ COLD void measure(Ctx<NMAX> x) {
             v[4] += p.x * dwr;
             v[5] += p.y * dwr;
         }
+        j += dj;
+        i += di;
+        if (j >= n) {
+            j -= n;
+            ++i;
+        }
     }
     for (int e = tid; e < 3 * n; e += blockDim.x) {   // bonds (x+1,y), (x,y+1), (x-1,y+1) (lattice.f90:98-111)
         const int i = e / 3, nb = e - (e / 3) * 3;
-        const int ix = i % lx, iy = i / lx;
+        const int ix = sxy[i] & 0xffff, iy = sxy[i] >> 16;
         const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
         const int jy = (nb == 0) ? iy : (iy + 1) % ly;
         const int jj = jy * lx + jx;
@@ -678,8 +722,10 @@ COLD void measure_pair(Ctx<NMAX> x) {
     double v[19];
 #pragma unroll
     for (int k = 0; k < 19; ++k) v[k] = 0.0;
-    for (int e = tid; e < ns * ns; e += blockDim.x) {
-        const int i = e / ns, j = e - (e / ns) * ns;
+    const int* sxy = s.sxy();
+    const int T = blockDim.x, stepi = T / ns, stepj = T - (T / ns) * ns;
+    int i = tid / ns, j = tid - (tid / ns) * ns;
+    for (int e = tid; e < ns * ns; e += T) {
         const cplx A = G[i * n + j], B = G[i * n + ns + j], C = G[(ns + i) * n + j], D = G[(ns + i) * n + ns + j];
         const cplx di = G[(ns + i) * n + ns + i], dj = G[(ns + j) * n + ns + j];
         const cplx nbi = cmk(-di.x, di.y), nbj = cmk(-dj.x, dj.y), ncj = cmk(-dj.x, -dj.y);
@@ -691,8 +737,8 @@ COLD void measure_pair(Ctx<NMAX> x) {
         v[3] += dbc.y;
         v[4] += D.x * D.x + D.y * D.y;
         if (hasK) {
-            const int ix = i % lx, iy = i / lx, jx = j % lx, jy = j / lx;
-            int dx = ix - jx, dy = iy - jy;
+            const int pi = sxy[i], pj = sxy[j];
+            int dx = (pi & 0xffff) - (pj & 0xffff), dy = (pi >> 16) - (pj >> 16);
             dx += (dx < 0) ? lx : 0;
             dy += (dy < 0) ? ly : 0;
             const cplx p = ph[dy * lx + dx];
@@ -703,10 +749,16 @@ COLD void measure_pair(Ctx<NMAX> x) {
             v[7] += p.x * dwr;
             v[8] += p.y * dwr;
         }
+        j += stepj;
+        i += stepi;
+        if (j >= ns) {
+            j -= ns;
+            ++i;
+        }
     }
     for (int e = tid; e < 3 * ns; e += blockDim.x) {   // bonds (x+1,y), (x,y+1), (x-1,y+1)
         const int i = e / 3, nb = e - (e / 3) * 3;
-        const int ix = i % lx, iy = i / lx;
+        const int ix = sxy[i] & 0xffff, iy = sxy[i] >> 16;
         const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
         const int jy = (nb == 0) ? iy : (iy + 1) % ly;
         const int jj = jy * lx + jx;
@@ -967,6 +1019,10 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     x.n = x.P().N;
     if (x.P().hasK)
         for (int r = threadIdx.x; r < x.P().Lq && r < NMAX; r += blockDim.x) x.s.ph()[r] = x.P().phaseR[r];
+    for (int i = threadIdx.x; i < x.P().Lq && i < NMAX; i += blockDim.x) {
+        const int lx = x.P().Lx;
+        x.s.sxy()[i] = (i % lx) | ((i / lx) << 16);
+    }
     x.abase = ka.arena + cd.arena_off;
     x.phi = ka.phi + cd.phi_off;
     x.sc = ka.sc + chain;
