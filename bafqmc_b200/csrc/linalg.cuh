@@ -1,5 +1,6 @@
 // CTA-level dense complex FP64 linear algebra on matrices resident in shared
-// memory (row-major, leading dimension n).  Every routine is called by all
+// memory (row-major n x n with leading dimension ld; the sweep kernels use an
+// odd ld so that a column walk touches every shared-memory bank group).  Every routine is called by all
 // threads of the block and returns with the block synchronised.
 //
 // These restate the LAPACK/BLAS operations the reference sweep calls
@@ -39,7 +40,7 @@ enum { TRI_NONE = 0, TRI_A_UPPER = 1, TRI_B_LOWER_FROM_C = 2 };
 // tri = TRI_A_UPPER zeroes A(r,k) for k < r (ZTRMM 'L','U','N');
 // tri = TRI_B_LOWER_FROM_C zeroes B(k,c) for k < c (ZTRMM 'R','U','C').
 template <int TR, int TC>
-COLD void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
+COLD void gemm_rs(int n, int ld, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const int g = threadIdx.x;
     const bool active = g < ncg * nrg;
@@ -77,7 +78,7 @@ COLD void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
 #pragma unroll
             for (int j = 0; j < TC; ++j) {
                 int r = r0 + i, c = c0 + j;
-                if (r < n && c < n) C[r * n + c] = acc[i][j];
+                if (r < n && c < n) C[r * ld + c] = acc[i][j];
             }
     }
     __syncthreads();
@@ -86,7 +87,7 @@ COLD void gemm_rs(int n, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
 // C = A * B with A, B, C n x n row-major in shared memory (C may alias A or
 // B); the per-slice propagation products.
 template <int TR, int TC>
-DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
+DEVI void gemm_smem(int n, int ld, cplx* C, const cplx* A, const cplx* B) {
     const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
     const int g = threadIdx.x;
     const bool active = g < ncg * nrg;
@@ -99,7 +100,7 @@ DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
     if (active) {
         int ra[TR], cb[TC];
 #pragma unroll
-        for (int i = 0; i < TR; ++i) ra[i] = min(r0 + i, n - 1) * n;
+        for (int i = 0; i < TR; ++i) ra[i] = min(r0 + i, n - 1) * ld;
 #pragma unroll
         for (int j = 0; j < TC; ++j) cb[j] = min(c0 + j, n - 1);
         for (int k = 0; k < n; ++k) {
@@ -107,7 +108,7 @@ DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
 #pragma unroll
             for (int i = 0; i < TR; ++i) a[i] = A[ra[i] + k];
 #pragma unroll
-            for (int j = 0; j < TC; ++j) b[j] = B[k * n + cb[j]];
+            for (int j = 0; j < TC; ++j) b[j] = B[k * ld + cb[j]];
 #pragma unroll
             for (int i = 0; i < TR; ++i)
 #pragma unroll
@@ -121,7 +122,7 @@ DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
 #pragma unroll
             for (int j = 0; j < TC; ++j) {
                 const int r = r0 + i, c = c0 + j;
-                if (r < n && c < n) C[r * n + c] = acc[i][j];
+                if (r < n && c < n) C[r * ld + c] = acc[i][j];
             }
     }
     __syncthreads();
@@ -129,25 +130,34 @@ DEVI void gemm_smem(int n, cplx* C, const cplx* A, const cplx* B) {
 
 // dst = op(src) elementwise copy for an n x n matrix (dst must not alias src
 // unless op is the identity view).
-COLD void copy_op(int n, cplx* dst, MatOp src) {
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) dst[e] = src.at(e / n, e % n);
+COLD void copy_op(int n, int ld, cplx* dst, MatOp src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        dst[r * ld + c] = src.at(r, c);
+    }
     __syncthreads();
 }
 
 // In-place conjugate transpose via register staging; MAXE >= ceil(n*n/blockDim).
 template <int MAXE>
-COLD void conj_transpose_inplace(int n, cplx* A) {
+COLD void conj_transpose_inplace(int n, int ld, cplx* A) {
     cplx v[MAXE];
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
-        if (e < n * n) v[k] = cconj(A[(e % n) * n + e / n]);
+        if (e < n * n) {
+            const int r = e / n, c = e - (e / n) * n;
+            v[k] = cconj(A[c * ld + r]);
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
-        if (e < n * n) A[e] = v[k];
+        if (e < n * n) {
+            const int r = e / n, c = e - (e / n) * n;
+            A[r * ld + c] = v[k];
+        }
     }
     __syncthreads();
 }
@@ -172,14 +182,14 @@ DEVI double seg8_max(double v) {
 }
 
 // Overflow-safe 2-norm of column j, rows [r0, n), computed by one 8-lane segment.
-DEVI double seg8_colnorm(int n, const cplx* A, int j, int r0, int lane8) {
+DEVI double seg8_colnorm(int n, int ld, const cplx* A, int j, int r0, int lane8) {
     double m = 0.0;
-    for (int r = r0 + lane8; r < n; r += 8) m = fmax(m, fmax(fabs(A[r * n + j].x), fabs(A[r * n + j].y)));
+    for (int r = r0 + lane8; r < n; r += 8) m = fmax(m, fmax(fabs(A[r * ld + j].x), fabs(A[r * ld + j].y)));
     m = seg8_max(m);
     if (m == 0.0) return 0.0;
     double s = 0.0;
     for (int r = r0 + lane8; r < n; r += 8) {
-        double a = A[r * n + j].x / m, b = A[r * n + j].y / m;
+        double a = A[r * ld + j].x / m, b = A[r * ld + j].y / m;
         s += a * a + b * b;
     }
     s = seg8_sum(s);
@@ -187,10 +197,10 @@ DEVI double seg8_colnorm(int n, const cplx* A, int j, int r0, int lane8) {
 }
 
 // Sum of squares of column j, rows r0..n-1, by one 8-lane segment.
-DEVI double seg8_sumsq_col(int n, const cplx* A, int j, int r0, int lane8) {
+DEVI double seg8_sumsq_col(int n, int ld, const cplx* A, int j, int r0, int lane8) {
     double ss = 0.0;
     for (int r = r0 + lane8; r < n; r += 8) {
-        const cplx a = A[r * n + j];
+        const cplx a = A[r * ld + j];
         ss = fma(a.x, a.x, fma(a.y, a.y, ss));
     }
     return seg8_sum(ss);
@@ -200,10 +210,10 @@ DEVI bool sumsq_unsafe(double ss) { return !(ss <= 1.0e300) || (ss != 0.0 && ss 
 
 // 2-norm of column j rows r0..n-1 (one segment); scaled only when the plain sum
 // of squares would over- or underflow.
-DEVI double seg8_norm(int n, const cplx* A, int j, int r0, int lane8) {
-    const double ss = seg8_sumsq_col(n, A, j, r0, lane8);
+DEVI double seg8_norm(int n, int ld, const cplx* A, int j, int r0, int lane8) {
+    const double ss = seg8_sumsq_col(n, ld, A, j, r0, lane8);
     if (!sumsq_unsafe(ss)) return sqrt(ss);
-    return seg8_colnorm(n, A, j, r0, lane8);
+    return seg8_colnorm(n, ld, A, j, r0, lane8);
 }
 
 // Shared scratch for the factorisations (lives in shared memory, size ~ 6n).
@@ -230,11 +240,11 @@ struct QRScratch {
 // norm downdate is ZLAQP2's, with its quotients multiplied out (no division).
 // R8 >= ceil(n/8) rows per lane, CPS >= ceil(n/segments) columns per segment.
 template <int R8, int CPS>
-COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
+COLD void qrp_inplace(int n, int ld, cplx* A, QRScratch s) {
     const int tid = threadIdx.x, lane = tid & 31, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     const double tol3z = 1.0536712127723509e-08;   // sqrt(2^-53), LAPACK's sqrt(dlamch('E'))
     for (int j = seg; j < n; j += nseg) {
-        const double v = seg8_norm(n, A, j, 0, lane8);
+        const double v = seg8_norm(n, ld, A, j, 0, lane8);
         if (lane8 == 0) { s.vn1[j] = v; s.vn2[j] = v; s.piv[j] = j; }
     }
     __syncthreads();
@@ -259,13 +269,13 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = lane8 + 8 * k;
-            v[k] = (r < n && r > i) ? A[r * n + pvt] : cmk(0.0, 0.0);
+            v[k] = (r < n && r > i) ? A[r * ld + pvt] : cmk(0.0, 0.0);
             ss = fma(v[k].x, v[k].x, fma(v[k].y, v[k].y, ss));
         }
         ss = seg8_sum(ss);
-        const cplx alpha = A[i * n + pvt];
+        const cplx alpha = A[i * ld + pvt];
         double xn = sqrt(ss);
-        if (sumsq_unsafe(ss)) xn = seg8_colnorm(n, A, pvt, i + 1, lane8);
+        if (sumsq_unsafe(ss)) xn = seg8_colnorm(n, ld, A, pvt, i + 1, lane8);
         cplx tau = cmk(0.0, 0.0), beta = alpha, scl = cmk(0.0, 0.0);
         if (!(xn == 0.0 && alpha.y == 0.0)) {
             const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn * xn);
@@ -293,29 +303,29 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
 #pragma unroll
             for (int k = 0; k < R8; ++k) {
                 const int r = lane8 + 8 * k;
-                a[q][k] = (ok && r < n && r >= i) ? A[r * n + src] : cmk(0.0, 0.0);
+                a[q][k] = (ok && r < n && r >= i) ? A[r * ld + src] : cmk(0.0, 0.0);
             }
             t1[q] = ok ? s.vn1[src] : 0.0;
             t2[q] = ok ? s.vn2[src] : 0.0;
         }
         cplx ui = cmk(0.0, 0.0), up = cmk(0.0, 0.0);   // rows < i of columns i and pvt
         if (tid < i) {
-            ui = A[tid * n + i];
-            up = A[tid * n + pvt];
+            ui = A[tid * ld + i];
+            up = A[tid * ld + pvt];
         }
         __syncthreads();
         if (pvt != i && tid < i) {
-            A[tid * n + i] = up;
-            A[tid * n + pvt] = ui;
+            A[tid * ld + i] = up;
+            A[tid * ld + pvt] = ui;
         }
         if (seg == 0) {
 #pragma unroll
             for (int k = 0; k < R8; ++k) {
                 const int r = lane8 + 8 * k;
-                if (r < n && r > i) A[r * n + i] = v[k];
+                if (r < n && r > i) A[r * ld + i] = v[k];
             }
             if (lane8 == 0) {
-                A[i * n + i] = beta;
+                A[i * ld + i] = beta;
                 s.tau[i] = tau;
             }
         }
@@ -343,7 +353,7 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
                 const double m2 = a[q][k].x * a[q][k].x + a[q][k].y * a[q][k].y;
                 if (r == i) ai2 = m2;
                 if (r > i && r < n) rest += m2;
-                if (r < n && r >= i) A[r * n + j] = a[q][k];
+                if (r < n && r >= i) A[r * ld + j] = a[q][k];
             }
             ai2 = seg8_sum(ai2);
             rest = seg8_sum(rest);
@@ -368,7 +378,7 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
                 if (recompute) {
                     if (sumsq_unsafe(rest)) {
                         __syncwarp(seg8_mask());
-                        nv1 = (i + 1 < n) ? seg8_colnorm(n, A, j, i + 1, lane8) : 0.0;
+                        nv1 = (i + 1 < n) ? seg8_colnorm(n, ld, A, j, i + 1, lane8) : 0.0;
                     } else {
                         nv1 = sqrt(rest);
                     }
@@ -384,7 +394,7 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
     }
     // D = |diag R|, rows of the upper triangle scaled by 1/D
     for (int i = tid; i < n; i += blockDim.x) {
-        const cplx a = A[i * n + i];
+        const cplx a = A[i * ld + i];
         const double d = hypot(a.x, a.y);
         s.d[i] = d;
         s.vn1[i] = 1.0 / d;
@@ -394,7 +404,8 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
         const int r = e / n, c = e - (e / n) * n;
         if (c >= r) {
             const double x = s.vn1[r];
-            A[e] = cmk(A[e].x * x, A[e].y * x);
+            const cplx a = A[r * ld + c];
+            A[r * ld + c] = cmk(a.x * x, a.y * x);
         }
     }
     for (int k = tid; k < n; k += blockDim.x) s.ipiv[s.piv[k]] = k;
@@ -403,7 +414,7 @@ COLD void qrp_inplace(int n, cplx* A, QRScratch s) {
 
 // C <- Q^H C (ZUNMQR 'L','C'): each segment holds its columns in registers.
 template <int R8, int CPS>
-COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
+COLD void apply_qh_left(int n, int ld, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     cplx c[CPS][R8];
 #pragma unroll
@@ -411,7 +422,7 @@ COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int j = seg + q * nseg, r = lane8 + 8 * k;
-            c[q][k] = (j < n && r < n) ? C[r * n + j] : cmk(0.0, 0.0);
+            c[q][k] = (j < n && r < n) ? C[r * ld + j] : cmk(0.0, 0.0);
         }
     for (int i = 0; i < n; ++i) {
         const cplx ct = cconj(tau[i]);
@@ -419,7 +430,7 @@ COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = lane8 + 8 * k;
-            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * n + i] : cmk(0.0, 0.0));
+            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * ld + i] : cmk(0.0, 0.0));
         }
 #pragma unroll
         for (int q = 0; q < CPS; ++q) {
@@ -438,14 +449,14 @@ COLD void apply_qh_left(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int j = seg + q * nseg, r = lane8 + 8 * k;
-            if (j < n && r < n) C[r * n + j] = c[q][k];
+            if (j < n && r < n) C[r * ld + j] = c[q][k];
         }
     __syncthreads();
 }
 
 // C <- C Q (ZUNMQR 'R','N'): each segment holds its rows in registers.
 template <int R8, int CPS>
-COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
+COLD void apply_q_right(int n, int ld, const cplx* F, const cplx* tau, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     cplx c[CPS][R8];   // c[q][k] = C[row seg+q*nseg][col lane8+8k]
 #pragma unroll
@@ -453,7 +464,7 @@ COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = seg + q * nseg, col = lane8 + 8 * k;
-            c[q][k] = (r < n && col < n) ? C[r * n + col] : cmk(0.0, 0.0);
+            c[q][k] = (r < n && col < n) ? C[r * ld + col] : cmk(0.0, 0.0);
         }
     for (int i = 0; i < n; ++i) {
         const cplx t = tau[i];
@@ -461,7 +472,7 @@ COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int col = lane8 + 8 * k;
-            v[k] = (col == i) ? cmk(1.0, 0.0) : ((col > i && col < n) ? F[col * n + i] : cmk(0.0, 0.0));
+            v[k] = (col == i) ? cmk(1.0, 0.0) : ((col > i && col < n) ? F[col * ld + i] : cmk(0.0, 0.0));
         }
 #pragma unroll
         for (int q = 0; q < CPS; ++q) {
@@ -480,14 +491,14 @@ COLD void apply_q_right(int n, const cplx* F, const cplx* tau, cplx* C) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = seg + q * nseg, col = lane8 + 8 * k;
-            if (r < n && col < n) C[r * n + col] = c[q][k];
+            if (r < n && col < n) C[r * ld + col] = c[q][k];
         }
     __syncthreads();
 }
 
 // Q = H_0 ... H_{n-1} (ZUNGQR), or Q^H with conjT, written to Q (no alias with F).
 template <int R8, int CPS>
-COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
+COLD void form_q(int n, int ld, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     cplx c[CPS][R8];
 #pragma unroll
@@ -503,7 +514,7 @@ COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = lane8 + 8 * k;
-            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * n + i] : cmk(0.0, 0.0));
+            v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * ld + i] : cmk(0.0, 0.0));
         }
 #pragma unroll
         for (int q = 0; q < CPS; ++q) {
@@ -525,8 +536,8 @@ COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
         for (int k = 0; k < R8; ++k) {
             const int j = seg + q * nseg, r = lane8 + 8 * k;
             if (j < n && r < n) {
-                if (conjT) Q[j * n + r] = cconj(c[q][k]);
-                else Q[r * n + j] = c[q][k];
+                if (conjT) Q[j * ld + r] = cconj(c[q][k]);
+                else Q[r * ld + j] = c[q][k];
             }
         }
     __syncthreads();
@@ -534,9 +545,9 @@ COLD void form_q(int n, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
 
 // Inverses of the diagonal of the upper triangle of F into rinv (n complex),
 // and of the positive vector d into dinv (n reals), for the triangular solves.
-COLD void diag_inverse(int n, const cplx* F, const double* d, cplx* rinv, double* dinv) {
+COLD void diag_inverse(int n, int ld, const cplx* F, const double* d, cplx* rinv, double* dinv) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const cplx a = F[i * n + i];
+        const cplx a = F[i * ld + i];
         const double id2 = 1.0 / (a.x * a.x + a.y * a.y);
         rinv[i] = cmk(a.x * id2, -a.y * id2);
         dinv[i] = 1.0 / d[i];
@@ -548,7 +559,7 @@ COLD void diag_inverse(int n, const cplx* F, const double* d, cplx* rinv, double
 // rs[r]); rinv from diag_inverse.  Each segment holds its columns in
 // registers; row i's value comes from lane i%8 by shuffle.
 template <int R8, int CPS>
-COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
+COLD void trsm_left_upper(int n, int ld, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     const unsigned m = seg8_mask();
     const int base = tid & 24;
@@ -559,7 +570,7 @@ COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* 
         for (int k = 0; k < R8; ++k) {
             const int j = seg + q * nseg, r = lane8 + 8 * k;
             if (j < n && r < n) {
-                const cplx x = C[r * n + j];
+                const cplx x = C[r * ld + j];
                 const double f = rs[r];
                 c[q][k] = cmk(x.x * f, x.y * f);
             } else {
@@ -576,7 +587,7 @@ COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* 
 #pragma unroll
             for (int k = 0; k < R8; ++k) {
                 const int r = lane8 + 8 * k;
-                fcol[k] = (r < i) ? F[r * n + i] : cmk(0.0, 0.0);
+                fcol[k] = (r < i) ? F[r * ld + i] : cmk(0.0, 0.0);
             }
 #pragma unroll
             for (int q = 0; q < CPS; ++q) {
@@ -595,7 +606,7 @@ COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* 
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int j = seg + q * nseg, r = lane8 + 8 * k;
-            if (j < n && r < n) C[r * n + j] = c[q][k];
+            if (j < n && r < n) C[r * ld + j] = c[q][k];
         }
     __syncthreads();
 }
@@ -604,7 +615,7 @@ COLD void trsm_left_upper(int n, const cplx* F, const cplx* rinv, const double* 
 // cs[c]): X R^H = C diag(cs) solved for columns n-1..0.  Each segment holds
 // its rows in registers; column c's value comes from lane c%8.
 template <int R8, int CPS>
-COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
+COLD void trsm_right_upperH(int n, int ld, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
     const int tid = threadIdx.x, lane8 = tid & 7, seg = tid >> 3, nseg = blockDim.x >> 3;
     const unsigned m = seg8_mask();
     const int base = tid & 24;
@@ -615,7 +626,7 @@ COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double
         for (int k = 0; k < R8; ++k) {
             const int r = seg + q * nseg, col = lane8 + 8 * k;
             if (r < n && col < n) {
-                const cplx x = C[r * n + col];
+                const cplx x = C[r * ld + col];
                 const double f = cs[col];
                 c[q][k] = cmk(x.x * f, x.y * f);
             } else {
@@ -632,7 +643,7 @@ COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double
 #pragma unroll
             for (int k = 0; k < R8; ++k) {
                 const int col = lane8 + 8 * k;
-                frow[k] = (col < cc) ? F[col * n + cc] : cmk(0.0, 0.0);
+                frow[k] = (col < cc) ? F[col * ld + cc] : cmk(0.0, 0.0);
             }
 #pragma unroll
             for (int q = 0; q < CPS; ++q) {
@@ -651,7 +662,7 @@ COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double
 #pragma unroll
         for (int k = 0; k < R8; ++k) {
             const int r = seg + q * nseg, col = lane8 + 8 * k;
-            if (r < n && col < n) C[r * n + col] = c[q][k];
+            if (r < n && col < n) C[r * ld + col] = c[q][k];
         }
     __syncthreads();
 }
@@ -659,21 +670,24 @@ COLD void trsm_right_upperH(int n, const cplx* F, const cplx* rinv, const double
 // Row permutation in place.  forward: out[k][:] = in[piv[k]][:] (ZLAPMR .true.,
 // i.e. P^T X); backward: out[piv[k]][:] = in[k][:] (ZLAPMR .false., i.e. P X).
 template <int MAXE>
-COLD void permute_rows(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
+COLD void permute_rows(int n, int ld, cplx* C, const int* piv, const int* ipiv, bool forward) {
     cplx v[MAXE];
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
         if (e < n * n) {
             const int r = e / n, c = e % n;
-            v[k] = C[(forward ? piv[r] : ipiv[r]) * n + c];
+            v[k] = C[(forward ? piv[r] : ipiv[r]) * ld + c];
         }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
-        if (e < n * n) C[e] = v[k];
+        if (e < n * n) {
+            const int r = e / n, c = e - (e / n) * n;
+            C[r * ld + c] = v[k];
+        }
     }
     __syncthreads();
 }
@@ -681,21 +695,24 @@ COLD void permute_rows(int n, cplx* C, const int* piv, const int* ipiv, bool for
 // Column permutation in place.  forward: out[:, k] = in[:, piv[k]] (ZLAPMT
 // .true., X P); backward: out[:, piv[k]] = in[:, k] (ZLAPMT .false., X P^T).
 template <int MAXE>
-COLD void permute_cols(int n, cplx* C, const int* piv, const int* ipiv, bool forward) {
+COLD void permute_cols(int n, int ld, cplx* C, const int* piv, const int* ipiv, bool forward) {
     cplx v[MAXE];
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
         if (e < n * n) {
             const int r = e / n, c = e % n;
-            v[k] = C[r * n + (forward ? piv[c] : ipiv[c])];
+            v[k] = C[r * ld + (forward ? piv[c] : ipiv[c])];
         }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = threadIdx.x + k * blockDim.x;
-        if (e < n * n) C[e] = v[k];
+        if (e < n * n) {
+            const int r = e / n, c = e - (e / n) * n;
+            C[r * ld + c] = v[k];
+        }
     }
     __syncthreads();
 }

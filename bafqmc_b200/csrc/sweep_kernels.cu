@@ -18,9 +18,11 @@ __constant__ uint32_t c_apow[kMaxPow];   // a^k mod 2^31 for k = 0 .. kMaxPow-1
 template <int NMAX> struct Cfg;
 // R8 rows per lane and CPS columns per 8-lane segment for the register-resident
 // factorisation routines: R8 >= NMAX/8, CPS >= NMAX/(THREADS/8).
-template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1; };
+// LD: leading dimension of the shared-memory matrices, odd so that a column
+// walk over 16-byte elements touches all eight bank groups.
+template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17; };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2; };
+template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37; };
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 static_assert(Cfg<16>::R8 * 8 >= 16 && Cfg<16>::CPS * (Cfg<16>::THREADS / 8) >= 16, "register layout must cover NMAX");
 static_assert(Cfg<36>::R8 * 8 >= 36 && Cfg<36>::CPS * (Cfg<36>::THREADS / 8) >= 36, "register layout must cover NMAX");
@@ -32,7 +34,7 @@ extern __shared__ __align__(16) unsigned char bq_smem[];
 template <int NMAX>
 struct Smem {
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
-    static constexpr size_t MM = sizeof(cplx) * NMAX * NMAX, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
+    static constexpr size_t MM = sizeof(cplx) * NMAX * Cfg<NMAX>::LD, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr int KB = Cfg<NMAX>::KB;
     static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
@@ -108,15 +110,37 @@ struct Ctx {
 DEVI void gcopy(cplx* dst, const cplx* src, int count) {
     for (int e = threadIdx.x; e < count; e += blockDim.x) dst[e] = src[e];
 }
-DEVI void set_identity(int n, cplx* A) {
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) A[e] = cmk((e / n) == (e % n) ? 1.0 : 0.0, 0.0);
+// identity in an n x n matrix with leading dimension ld
+DEVI void set_identity(int n, int ld, cplx* A) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        A[r * ld + c] = cmk(r == c ? 1.0 : 0.0, 0.0);
+    }
+}
+// dense n x n (global) <-> shared n x n with leading dimension ld
+DEVI void sload(int n, int ld, cplx* dst, const cplx* src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        dst[r * ld + c] = src[e];
+    }
+}
+DEVI void sstore(int n, int ld, cplx* dst, const cplx* src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        dst[e] = src[r * ld + c];
+    }
+}
+DEVI void scopy(int n, int ld, cplx* dst, const cplx* src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        dst[r * ld + c] = src[r * ld + c];
+    }
 }
 
 template <int NMAX>
 DEVI void load_expT(Ctx<NMAX>& x) {
-    const int nn = x.n * x.n;
-    gcopy(x.s.W1(), x.P().expP, nn);
-    gcopy(x.s.W2(), x.P().expM, nn);
+    sload(x.n, Cfg<NMAX>::LD, x.s.W1(), x.P().expP);
+    sload(x.n, Cfg<NMAX>::LD, x.s.W2(), x.P().expM);
     __syncthreads();
 }
 
@@ -174,7 +198,7 @@ DEVI bool metro_ratio(cplx d, double rg, double u, cplx gjj, cplx& coef) {
 
 template <int NMAX, bool LEFT>
 COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n, tid = threadIdx.x;
     const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
@@ -235,8 +259,8 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
 #pragma unroll
             for (int q = 0; q < KB; ++q) {
                 const int sq = SITE(q);
-                ra[q] = (tv && q < kb) ? G[sq * n + t] : cmk(0.0, 0.0);
-                ca[q] = (tv && q < kb && !tin) ? G[t * n + sq] : cmk(0.0, 0.0);
+                ra[q] = (tv && q < kb) ? G[sq * LD + t] : cmk(0.0, 0.0);
+                ca[q] = (tv && q < kb && !tin) ? G[t * LD + sq] : cmk(0.0, 0.0);
             }
 #pragma unroll
             for (int m = 0; m < KB; ++m) {
@@ -317,8 +341,8 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
 #pragma unroll
             for (int q = 0; q < KB; ++q) {
                 const int sq = SITE(q);
-                if (tv && q < kb) G[sq * n + t] = ra[q];
-                if (tv && q < kb && !tin) G[t * n + sq] = ca[q];
+                if (tv && q < kb) G[sq * LD + t] = ra[q];
+                if (tv && q < kb && !tin) G[t * LD + sq] = ca[q];
             }
 #undef SITE
         }
@@ -334,7 +358,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
                     const int r = r0 + a, c = c0 + b;
                     own[a][b] = r < n && c < n && (unsigned)(r - slo) >= (unsigned)kb &&
                                 (unsigned)(c - slo) >= (unsigned)kb;
-                    g[a][b] = G[min(r, n - 1) * n + min(c, n - 1)];
+                    g[a][b] = G[min(r, n - 1) * LD + min(c, n - 1)];
                 }
 #pragma unroll
             for (int m = 0; m < KB; ++m) {
@@ -357,7 +381,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
             for (int a = 0; a < TR; ++a)
 #pragma unroll
                 for (int b = 0; b < TC; ++b)
-                    if (own[a][b]) G[(r0 + a) * n + c0 + b] = g[a][b];
+                    if (own[a][b]) G[(r0 + a) * LD + c0 + b] = g[a][b];
         }
         __syncthreads();
     }
@@ -373,7 +397,6 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     }
     {
         constexpr int MAXE = Cfg<NMAX>::MAXE, T = Cfg<NMAX>::THREADS;
-        cplx u[MAXE], f[MAXE];
         int r = tid / n, c = tid - (tid / n) * n;
         const int dr = T / n, dc = T - (T / n) * n;
 #pragma unroll
@@ -381,8 +404,8 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
             const int e = tid + k * T;
             if (e < n * n) {
                 const int site = LEFT ? c : r;
-                u[k] = s.U()[e];
-                f[k] = s.accf()[site] ? s.ean()[site] : s.eao()[site];
+                const cplx f = s.accf()[site] ? s.ean()[site] : s.eao()[site];
+                s.U()[r * LD + c] = cmul(s.U()[r * LD + c], f);
             }
             c += dc;
             r += dr;
@@ -390,11 +413,6 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
                 c -= n;
                 ++r;
             }
-        }
-#pragma unroll
-        for (int k = 0; k < MAXE; ++k) {
-            const int e = tid + k * T;
-            if (e < n * n) s.U()[e] = cmul(u[k], f[k]);
         }
     }
     __syncthreads();
@@ -422,7 +440,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
 // updates its own elements.
 template <int NMAX, bool LEFT>
 COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
-    constexpr int MAXE = Cfg<NMAX>::MAXE;
+    constexpr int MAXE = Cfg<NMAX>::MAXE, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n, ns = x.P().Ns, tid = threadIdx.x;
     const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
@@ -467,7 +485,7 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
         const int e = tid + k * blockDim.x;
         er[k] = (e < n * n) ? e / n : -1;
         ec[k] = (e < n * n) ? e - (e / n) * n : -1;
-        g[k] = (e < n * n) ? G[e] : cmk(0.0, 0.0);
+        g[k] = (e < n * n) ? G[er[k] * LD + ec[k]] : cmk(0.0, 0.0);
     }
     for (int q = 0; q < ns; ++q) {
         const int i = LEFT ? ns - 1 - q : q;
@@ -539,7 +557,7 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
     }
 #pragma unroll
     for (int k = 0; k < MAXE; ++k)
-        if (er[k] >= 0) G[tid + k * blockDim.x] = g[k];
+        if (er[k] >= 0) G[er[k] * LD + ec[k]] = g[k];
     __syncthreads();
     for (int i = tid; i < ns; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
@@ -561,7 +579,8 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
             const cplx ep = acc ? s.ean()[site] : s.eao()[site];
             const cplx em = acc ? s.ebn()[site] : s.ebo()[site];
             const cplx f = (idx >= ns && flip) ? em : ep;
-            s.U()[e] = LEFT ? cmul(s.U()[e], f) : cmul(f, s.U()[e]);
+            cplx* u = s.U() + er[k] * LD + ec[k];
+            *u = LEFT ? cmul(*u, f) : cmul(f, *u);
         }
     }
     __syncthreads();
@@ -573,17 +592,17 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
 // right.  e^{-dtau K} is in W1, e^{+dtau K} in W2.
 template <int NMAX, bool LEFT>
 COLD void slice_products(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     if (LEFT) {
-        gemm_smem<TR, TC>(n, s.G(), s.G(), s.W1());
-        gemm_smem<TR, TC>(n, s.G(), s.W2(), s.G());
-        gemm_smem<TR, TC>(n, s.U(), s.U(), s.W1());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), s.W1());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.W2(), s.G());
+        gemm_smem<TR, TC>(n, LD, s.U(), s.U(), s.W1());
     } else {
-        gemm_smem<TR, TC>(n, s.G(), s.W1(), s.G());
-        gemm_smem<TR, TC>(n, s.G(), s.G(), s.W2());
-        gemm_smem<TR, TC>(n, s.U(), s.W1(), s.U());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.W1(), s.G());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), s.W2());
+        gemm_smem<TR, TC>(n, LD, s.U(), s.W1(), s.U());
     }
 }
 
@@ -595,6 +614,7 @@ COLD void slice_products(Ctx<NMAX> x) {
 // displacement r = i - j, so it comes from an Lq-entry table in shared memory.
 template <int NMAX>
 COLD void measure(Ctx<NMAX> x) {
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const PointDev& P = x.P();
     const int n = x.n, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
@@ -611,11 +631,11 @@ COLD void measure(Ctx<NMAX> x) {
     const int T = blockDim.x, di = T / n, dj = T - (T / n) * n;
     int i = tid / n, j = tid - (tid / n) * n;
     for (int e = tid; e < n * n; e += T) {
-        const cplx a = G[i * n + j];                  // Grup(i,j)
-        cplx gc = G[j * n + i];                       // Grupc(i,j) = G(j,i) - delta_ij
+        const cplx a = G[i * LD + j];                 // Grup(i,j)
+        cplx gc = G[j * LD + i];                      // Grupc(i,j) = G(j,i) - delta_ij
         if (i == j) gc.x -= 1.0;
-        const cplx dui = cmk(G[i * n + i].x - 1.0, G[i * n + i].y);
-        const cplx duj = cmk(G[j * n + j].x - 1.0, G[j * n + j].y);
+        const cplx dui = cmk(G[i * LD + i].x - 1.0, G[i * LD + i].y);
+        const cplx duj = cmk(G[j * LD + j].x - 1.0, G[j * LD + j].y);
         const cplx tup = cadd(cmul(dui, duj), cmul(gc, a));   // b-flavour density correlator
         const cplx tud = cmulcj(dui, duj);                     // du_i * dd_j
         v[0] += tup.x;
@@ -650,12 +670,12 @@ COLD void measure(Ctx<NMAX> x) {
         const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
         const int jy = (nb == 0) ? iy : (iy + 1) % ly;
         const int jj = jy * lx + jx;
-        cplx gij = G[jj * n + i], gji = G[i * n + jj];   // Grupc(i,jj), Grupc(jj,i)
+        cplx gij = G[jj * LD + i], gji = G[i * LD + jj];   // Grupc(i,jj), Grupc(jj,i)
         if (i == jj) { gij.x -= 1.0; gji.x -= 1.0; }
         v[10] += 2.0 * (gij.x + gji.x);
     }
     for (int i = tid; i < n; i += blockDim.x) {
-        const cplx du = cmk(G[i * n + i].x - 1.0, G[i * n + i].y);
+        const cplx du = cmk(G[i * LD + i].x - 1.0, G[i * LD + i].y);
         v[11] += du.x;
         v[12] += du.x * du.x + du.y * du.y;
         v[13] += du.x * du.x - du.y * du.y;
@@ -709,6 +729,7 @@ COLD void measure(Ctx<NMAX> x) {
 //   Dcc = conj(Dbb), Dcb = conj(Dbc).
 template <int NMAX>
 COLD void measure_pair(Ctx<NMAX> x) {
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const PointDev& P = x.P();
     const int n = x.n, ns = P.Ns, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
@@ -726,8 +747,8 @@ COLD void measure_pair(Ctx<NMAX> x) {
     const int T = blockDim.x, stepi = T / ns, stepj = T - (T / ns) * ns;
     int i = tid / ns, j = tid - (tid / ns) * ns;
     for (int e = tid; e < ns * ns; e += T) {
-        const cplx A = G[i * n + j], B = G[i * n + ns + j], C = G[(ns + i) * n + j], D = G[(ns + i) * n + ns + j];
-        const cplx di = G[(ns + i) * n + ns + i], dj = G[(ns + j) * n + ns + j];
+        const cplx A = G[i * LD + j], B = G[i * LD + ns + j], C = G[(ns + i) * LD + j], D = G[(ns + i) * LD + ns + j];
+        const cplx di = G[(ns + i) * LD + ns + i], dj = G[(ns + j) * LD + ns + j];
         const cplx nbi = cmk(-di.x, di.y), nbj = cmk(-dj.x, dj.y), ncj = cmk(-dj.x, -dj.y);
         const cplx dbb = csub(cmul(nbi, nbj), cmul(cconj(D), A));
         const cplx dbc = csub(cmul(nbi, ncj), cmul(cconj(C), B));
@@ -762,10 +783,10 @@ COLD void measure_pair(Ctx<NMAX> x) {
         const int jx = (nb == 0) ? (ix + 1) % lx : (nb == 1 ? ix : (ix + lx - 1) % lx);
         const int jy = (nb == 0) ? iy : (iy + 1) % ly;
         const int jj = jy * lx + jx;
-        v[9] += -2.0 * (G[(ns + i) * n + ns + jj].x + G[(ns + jj) * n + ns + i].x);
+        v[9] += -2.0 * (G[(ns + i) * LD + ns + jj].x + G[(ns + jj) * LD + ns + i].x);
     }
     for (int i = tid; i < ns; i += blockDim.x) {
-        const cplx A = G[i * n + i], B = G[i * n + ns + i], C = G[(ns + i) * n + i], D = G[(ns + i) * n + ns + i];
+        const cplx A = G[i * LD + i], B = G[i * LD + ns + i], C = G[(ns + i) * LD + i], D = G[(ns + i) * LD + ns + i];
         const cplx nb = cmk(-D.x, D.y);
         const double nbnc = D.x * D.x + D.y * D.y;          // n_b n_c = |D_ii|^2
         const cplx cb = cmul(cconj(C), B);
@@ -838,39 +859,48 @@ COLD void measure_pair(Ctx<NMAX> x) {
 // U_R is s.U(); on exit the new V_R is in s.W2() and in A.VRc, D_R in A.DRc.
 template <int NMAX>
 COLD void stab_UR(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W1()[e] = cmul(s.U()[e], x.A().DRc[e % n]);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        s.W1()[r * LD + c] = cmul(s.U()[r * LD + c], x.A().DRc[c]);
+    }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DRc[i] = cmk(s.d()[i], 0.0);
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VRc[s.piv()[e / n] * n + e % n];
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        s.W2()[r * LD + c] = x.A().VRc[s.piv()[r] * n + c];
+    }
     __syncthreads();
-    gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), op_n(s.W2(), n), TRI_A_UPPER);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.tau(), s.U(), false);
-    gcopy(x.A().VRc, s.W2(), n * n);
+    gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W1(), LD), op_n(s.W2(), LD), TRI_A_UPPER);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.tau(), s.U(), false);
+    sstore(n, LD, x.A().VRc, s.W2());
     __syncthreads();
 }
 
 // stab_UL: (U_L^H D_L) P = Q R;  D_L <- |diag R|;  V_L <- V_L P R^H;  U_L <- Q^H.
 template <int NMAX>
 COLD void stab_UL(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-        const int r = e / n, c = e % n;
-        s.W1()[e] = cmul(cconj(s.U()[c * n + r]), x.A().DLc[c]);
+        const int r = e / n, c = e - (e / n) * n;
+        s.W1()[r * LD + c] = cmul(cconj(s.U()[c * LD + r]), x.A().DLc[c]);
     }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DLc[i] = cmk(s.d()[i], 0.0);
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.W2()[e] = x.A().VLc[(e / n) * n + s.piv()[e % n]];
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        s.W2()[r * LD + c] = x.A().VLc[r * n + s.piv()[c]];
+    }
     __syncthreads();
-    gemm_rs<TR, TC>(n, s.W2(), op_n(s.W2(), n), op_c(s.W1(), n), TRI_B_LOWER_FROM_C);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, s.W1(), s.tau(), s.U(), true);
-    gcopy(x.A().VLc, s.W2(), n * n);
+    gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W2(), LD), op_c(s.W1(), LD), TRI_B_LOWER_FROM_C);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.tau(), s.U(), true);
+    sstore(n, LD, x.A().VLc, s.W2());
     __syncthreads();
 }
 
@@ -882,26 +912,27 @@ COLD void stab_UL(Ctx<NMAX> x) {
 template <int NMAX>
 COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, R8 = Cfg<NMAX>::R8, CPS = Cfg<NMAX>::CPS;
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
     cplx* rinv = reinterpret_cast<cplx*>(s.vn1());   // vn1 | vn2, n complex
     double* dinv = s.u2();
-    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, s.W2());
-    qrp_inplace<R8, CPS>(n, s.W2(), s.qr());
+    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, LD, s.W2());
+    qrp_inplace<R8, CPS>(n, LD, s.W2(), s.qr());
     if (nt < L / 2 + 1) {
-        copy_op(n, s.W1(), URh);
-        apply_qh_left<R8, CPS>(n, s.W2(), s.tau(), s.W1());
-        diag_inverse(n, s.W2(), s.d(), rinv, dinv);
-        trsm_left_upper<R8, CPS>(n, s.W2(), rinv, dinv, s.W1());
-        permute_rows<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, s.W2(), ULh, op_n(s.W1(), n));
+        copy_op(n, LD, s.W1(), URh);
+        apply_qh_left<R8, CPS>(n, LD, s.W2(), s.tau(), s.W1());
+        diag_inverse(n, LD, s.W2(), s.d(), rinv, dinv);
+        trsm_left_upper<R8, CPS>(n, LD, s.W2(), rinv, dinv, s.W1());
+        permute_rows<Cfg<NMAX>::MAXE>(n, LD, s.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, LD, s.W2(), ULh, op_n(s.W1(), LD));
     } else {
-        copy_op(n, s.W1(), ULh);
-        apply_q_right<R8, CPS>(n, s.W2(), s.tau(), s.W1());
-        diag_inverse(n, s.W2(), s.d(), rinv, dinv);
-        trsm_right_upperH<R8, CPS>(n, s.W2(), rinv, dinv, s.W1());
-        permute_cols<Cfg<NMAX>::MAXE>(n, s.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, s.W2(), op_n(s.W1(), n), URh);
+        copy_op(n, LD, s.W1(), ULh);
+        apply_q_right<R8, CPS>(n, LD, s.W2(), s.tau(), s.W1());
+        diag_inverse(n, LD, s.W2(), s.d(), rinv, dinv);
+        trsm_right_upperH<R8, CPS>(n, LD, s.W2(), rinv, dinv, s.W1());
+        permute_cols<Cfg<NMAX>::MAXE>(n, LD, s.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W1(), LD), URh);
     }
     if (want_logdet) {
         double v[1] = {0.0};
@@ -914,12 +945,13 @@ COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logd
 // M = invULUR - D_R (V_R V_L) D_L with V_R V_L already in W1 and invULUR in W2.
 template <int NMAX>
 DEVI void form_M(Ctx<NMAX>& x) {
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-        const int r = e / n, c = e % n;
-        const cplx t = cmul(x.A().DLc[c], s.W1()[e]);
-        s.W2()[e] = csub(s.W2()[e], cmul(x.A().DRc[r], t));
+        const int r = e / n, c = e - (e / n) * n;
+        const cplx t = cmul(x.A().DLc[c], s.W1()[r * LD + c]);
+        s.W2()[r * LD + c] = csub(s.W2()[r * LD + c], cmul(x.A().DRc[r], t));
     }
     __syncthreads();
 }
@@ -930,7 +962,11 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
     auto& s = x.s;
     const int n = x.n;
     double v[1] = {0.0};
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) v[0] += cabsv(csub(s.W2()[e], s.G()[e]));
+    constexpr int LD = Cfg<NMAX>::LD;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        v[0] += cabsv(csub(s.W2()[r * LD + c], s.G()[r * LD + c]));
+    }
     block_sum<1>(v, s.red());
     if (threadIdx.x == 0) {
         const double dif = v[0];
@@ -938,7 +974,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
         x.sc->xmean += dif;
         if (!(dif == dif) || dif > 1.0e300) x.sc->status |= 1;
     }
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) s.G()[e] = s.W2()[e];
+    scopy(n, LD, s.G(), s.W2());
     __syncthreads();
 }
 
@@ -946,26 +982,26 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
 // and the left side in HBM (A.ULc, A.VLc, A.DLc).
 template <int NMAX>
 COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, s.W1(), op_n(s.W2(), n), op_n(x.A().VLc, n));        // V_R V_L
-    gemm_rs<TR, TC>(n, s.W2(), op_c(s.U(), n), op_c(x.A().ULc, n));         // U_R^H U_L^H
+    gemm_rs<TR, TC>(n, LD, s.W1(), op_n(s.W2(), LD), op_n(x.A().VLc, n));        // V_R V_L
+    gemm_rs<TR, TC>(n, LD, s.W2(), op_c(s.U(), LD), op_c(x.A().ULc, n));         // U_R^H U_L^H
     form_M(x);
-    green_from_M(x, nt, op_c(s.U(), n), op_c(x.A().ULc, n), want_logdet);
+    green_from_M(x, nt, op_c(s.U(), LD), op_c(x.A().ULc, n), want_logdet);
 }
 
 // stab_green with the left side in shared memory (U = U_L, W2 = V_L) and the
 // right side in HBM.
 template <int NMAX>
 COLD void stab_green_left_local(Ctx<NMAX> x, int nt) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, s.W1(), op_n(x.A().VRc, n), op_n(s.W2(), n));
-    gemm_rs<TR, TC>(n, s.W2(), op_c(x.A().URc, n), op_c(s.U(), n));
+    gemm_rs<TR, TC>(n, LD, s.W1(), op_n(x.A().VRc, n), op_n(s.W2(), LD));
+    gemm_rs<TR, TC>(n, LD, s.W2(), op_c(x.A().URc, n), op_c(s.U(), LD));
     form_M(x);
-    green_from_M(x, nt, op_c(x.A().URc, n), op_c(s.U(), n), false);
+    green_from_M(x, nt, op_c(x.A().URc, n), op_c(s.U(), LD), false);
 }
 
 // Wrap_L (stabilization.f90:301-331)
@@ -982,7 +1018,7 @@ COLD void wrap_L(Ctx<NMAX> x, int nt) {
         stab_green_left_local(x, nt);
         drift_and_replace(x);
     }
-    gcopy(x.A().ULs(st), s.U(), n * n);
+    sstore(n, Cfg<NMAX>::LD, x.A().ULs(st), s.U());
     gcopy(x.A().VLs(st), x.A().VLc, n * n);
     gcopy(x.A().DLs(st), x.A().DLc, n);
     __syncthreads();
@@ -1003,7 +1039,7 @@ COLD void wrap_R(Ctx<NMAX> x, int nt) {
         stab_green_right_local(x, nt, nt == x.P().L);
         drift_and_replace(x);
     }
-    gcopy(x.A().URs(st), s.U(), n * n);
+    sstore(n, Cfg<NMAX>::LD, x.A().URs(st), s.U());
     gcopy(x.A().VRs(st), x.A().VRc, n * n);
     gcopy(x.A().DRs(st), x.A().DRc, n);
     __syncthreads();
@@ -1070,8 +1106,8 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
     } while (0)
     if (threadIdx.x == 0) *s.seed() = x.sc->seed;
     load_obs(x);
-    gcopy(s.G(), x.A().G, n * n);
-    gcopy(s.U(), x.A().ULc, n * n);
+    sload(n, Cfg<NMAX>::LD, s.G(), x.A().G);
+    sload(n, Cfg<NMAX>::LD, s.U(), x.A().ULc);
     __syncthreads();
     load_expT(x);
     lap(3);
@@ -1090,10 +1126,10 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
         lap(0);
     }
     wrap_L(x, 0);
-    gcopy(x.A().ULc, s.U(), n * n);
+    sstore(n, Cfg<NMAX>::LD, x.A().ULc, s.U());
     __syncthreads();
     // ---- right traversal
-    gcopy(s.U(), x.A().URc, n * n);
+    sload(n, Cfg<NMAX>::LD, s.U(), x.A().URc);
     __syncthreads();
     wrap_R(x, 0);
     lap(3);
@@ -1110,8 +1146,8 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
         measure_any<NMAX, PAIR>(x);
         lap(2);
     }
-    gcopy(x.A().URc, s.U(), n * n);
-    gcopy(x.A().G, s.G(), n * n);
+    sstore(n, Cfg<NMAX>::LD, x.A().URc, s.U());
+    sstore(n, Cfg<NMAX>::LD, x.A().G, s.G());
     flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
     if (threadIdx.x == 0) x.sc->seed = *s.seed();
     lap(3);
@@ -1124,27 +1160,27 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
 // e^{-alpha phi} in the U2 channel (src/pairing/src/operator_Hubbard.f90:155-166).
 template <int NMAX, bool PAIR>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs ka, const int* idx, int count) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC;
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
     if (!setup_ctx(x, ka, chain)) return;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
-    set_identity(n, s.U());
-    set_identity(n, s.G());
-    set_identity(n, x.A().VRc);
-    set_identity(n, x.A().ULc);
-    set_identity(n, x.A().VLc);
+    set_identity(n, LD, s.U());
+    set_identity(n, LD, s.G());
+    set_identity(n, n, x.A().VRc);
+    set_identity(n, n, x.A().ULc);
+    set_identity(n, n, x.A().VLc);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         x.A().DRc[i] = cmk(1.0, 0.0);
         x.A().DLc[i] = cmk(1.0, 0.0);
     }
     __syncthreads();
-    gcopy(x.A().URs(0), s.U(), n * n);
+    sstore(n, LD, x.A().URs(0), s.U());
     gcopy(x.A().VRs(0), x.A().VRc, n * n);
     gcopy(x.A().DRs(0), x.A().DRc, n);
-    gcopy(s.W1(), x.P().expP, n * n);
+    sload(n, LD, s.W1(), x.P().expP);
     __syncthreads();
     const int ns = x.P().Ns;
     for (int nt = 1; nt <= L; ++nt) {
@@ -1154,34 +1190,34 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs k
             const double ar = x.P().alpha_re[ch], ai = x.P().alpha_im[ch];
             const bool flip = x.P().flip[ch] != 0;
             for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-                const int r = e / n;
+                const int r = e / n, c = e - (e / n) * n;
                 const int site = (PAIR && r >= ns) ? r - ns : r;
                 const double p = ph[site * 2 + ch];
                 const bool neg = PAIR && r >= ns && flip;
                 const cplx f = neg ? cexpz(cmk(-(ar * p), -(ai * p))) : cexpz(cmk(ar * p, ai * p));
-                s.U()[e] = cmul(f, s.U()[e]);
+                s.U()[r * LD + c] = cmul(f, s.U()[r * LD + c]);
             }
             __syncthreads();
         }
-        gemm_rs<TR, TC>(n, s.U(), op_n(s.W1(), n), op_n(s.U(), n));
+        gemm_rs<TR, TC>(n, LD, s.U(), op_n(s.W1(), LD), op_n(s.U(), LD));
         if (nt % x.P().Nwrap == 0) {
             const int st = nt / x.P().Nwrap;
             stab_UR(x);
-            gcopy(x.A().URs(st), s.U(), n * n);
+            sstore(n, LD, x.A().URs(st), s.U());
             gcopy(x.A().VRs(st), x.A().VRc, n * n);
             gcopy(x.A().DRs(st), x.A().DRc, n);
             __syncthreads();
             if (nt == L) {
                 stab_green_right_local(x, nt, true);
-                gcopy(s.G(), s.W2(), n * n);
+                scopy(n, LD, s.G(), s.W2());
                 __syncthreads();
             }
-            gcopy(s.W1(), x.P().expP, n * n);
+            sload(n, LD, s.W1(), x.P().expP);
             __syncthreads();
         }
     }
-    gcopy(x.A().URc, s.U(), n * n);
-    gcopy(x.A().G, s.G(), n * n);
+    sstore(n, LD, x.A().URc, s.U());
+    sstore(n, LD, x.A().G, s.G());
 }
 
 // LocalU_prop_therm / LocalU_metro_therm over the whole field, nwarm sweeps
