@@ -22,9 +22,9 @@ struct KernelArgs {
     int timers;   // nonzero: accumulate per-phase SM cycles into ChainScalars::cyc
 };
 
-// kernel classes of the fused sweep: bit 0 selects the shared-memory size
-// (N <= 16 or N <= 36), bit 1 the sector (0 number-conserving, 1 Nambu)
-constexpr int kNumClasses = 4;
+// kernel classes of the fused sweep: size (N <= 16, N <= 36, N <= 72) + 3 * sector
+// (0 number-conserving, 1 Nambu)
+constexpr int kNumClasses = 6;
 int class_nmax(int cls);
 size_t smem_bytes(int cls);
 int class_of(int n, int pairing);   // -1 if no class holds n

@@ -89,8 +89,16 @@ struct Arena {
     DEVI cplx* DLs(int s) const { return URs(s) + 4 * N * N + N; }
 };
 
-__host__ __device__ inline long long arena_size(int N, int Nst) {
+// Chains with N > kSmemWorkMax keep the two N x N workspaces (e^{-+dtau K} during
+// slice products, QR workspace at wraps) in HBM after the arena, as
+// kWorkNmax x kWorkLd matrices; smaller chains keep them in shared memory.
+constexpr int kSmemWorkMax = 36, kWorkNmax = 72, kWorkLd = 73;
+
+__host__ __device__ inline long long arena_base(int N, int Nst) {
     return 5LL * N * N + 2LL * N + (long long)(Nst + 1) * (4LL * N * N + 2LL * N);
+}
+__host__ __device__ inline long long arena_size(int N, int Nst) {
+    return arena_base(N, Nst) + (N > kSmemWorkMax ? 2LL * kWorkNmax * kWorkLd : 0LL);
 }
 
 DEVI Arena make_arena(cplx* base, int N) {

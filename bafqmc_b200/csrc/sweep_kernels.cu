@@ -19,10 +19,24 @@ template <int NMAX> struct Cfg;
 // R8 rows per lane and CPS columns per 8-lane segment for the register-resident
 // factorisation routines: R8 >= NMAX/8, CPS >= NMAX/(THREADS/8).
 // LD: leading dimension of the shared-memory matrices, odd so that a column
-// walk over 16-byte elements touches all eight bank groups.
-template <> struct Cfg<16> { static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17; };
+// walk over 16-byte elements touches all eight bank groups.  NB: threads of the
+// site strip (>= NMAX, a multiple of 32).  MINB: CTAs per SM for the register
+// budget.
+template <> struct Cfg<16> {
+    static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, NB = 64, MINB = 2;
+};
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
-template <> struct Cfg<36> { static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37; };
+template <> struct Cfg<36> {
+    static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, NB = 64, MINB = 2;
+};
+// N <= 72: G and U in shared memory, the two workspaces in HBM (one CTA per SM)
+template <> struct Cfg<72> {
+    static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = kWorkLd, NB = 96,
+                         MINB = 1;
+};
+static_assert(72 % 3 == 0 && 72 % 4 == 0 && (72 / 3) * (72 / 4) <= 512 && 11 * 512 >= 72 * 72, "N <= 72 tiles");
+static_assert(Cfg<72>::R8 * 8 >= 72 && Cfg<72>::CPS * (512 / 8) >= 72 && Cfg<72>::NB >= 72, "N <= 72 register layout");
+static_assert(Cfg<72>::LD == kWorkLd && 72 == kWorkNmax, "HBM workspace layout");
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 static_assert(Cfg<16>::R8 * 8 >= 16 && Cfg<16>::CPS * (Cfg<16>::THREADS / 8) >= 16, "register layout must cover NMAX");
 static_assert(Cfg<36>::R8 * 8 >= 36 && Cfg<36>::CPS * (Cfg<36>::THREADS / 8) >= 36, "register layout must cover NMAX");
@@ -35,9 +49,10 @@ template <int NMAX>
 struct Smem {
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
     static constexpr size_t MM = sizeof(cplx) * NMAX * Cfg<NMAX>::LD, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
+    static constexpr bool GW = NMAX > kSmemWorkMax;   // workspaces in HBM
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr int KB = Cfg<NMAX>::KB;
-    static constexpr size_t oTau = 4 * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
+    static constexpr size_t oTau = (GW ? 2 : 4) * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
     static constexpr size_t oDelta2 = oDelta + VC;
     static constexpr size_t oEao = oDelta2 + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
     static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + KB * sizeof(cplx);
@@ -55,7 +70,7 @@ struct Smem {
     static DEVI T* at(size_t off) { return reinterpret_cast<T*>(bq_smem + off); }
     DEVI cplx* G() const { return at<cplx>(oG); }
     DEVI cplx* U() const { return at<cplx>(oU); }
-    DEVI cplx* W1() const { return at<cplx>(oW1); }
+    DEVI cplx* W1() const { return at<cplx>(oW1); }   // shared-memory workspaces (N <= 36 classes)
     DEVI cplx* W2() const { return at<cplx>(oW2); }
     DEVI cplx* tau() const { return at<cplx>(oTau); }
     DEVI cplx* col(int m) const { return at<cplx>(oCol) + m * NMAX; }   // column of the m-th site of a block
@@ -88,9 +103,11 @@ struct Smem {
 };
 
 // green_from_M keeps n complex reciprocals in vn1 | vn2
-static_assert(Smem<16>::oVn1 % 16 == 0 && Smem<36>::oVn1 % 16 == 0 && Smem<16>::oVn2 == Smem<16>::oVn1 + 8 * 16 &&
-                  Smem<36>::oVn2 == Smem<36>::oVn1 + 8 * 36,
+static_assert(Smem<16>::oVn1 % 16 == 0 && Smem<36>::oVn1 % 16 == 0 && Smem<72>::oVn1 % 16 == 0 &&
+                  Smem<16>::oVn2 == Smem<16>::oVn1 + 8 * 16 && Smem<36>::oVn2 == Smem<36>::oVn1 + 8 * 36 &&
+                  Smem<72>::oVn2 == Smem<72>::oVn1 + 8 * 72,
               "vn1 | vn2 must hold NMAX aligned complex values");
+static_assert(Smem<72>::bytes() <= 227 * 1024 && 2 * (Smem<36>::bytes() + 1024) <= 228 * 1024, "shared memory per SM");
 
 // Per-chain view: the chain's arena base and fields in registers, the point
 // parameters in shared memory.
@@ -100,9 +117,18 @@ struct Ctx {
     cplx* abase;
     double* phi;
     ChainScalars* sc;
+    cplx* wg;   // HBM workspaces of an N > 36 chain (two NMAX x LD matrices)
     int n;
     DEVI const PointDev& P() const { return *s.P(); }
     DEVI Arena A() const { return make_arena(abase, n); }
+    DEVI cplx* W1() const {
+        if constexpr (Smem<NMAX>::GW) return wg;
+        else return s.W1();
+    }
+    DEVI cplx* W2() const {
+        if constexpr (Smem<NMAX>::GW) return wg + NMAX * Cfg<NMAX>::LD;
+        else return s.W2();
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -139,8 +165,8 @@ DEVI void scopy(int n, int ld, cplx* dst, const cplx* src) {
 
 template <int NMAX>
 DEVI void load_expT(Ctx<NMAX>& x) {
-    sload(x.n, Cfg<NMAX>::LD, x.s.W1(), x.P().expP);
-    sload(x.n, Cfg<NMAX>::LD, x.s.W2(), x.P().expM);
+    sload(x.n, Cfg<NMAX>::LD, x.W1(), x.P().expP);
+    sload(x.n, Cfg<NMAX>::LD, x.W2(), x.P().expM);
     __syncthreads();
 }
 
@@ -245,7 +271,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // and update their own registers.
     // The rank-1 term is ZGERU's x(i) alpha y(j): grouped x(i) (alpha y(j)) on
     // the block rows and (x(i) alpha) y(j) on the block columns.
-    constexpr int NB = 64;
+    constexpr int NB = Cfg<NMAX>::NB;
     for (int k0 = 0; k0 < n; k0 += KB) {
         const int kb = min(KB, n - k0);
         const int slo = LEFT ? n - k0 - kb : k0;   // block sites are slo .. slo+kb-1
@@ -289,7 +315,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
                                 if (q < kb) xr[SITE(q)] = ra[q];
                         }
                     }
-                    asm volatile("bar.sync 1, 64;" ::: "memory");
+                    asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
                     // every operand of this site in registers before any arithmetic
                     const cplx yii = yr[i];
                     const cplx dl = s.delta()[i];
@@ -596,13 +622,13 @@ COLD void slice_products(Ctx<NMAX> x) {
     auto& s = x.s;
     const int n = x.n;
     if (LEFT) {
-        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), s.W1());
-        gemm_smem<TR, TC>(n, LD, s.G(), s.W2(), s.G());
-        gemm_smem<TR, TC>(n, LD, s.U(), s.U(), s.W1());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), x.W1());
+        gemm_smem<TR, TC>(n, LD, s.G(), x.W2(), s.G());
+        gemm_smem<TR, TC>(n, LD, s.U(), s.U(), x.W1());
     } else {
-        gemm_smem<TR, TC>(n, LD, s.G(), s.W1(), s.G());
-        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), s.W2());
-        gemm_smem<TR, TC>(n, LD, s.U(), s.W1(), s.U());
+        gemm_smem<TR, TC>(n, LD, s.G(), x.W1(), s.G());
+        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), x.W2());
+        gemm_smem<TR, TC>(n, LD, s.U(), x.W1(), s.U());
     }
 }
 
@@ -856,7 +882,7 @@ COLD void measure_pair(Ctx<NMAX> x) {
 // stabilisation (stabilization.f90:69-190)
 
 // stab_UR: (U_R D_R) P = Q R;  D_R <- |diag R|;  V_R <- R P^T V_R;  U_R <- Q.
-// U_R is s.U(); on exit the new V_R is in s.W2() and in A.VRc, D_R in A.DRc.
+// U_R is s.U(); on exit the new V_R is in x.W2() and in A.VRc, D_R in A.DRc.
 template <int NMAX>
 COLD void stab_UR(Ctx<NMAX> x) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
@@ -864,19 +890,19 @@ COLD void stab_UR(Ctx<NMAX> x) {
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        s.W1()[r * LD + c] = cmul(s.U()[r * LD + c], x.A().DRc[c]);
+        x.W1()[r * LD + c] = cmul(s.U()[r * LD + c], x.A().DRc[c]);
     }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DRc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        s.W2()[r * LD + c] = x.A().VRc[s.piv()[r] * n + c];
+        x.W2()[r * LD + c] = x.A().VRc[s.piv()[r] * n + c];
     }
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W1(), LD), op_n(s.W2(), LD), TRI_A_UPPER);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.tau(), s.U(), false);
-    sstore(n, LD, x.A().VRc, s.W2());
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), op_n(x.W2(), LD), TRI_A_UPPER);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.tau(), s.U(), false);
+    sstore(n, LD, x.A().VRc, x.W2());
     __syncthreads();
 }
 
@@ -888,19 +914,19 @@ COLD void stab_UL(Ctx<NMAX> x) {
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        s.W1()[r * LD + c] = cmul(cconj(s.U()[c * LD + r]), x.A().DLc[c]);
+        x.W1()[r * LD + c] = cmul(cconj(s.U()[c * LD + r]), x.A().DLc[c]);
     }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.qr());
+    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.qr());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DLc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        s.W2()[r * LD + c] = x.A().VLc[r * n + s.piv()[c]];
+        x.W2()[r * LD + c] = x.A().VLc[r * n + s.piv()[c]];
     }
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W2(), LD), op_c(s.W1(), LD), TRI_B_LOWER_FROM_C);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, s.W1(), s.tau(), s.U(), true);
-    sstore(n, LD, x.A().VLc, s.W2());
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W2(), LD), op_c(x.W1(), LD), TRI_B_LOWER_FROM_C);
+    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.tau(), s.U(), true);
+    sstore(n, LD, x.A().VLc, x.W2());
     __syncthreads();
 }
 
@@ -917,22 +943,22 @@ COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logd
     const int n = x.n, L = x.P().L;
     cplx* rinv = reinterpret_cast<cplx*>(s.vn1());   // vn1 | vn2, n complex
     double* dinv = s.u2();
-    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, LD, s.W2());
-    qrp_inplace<R8, CPS>(n, LD, s.W2(), s.qr());
+    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, LD, x.W2());
+    qrp_inplace<R8, CPS>(n, LD, x.W2(), s.qr());
     if (nt < L / 2 + 1) {
-        copy_op(n, LD, s.W1(), URh);
-        apply_qh_left<R8, CPS>(n, LD, s.W2(), s.tau(), s.W1());
-        diag_inverse(n, LD, s.W2(), s.d(), rinv, dinv);
-        trsm_left_upper<R8, CPS>(n, LD, s.W2(), rinv, dinv, s.W1());
-        permute_rows<Cfg<NMAX>::MAXE>(n, LD, s.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, LD, s.W2(), ULh, op_n(s.W1(), LD));
+        copy_op(n, LD, x.W1(), URh);
+        apply_qh_left<R8, CPS>(n, LD, x.W2(), s.tau(), x.W1());
+        diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
+        trsm_left_upper<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
+        permute_rows<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, LD, x.W2(), ULh, op_n(x.W1(), LD));
     } else {
-        copy_op(n, LD, s.W1(), ULh);
-        apply_q_right<R8, CPS>(n, LD, s.W2(), s.tau(), s.W1());
-        diag_inverse(n, LD, s.W2(), s.d(), rinv, dinv);
-        trsm_right_upperH<R8, CPS>(n, LD, s.W2(), rinv, dinv, s.W1());
-        permute_cols<Cfg<NMAX>::MAXE>(n, LD, s.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, LD, s.W2(), op_n(s.W1(), LD), URh);
+        copy_op(n, LD, x.W1(), ULh);
+        apply_q_right<R8, CPS>(n, LD, x.W2(), s.tau(), x.W1());
+        diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
+        trsm_right_upperH<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
+        permute_cols<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
+        gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), URh);
     }
     if (want_logdet) {
         double v[1] = {0.0};
@@ -950,8 +976,8 @@ DEVI void form_M(Ctx<NMAX>& x) {
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        const cplx t = cmul(x.A().DLc[c], s.W1()[r * LD + c]);
-        s.W2()[r * LD + c] = csub(s.W2()[r * LD + c], cmul(x.A().DRc[r], t));
+        const cplx t = cmul(x.A().DLc[c], x.W1()[r * LD + c]);
+        x.W2()[r * LD + c] = csub(x.W2()[r * LD + c], cmul(x.A().DRc[r], t));
     }
     __syncthreads();
 }
@@ -965,7 +991,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
     constexpr int LD = Cfg<NMAX>::LD;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        v[0] += cabsv(csub(s.W2()[r * LD + c], s.G()[r * LD + c]));
+        v[0] += cabsv(csub(x.W2()[r * LD + c], s.G()[r * LD + c]));
     }
     block_sum<1>(v, s.red());
     if (threadIdx.x == 0) {
@@ -974,7 +1000,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
         x.sc->xmean += dif;
         if (!(dif == dif) || dif > 1.0e300) x.sc->status |= 1;
     }
-    scopy(n, LD, s.G(), s.W2());
+    scopy(n, LD, s.G(), x.W2());
     __syncthreads();
 }
 
@@ -985,8 +1011,8 @@ COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, LD, s.W1(), op_n(s.W2(), LD), op_n(x.A().VLc, n));        // V_R V_L
-    gemm_rs<TR, TC>(n, LD, s.W2(), op_c(s.U(), LD), op_c(x.A().ULc, n));         // U_R^H U_L^H
+    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W2(), LD), op_n(x.A().VLc, n));        // V_R V_L
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(s.U(), LD), op_c(x.A().ULc, n));         // U_R^H U_L^H
     form_M(x);
     green_from_M(x, nt, op_c(s.U(), LD), op_c(x.A().ULc, n), want_logdet);
 }
@@ -998,8 +1024,8 @@ COLD void stab_green_left_local(Ctx<NMAX> x, int nt) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, LD, s.W1(), op_n(x.A().VRc, n), op_n(s.W2(), LD));
-    gemm_rs<TR, TC>(n, LD, s.W2(), op_c(x.A().URc, n), op_c(s.U(), LD));
+    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.A().VRc, n), op_n(x.W2(), LD));
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.A().URc, n), op_c(s.U(), LD));
     form_M(x);
     green_from_M(x, nt, op_c(x.A().URc, n), op_c(s.U(), LD), false);
 }
@@ -1060,6 +1086,7 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
         x.s.sxy()[i] = (i % lx) | ((i / lx) << 16);
     }
     x.abase = ka.arena + cd.arena_off;
+    x.wg = x.abase + arena_base(x.n, x.P().Nst);
     x.phi = ka.phi + cd.phi_off;
     x.sc = ka.sc + chain;
     return x.n <= NMAX;
@@ -1087,7 +1114,7 @@ DEVI void measure_any(Ctx<NMAX>& x) {
 
 // one sweep: Local_sweep_L then Local_sweep_R (local_sweep.f90:96-134)
 template <int NMAX, bool PAIR>
-__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs ka, const int* idx, int count) {
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_kernel(KernelArgs ka, const int* idx, int count) {
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
@@ -1159,7 +1186,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) sweep_kernel(KernelArgs
 // factors (multiply.f90:7-16); for a Nambu chain row Ns+i (c^dagger_i) takes
 // e^{-alpha phi} in the U2 channel (src/pairing/src/operator_Hubbard.f90:155-166).
 template <int NMAX, bool PAIR>
-__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs ka, const int* idx, int count) {
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kernel(KernelArgs ka, const int* idx, int count) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
@@ -1180,7 +1207,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs k
     sstore(n, LD, x.A().URs(0), s.U());
     gcopy(x.A().VRs(0), x.A().VRc, n * n);
     gcopy(x.A().DRs(0), x.A().DRc, n);
-    sload(n, LD, s.W1(), x.P().expP);
+    sload(n, LD, x.W1(), x.P().expP);
     __syncthreads();
     const int ns = x.P().Ns;
     for (int nt = 1; nt <= L; ++nt) {
@@ -1199,7 +1226,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs k
             }
             __syncthreads();
         }
-        gemm_rs<TR, TC>(n, LD, s.U(), op_n(s.W1(), LD), op_n(s.U(), LD));
+        gemm_rs<TR, TC>(n, LD, s.U(), op_n(x.W1(), LD), op_n(s.U(), LD));
         if (nt % x.P().Nwrap == 0) {
             const int st = nt / x.P().Nwrap;
             stab_UR(x);
@@ -1209,10 +1236,10 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 2) pre_kernel(KernelArgs k
             __syncthreads();
             if (nt == L) {
                 stab_green_right_local(x, nt, true);
-                scopy(n, LD, s.G(), s.W2());
+                scopy(n, LD, s.G(), x.W2());
                 __syncthreads();
             }
-            sload(n, LD, s.W1(), x.P().expP);
+            sload(n, LD, x.W1(), x.P().expP);
             __syncthreads();
         }
     }
@@ -1355,13 +1382,15 @@ static cudaError_t launch_cls(int which, const KernelArgs& ka, const int* idx, i
     return cudaGetLastError();
 }
 
-// class index: bit 0 = size class (NMAX 16 / 36), bit 1 = Nambu sector
+// class index: size class (NMAX 16 / 36 / 72) + 3 * Nambu sector
 static cudaError_t launch_any(int which, int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
     switch (cls) {
         case 0: return launch_cls<16, false>(which, ka, idx, count, st);
         case 1: return launch_cls<36, false>(which, ka, idx, count, st);
-        case 2: return launch_cls<16, true>(which, ka, idx, count, st);
-        case 3: return launch_cls<36, true>(which, ka, idx, count, st);
+        case 2: return launch_cls<72, false>(which, ka, idx, count, st);
+        case 3: return launch_cls<16, true>(which, ka, idx, count, st);
+        case 4: return launch_cls<36, true>(which, ka, idx, count, st);
+        case 5: return launch_cls<72, true>(which, ka, idx, count, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1398,11 +1427,17 @@ cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st
     field_norm_kernel<<<ka.nchains, 256, 0, st>>>(ka, out);
     return cudaGetLastError();
 }
-size_t smem_bytes(int cls) { return (cls & 1) == 0 ? Smem<16>::bytes() : Smem<36>::bytes(); }
-int class_nmax(int cls) { return (cls & 1) == 0 ? 16 : 36; }
+size_t smem_bytes(int cls) {
+    const int sz = cls % 3;
+    return sz == 0 ? Smem<16>::bytes() : (sz == 1 ? Smem<36>::bytes() : Smem<72>::bytes());
+}
+int class_nmax(int cls) {
+    const int sz = cls % 3;
+    return sz == 0 ? 16 : (sz == 1 ? 36 : 72);
+}
 int class_of(int n, int pairing) {
-    for (int c = 0; c < 2; ++c)
-        if (n <= class_nmax(c)) return c + (pairing ? 2 : 0);
+    for (int c = 0; c < 3; ++c)
+        if (n <= class_nmax(c)) return c + (pairing ? 3 : 0);
     return -1;
 }
 

@@ -206,3 +206,9 @@ def test_run_directory_pairing_program(solver_mod, tmp_path):
     assert int(toks[0]) == chains[0].seed
     np.testing.assert_array_equal(np.array([float(t) for t in toks[1:1 + chains[0].phi.size]]),
                                   chains[0].phi.ravel())
+
+
+def test_nambu_6x6_in_the_n72_class(solver_mod):
+    """2Ns = 72: G and U in shared memory, the two workspaces in HBM."""
+    op, sp = pair_params(0.5, mu=-6.0, Nlx=6, Nly=6, Ltrot=20, Beta=1.0, Nwrap=5)
+    _run_both([op], [sp], [0, 0], [606, 607], nbins=1)

@@ -187,3 +187,11 @@ def test_ragged_points_one_handle(solver_mod):
         assert_green_close(ens.green(c), chains[0].prop.Gr, f"chain {c}")
         compare_bin(cobs[c], chains[0].obs.as_dict(latt), f"chain {c}")
     ens.close()
+
+
+@pytest.mark.parametrize("lx,ly", [(8, 8), (6, 7)])
+def test_n72_class_against_oracle(solver_mod, lx, ly):
+    """N = 64 and 42 sites: the size class with G and U in shared memory and
+    the two workspaces in HBM, one CTA per SM; 6x7 has no K point."""
+    op, sp = both_params(U2=-0.5, Nlx=lx, Nly=ly, Ltrot=20, Beta=1.0, Nwrap=5)
+    _run_both(op, sp, [31, 32], nbins=1)
