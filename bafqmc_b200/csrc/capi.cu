@@ -365,7 +365,7 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         }
         const PointHost& ph = h->pts[p];
         h->arena_off[c] = h->arena_total;
-        h->arena_total += bq::arena_size(ph.N, ph.Nst);
+        h->arena_total += bq::arena_size(ph.N, ph.Nst, bq::class_work_elems(point_class(ph)));
         h->phi_off[c] = h->phi_total;
         h->phi_total += (long long)ph.p.Ltrot * ph.Lq * 2;
         h->cls_list[point_class(ph)].push_back(c);
@@ -737,7 +737,7 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     if (rc != BAFQMC_OK) return rc;
     const int n = ph.N, cls = point_class(ph);
     const int stride = bq::kObsScalars + ph.Lq;
-    const long long asz = bq::arena_size(n, ph.Nst);
+    const long long asz = bq::arena_size(n, ph.Nst, bq::class_work_elems(cls));
     // scratch layout: point | chains | scalars | index list | matrices | observables | arenas
     const size_t o_pt = 0;
     const size_t o_ch = align256(o_pt + sizeof(PointDev));

@@ -28,6 +28,7 @@ constexpr int kNumClasses = 6;
 int class_nmax(int cls);
 size_t smem_bytes(int cls);
 int class_of(int n, int pairing);   // -1 if no class holds n
+long long class_work_elems(int cls); // complex values of HBM workspace per chain
 
 cudaError_t upload_pow_table(const uint32_t* tab, int count);
 cudaError_t launch_sweep(int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st);

@@ -89,16 +89,14 @@ struct Arena {
     DEVI cplx* DLs(int s) const { return URs(s) + 4 * N * N + N; }
 };
 
-// Chains with N > kSmemWorkMax keep the two N x N workspaces (e^{-+dtau K} during
-// slice products, QR workspace at wraps) in HBM after the arena, as
-// kWorkNmax x kWorkLd matrices; smaller chains keep them in shared memory.
-constexpr int kSmemWorkMax = 36, kWorkNmax = 72, kWorkLd = 73;
-
 __host__ __device__ inline long long arena_base(int N, int Nst) {
     return 5LL * N * N + 2LL * N + (long long)(Nst + 1) * (4LL * N * N + 2LL * N);
 }
-__host__ __device__ inline long long arena_size(int N, int Nst) {
-    return arena_base(N, Nst) + (N > kSmemWorkMax ? 2LL * kWorkNmax * kWorkLd : 0LL);
+// Kernel classes that keep the two workspaces (e^{-+dtau K} during slice
+// products, QR workspace at wraps) in HBM append them after the arena:
+// work = 2 * NMAX * LD complex values of the class, 0 otherwise.
+__host__ __device__ inline long long arena_size(int N, int Nst, long long work) {
+    return arena_base(N, Nst) + work;
 }
 
 DEVI Arena make_arena(cplx* base, int N) {

@@ -21,22 +21,33 @@ template <int NMAX> struct Cfg;
 // LD: leading dimension of the shared-memory matrices, odd so that a column
 // walk over 16-byte elements touches all eight bank groups.  NB: threads of the
 // site strip (>= NMAX, a multiple of 32).  MINB: CTAs per SM for the register
-// budget.
+// budget.  GW: the two workspaces live in HBM (after the chain's arena) and
+// only G and U in shared memory.
 template <> struct Cfg<16> {
     static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, NB = 64, MINB = 2;
+    static constexpr bool GW = false;
 };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
+// N <= 36: two CTAs per SM, all four matrices in shared memory.  (Three CTAs
+// per SM at 192 threads with the workspaces in HBM measured 42% slower: the
+// slice products and wraps slow down more than the third chain adds.)
 template <> struct Cfg<36> {
     static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, NB = 64, MINB = 2;
+    static constexpr bool GW = false;
 };
-// N <= 72: G and U in shared memory, the two workspaces in HBM (one CTA per SM)
+// N <= 72: G and U in shared memory, the workspaces in HBM (one CTA per SM)
 template <> struct Cfg<72> {
-    static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = kWorkLd, NB = 96,
-                         MINB = 1;
+    static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = 73, NB = 96, MINB = 1;
+    static constexpr bool GW = true;
 };
-static_assert(72 % 3 == 0 && 72 % 4 == 0 && (72 / 3) * (72 / 4) <= 512 && 11 * 512 >= 72 * 72, "N <= 72 tiles");
-static_assert(Cfg<72>::R8 * 8 >= 72 && Cfg<72>::CPS * (512 / 8) >= 72 && Cfg<72>::NB >= 72, "N <= 72 register layout");
-static_assert(Cfg<72>::LD == kWorkLd && 72 == kWorkNmax, "HBM workspace layout");
+template <int NMAX>
+constexpr bool cfg_ok() {
+    using C = Cfg<NMAX>;
+    return NMAX % C::TR == 0 && NMAX % C::TC == 0 && (NMAX / C::TR) * (NMAX / C::TC) <= C::THREADS &&
+           C::MAXE * C::THREADS >= NMAX * NMAX && C::R8 * 8 >= NMAX && C::CPS * (C::THREADS / 8) >= NMAX &&
+           C::NB >= NMAX && C::NB % 32 == 0 && C::NB <= C::THREADS && (C::LD & 1) == 1 && C::LD >= NMAX;
+}
+static_assert(cfg_ok<16>() && cfg_ok<36>() && cfg_ok<72>(), "class tiles and register layouts must cover NMAX");
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 static_assert(Cfg<16>::R8 * 8 >= 16 && Cfg<16>::CPS * (Cfg<16>::THREADS / 8) >= 16, "register layout must cover NMAX");
 static_assert(Cfg<36>::R8 * 8 >= 36 && Cfg<36>::CPS * (Cfg<36>::THREADS / 8) >= 36, "register layout must cover NMAX");
@@ -49,7 +60,7 @@ template <int NMAX>
 struct Smem {
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
     static constexpr size_t MM = sizeof(cplx) * NMAX * Cfg<NMAX>::LD, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
-    static constexpr bool GW = NMAX > kSmemWorkMax;   // workspaces in HBM
+    static constexpr bool GW = Cfg<NMAX>::GW;   // workspaces in HBM
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr int KB = Cfg<NMAX>::KB;
     static constexpr size_t oTau = (GW ? 2 : 4) * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
@@ -107,7 +118,9 @@ static_assert(Smem<16>::oVn1 % 16 == 0 && Smem<36>::oVn1 % 16 == 0 && Smem<72>::
                   Smem<16>::oVn2 == Smem<16>::oVn1 + 8 * 16 && Smem<36>::oVn2 == Smem<36>::oVn1 + 8 * 36 &&
                   Smem<72>::oVn2 == Smem<72>::oVn1 + 8 * 72,
               "vn1 | vn2 must hold NMAX aligned complex values");
-static_assert(Smem<72>::bytes() <= 227 * 1024 && 2 * (Smem<36>::bytes() + 1024) <= 228 * 1024, "shared memory per SM");
+template <int NMAX>
+constexpr bool smem_fits() { return Cfg<NMAX>::MINB * (Smem<NMAX>::bytes() + 1024) <= 228 * 1024; }
+static_assert(smem_fits<16>() && smem_fits<36>() && smem_fits<72>(), "shared memory per SM for MINB CTAs");
 
 // Per-chain view: the chain's arena base and fields in registers, the point
 // parameters in shared memory.
@@ -1426,6 +1439,12 @@ cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* star
 cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st) {
     field_norm_kernel<<<ka.nchains, 256, 0, st>>>(ka, out);
     return cudaGetLastError();
+}
+long long class_work_elems(int cls) {
+    const int sz = cls % 3;
+    auto w = [](int nmax, int ld, bool gw) { return gw ? 2LL * nmax * ld : 0LL; };
+    return sz == 0 ? w(16, Cfg<16>::LD, Cfg<16>::GW)
+                   : (sz == 1 ? w(36, Cfg<36>::LD, Cfg<36>::GW) : w(72, Cfg<72>::LD, Cfg<72>::GW));
 }
 size_t smem_bytes(int cls) {
     const int sz = cls % 3;
