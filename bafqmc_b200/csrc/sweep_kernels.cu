@@ -948,14 +948,22 @@ COLD void stab_UL(Ctx<NMAX> x) {
 // D^{-1} scaling before ZTRSM is applied as the solve loads its operand; the
 // reciprocals of R's diagonal and of D live in the QR norm vectors (free once
 // the factorisation is done) and in u2.
+//
+// right_local: the right side (U_R) is in shared memory and U_L in HBM
+// (stab_green_right_local); otherwise the left side is local and U_R in HBM.
+// The HBM factor of the final product is staged into W2 (free after the
+// triangular solve) so that every product runs on shared memory.
 template <int NMAX>
-COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logdet) {
+COLD void green_from_M(Ctx<NMAX> x, int nt, bool right_local, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, R8 = Cfg<NMAX>::R8, CPS = Cfg<NMAX>::CPS;
     constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
     cplx* rinv = reinterpret_cast<cplx*>(s.vn1());   // vn1 | vn2, n complex
     double* dinv = s.u2();
+    const MatOp Uloc = op_c(s.U(), LD);
+    const MatOp URh = right_local ? Uloc : op_c(x.A().URc, n);
+    const MatOp ULh = right_local ? op_c(x.A().ULc, n) : Uloc;
     if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, LD, x.W2());
     qrp_inplace<R8, CPS>(n, LD, x.W2(), s.qr());
     if (nt < L / 2 + 1) {
@@ -964,14 +972,26 @@ COLD void green_from_M(Ctx<NMAX> x, int nt, MatOp URh, MatOp ULh, bool want_logd
         diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
         trsm_left_upper<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
         permute_rows<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, LD, x.W2(), ULh, op_n(x.W1(), LD));
+        if (right_local) {   // U_L^H from HBM, staged
+            sload(n, LD, x.W2(), x.A().ULc);
+            __syncthreads();
+            gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.W2(), LD), op_n(x.W1(), LD));
+        } else {
+            gemm_rs<TR, TC>(n, LD, x.W2(), Uloc, op_n(x.W1(), LD));
+        }
     } else {
         copy_op(n, LD, x.W1(), ULh);
         apply_q_right<R8, CPS>(n, LD, x.W2(), s.tau(), x.W1());
         diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
         trsm_right_upperH<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
         permute_cols<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
-        gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), URh);
+        if (right_local) {
+            gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), Uloc);
+        } else {             // U_R^H from HBM, staged
+            sload(n, LD, x.W2(), x.A().URc);
+            __syncthreads();
+            gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), op_c(x.W2(), LD));
+        }
     }
     if (want_logdet) {
         double v[1] = {0.0};
@@ -1024,10 +1044,17 @@ COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W2(), LD), op_n(x.A().VLc, n));        // V_R V_L
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(s.U(), LD), op_c(x.A().ULc, n));         // U_R^H U_L^H
+    // HBM operands are staged into the workspace the product overwrites (the
+    // products stage their results in registers, so C may alias an operand);
+    // V_R in W2 is no longer needed after the first product (VRc holds it).
+    sload(n, LD, x.W1(), x.A().VLc);
+    __syncthreads();
+    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W2(), LD), op_n(x.W1(), LD));   // V_R V_L
+    sload(n, LD, x.W2(), x.A().ULc);
+    __syncthreads();
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(s.U(), LD), op_c(x.W2(), LD));    // U_R^H U_L^H
     form_M(x);
-    green_from_M(x, nt, op_c(s.U(), LD), op_c(x.A().ULc, n), want_logdet);
+    green_from_M(x, nt, true, want_logdet);
 }
 
 // stab_green with the left side in shared memory (U = U_L, W2 = V_L) and the
@@ -1037,10 +1064,14 @@ COLD void stab_green_left_local(Ctx<NMAX> x, int nt) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
-    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.A().VRc, n), op_n(x.W2(), LD));
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.A().URc, n), op_c(s.U(), LD));
+    sload(n, LD, x.W1(), x.A().VRc);
+    __syncthreads();
+    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W1(), LD), op_n(x.W2(), LD));   // V_R V_L
+    sload(n, LD, x.W2(), x.A().URc);
+    __syncthreads();
+    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.W2(), LD), op_c(s.U(), LD));    // U_R^H U_L^H
     form_M(x);
-    green_from_M(x, nt, op_c(x.A().URc, n), op_c(s.U(), LD), false);
+    green_from_M(x, nt, false, false);
 }
 
 // Wrap_L (stabilization.f90:301-331)
