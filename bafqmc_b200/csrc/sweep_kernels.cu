@@ -176,10 +176,18 @@ DEVI void scopy(int n, int ld, cplx* dst, const cplx* src) {
     }
 }
 
+// e^{-dtau K} (real) into W1 and e^{+dtau K} into W2 as doubles with the
+// matrices' leading dimension.
+DEVI void sload_real(int n, int ld, double* dst, const cplx* src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - (e / n) * n;
+        dst[r * ld + c] = src[e].x;
+    }
+}
 template <int NMAX>
 DEVI void load_expT(Ctx<NMAX>& x) {
-    sload(x.n, Cfg<NMAX>::LD, x.W1(), x.P().expP);
-    sload(x.n, Cfg<NMAX>::LD, x.W2(), x.P().expM);
+    sload_real(x.n, Cfg<NMAX>::LD, reinterpret_cast<double*>(x.W1()), x.P().expP);
+    sload_real(x.n, Cfg<NMAX>::LD, reinterpret_cast<double*>(x.W2()), x.P().expM);
     __syncthreads();
 }
 
@@ -634,14 +642,16 @@ COLD void slice_products(Ctx<NMAX> x) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
+    const double* P = reinterpret_cast<const double*>(x.W1());   // e^{-dtau K}, real
+    const double* M = reinterpret_cast<const double*>(x.W2());   // e^{+dtau K}, real
     if (LEFT) {
-        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), x.W1());
-        gemm_smem<TR, TC>(n, LD, s.G(), x.W2(), s.G());
-        gemm_smem<TR, TC>(n, LD, s.U(), s.U(), x.W1());
+        gemm_smem_real<TR, TC, true>(n, LD, s.G(), s.G(), P);
+        gemm_smem_real<TR, TC, false>(n, LD, s.G(), M, s.G());
+        gemm_smem_real<TR, TC, true>(n, LD, s.U(), s.U(), P);
     } else {
-        gemm_smem<TR, TC>(n, LD, s.G(), x.W1(), s.G());
-        gemm_smem<TR, TC>(n, LD, s.G(), s.G(), x.W2());
-        gemm_smem<TR, TC>(n, LD, s.U(), x.W1(), s.U());
+        gemm_smem_real<TR, TC, false>(n, LD, s.G(), P, s.G());
+        gemm_smem_real<TR, TC, true>(n, LD, s.G(), s.G(), M);
+        gemm_smem_real<TR, TC, false>(n, LD, s.U(), P, s.U());
     }
 }
 
@@ -1251,7 +1261,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
     sstore(n, LD, x.A().URs(0), s.U());
     gcopy(x.A().VRs(0), x.A().VRc, n * n);
     gcopy(x.A().DRs(0), x.A().DRc, n);
-    sload(n, LD, x.W1(), x.P().expP);
+    sload_real(n, LD, reinterpret_cast<double*>(x.W1()), x.P().expP);
     __syncthreads();
     const int ns = x.P().Ns;
     for (int nt = 1; nt <= L; ++nt) {
@@ -1270,7 +1280,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
             }
             __syncthreads();
         }
-        gemm_rs<TR, TC>(n, LD, s.U(), op_n(x.W1(), LD), op_n(s.U(), LD));
+        gemm_smem_real<TR, TC, false>(n, LD, s.U(), reinterpret_cast<const double*>(x.W1()), s.U());
         if (nt % x.P().Nwrap == 0) {
             const int st = nt / x.P().Nwrap;
             stab_UR(x);
@@ -1283,7 +1293,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
                 scopy(n, LD, s.G(), x.W2());
                 __syncthreads();
             }
-            sload(n, LD, x.W1(), x.P().expP);
+            sload_real(n, LD, reinterpret_cast<double*>(x.W1()), x.P().expP);
             __syncthreads();
         }
     }

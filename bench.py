@@ -60,10 +60,11 @@ def ess_rate(chain_sweeps_per_s: float):
 
 def flops_per_chain_sweep(n: int, L: int, nwrap: int, naccept: float) -> float:
     """Algorithmic FP64 flops of one sweep of one chain: 2L slice steps of three
-    complex N^3 products (8 N^3 each), 8 N^2 per accepted rank-1 update, and
-    2L/Nwrap stabilisations at (15 + 45) N^3 (pivoted QR + ZUNGQR + ZTRMM, and
-    stab_green), by LAPACK's complex flop counts."""
-    return 2 * L * 24.0 * n ** 3 + 8.0 * n ** 2 * naccept + (2.0 * L / nwrap) * 60.0 * n ** 3
+    N^3 products of a complex matrix with the real e^{-+dtau K} (4 N^3 each; the
+    reference's ZGEMMs count 8 N^3 because they carry the zero imaginary part),
+    8 N^2 per accepted rank-1 update, and 2L/Nwrap stabilisations at (15 + 45) N^3
+    (pivoted QR + ZUNGQR + ZTRMM, and stab_green), by LAPACK's complex flop counts."""
+    return 2 * L * 12.0 * n ** 3 + 8.0 * n ** 2 * naccept + (2.0 * L / nwrap) * 60.0 * n ** 3
 
 
 class ClockSampler:
