@@ -75,7 +75,8 @@ struct Smem {
     static constexpr size_t oIpiv = oPiv + sizeof(int) * NMAX, oAccf = oIpiv + sizeof(int) * NMAX;
     static constexpr size_t oIbc = oAccf + sizeof(int) * NMAX, oSeed = oIbc + 4 * sizeof(int);
     static constexpr size_t oSxy = oSeed + 16;   // site coordinates x | y << 16
-    static constexpr size_t bytes() { return oSxy + ((sizeof(int) * NMAX + 15) / 16) * 16; }
+    static constexpr size_t oCnt = oSxy + ((sizeof(int) * NMAX + 15) / 16) * 16;   // nacc[2], nc[2], nobs of the sweep
+    static constexpr size_t bytes() { return oCnt + 48; }
 
     template <class T>
     static DEVI T* at(size_t off) { return reinterpret_cast<T*>(bq_smem + off); }
@@ -110,6 +111,7 @@ struct Smem {
     DEVI int* ibc() const { return at<int>(oIbc); }
     DEVI uint32_t* seed() const { return at<uint32_t>(oSeed); }
     DEVI int* sxy() const { return at<int>(oSxy); }
+    DEVI long long* cnt() const { return at<long long>(oCnt); }
     DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
 
@@ -293,6 +295,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // The rank-1 term is ZGERU's x(i) alpha y(j): grouped x(i) (alpha y(j)) on
     // the block rows and (x(i) alpha) y(j) on the block columns.
     constexpr int NB = Cfg<NMAX>::NB;
+    long long nacc = 0;   // accepted proposals, counted by thread 0
     for (int k0 = 0; k0 < n; k0 += KB) {
         const int kb = min(KB, n - k0);
         const int slo = LEFT ? n - k0 - kb : k0;   // block sites are slo .. slo+kb-1
@@ -382,6 +385,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
                     if (t == 0) {
                         s.accf()[i] = accept ? 1 : 0;
                         s.coef()[m] = coef;
+                        nacc += accept ? 1 : 0;
                     }
                 }
             }
@@ -435,11 +439,9 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
-    if (tid == 0) {
-        long long na = 0;
-        for (int i = 0; i < n; ++i) na += s.accf()[i];
-        x.sc->nacc[ch] += na;
-        x.sc->nc[ch] += n;
+    if (tid == 0) {   // AccCounter%count, kept in shared memory for the sweep
+        s.cnt()[ch] += nacc;
+        s.cnt()[2 + ch] += n;
         *s.seed() = lcg_mul(c_apow[2 * n], s0);
     }
     {
@@ -527,6 +529,7 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
 
     cplx g[MAXE];
     int er[MAXE], ec[MAXE];
+    long long nacc = 0;   // accepted proposals, counted by thread 0
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
         const int e = tid + k * blockDim.x;
@@ -570,7 +573,10 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
         const cplx det = csub(cmul(p00, p11), cmul(p01, p10));
         const double det2 = det.x * det.x + det.y * det.y;
         const bool accept = s.rg()[i] / sqrt(det2) > s.u2()[i];
-        if (tid == 0) s.accf()[i] = accept ? 1 : 0;
+        if (tid == 0) {
+            s.accf()[i] = accept ? 1 : 0;
+            nacc += accept ? 1 : 0;
+        }
         if (accept) {
             // M = P1^{-1} D1, P1^{-1} = adj(P1) conj(det) / |det|^2
             const cplx id = cmk(det.x / det2, -det.y / det2);
@@ -609,10 +615,8 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
     for (int i = tid; i < ns; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
     if (tid == 0) {
-        long long na = 0;
-        for (int i = 0; i < ns; ++i) na += s.accf()[i];
-        x.sc->nacc[ch] += na;
-        x.sc->nc[ch] += ns;
+        s.cnt()[ch] += nacc;
+        s.cnt()[2 + ch] += ns;
         *s.seed() = lcg_mul(c_apow[2 * ns], s0);
     }
     // U_L columns (left) or U_R rows (right) of both indices of every site, final fields
@@ -762,7 +766,7 @@ COLD void measure(Ctx<NMAX> x) {
         o[O_DEN_DODO + 1] -= v[7] / lq;
         o[O_DEN_UPDO] += v[8] / lq;
         o[O_DEN_UPDO + 1] += v[9] / lq;
-        x.sc->nobs += 1;
+        s.cnt()[4] += 1;
     }
     __syncthreads();
 }
@@ -896,7 +900,7 @@ COLD void measure_pair(Ctx<NMAX> x) {
         o[O_DEN_DODO + 1] -= v[1] / lq;
         o[O_DEN_UPDO] += v[2] / lq;
         o[O_DEN_UPDO + 1] += v[3] / lq;
-        x.sc->nobs += 1;
+        s.cnt()[4] += 1;
     }
     __syncthreads();
 }
@@ -1185,7 +1189,10 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
             tk = t_;                                 \
         }                                            \
     } while (0)
-    if (threadIdx.x == 0) *s.seed() = x.sc->seed;
+    if (threadIdx.x == 0) {
+        *s.seed() = x.sc->seed;
+        for (int k = 0; k < 5; ++k) s.cnt()[k] = 0;
+    }
     load_obs(x);
     sload(n, Cfg<NMAX>::LD, s.G(), x.A().G);
     sload(n, Cfg<NMAX>::LD, s.U(), x.A().ULc);
@@ -1230,7 +1237,14 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
     sstore(n, Cfg<NMAX>::LD, x.A().URc, s.U());
     sstore(n, Cfg<NMAX>::LD, x.A().G, s.G());
     flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
-    if (threadIdx.x == 0) x.sc->seed = *s.seed();
+    if (threadIdx.x == 0) {
+        x.sc->seed = *s.seed();
+        x.sc->nacc[0] += s.cnt()[0];
+        x.sc->nacc[1] += s.cnt()[1];
+        x.sc->nc[0] += s.cnt()[2];
+        x.sc->nc[1] += s.cnt()[3];
+        x.sc->nobs += s.cnt()[4];
+    }
     lap(3);
 #undef lap
 }
