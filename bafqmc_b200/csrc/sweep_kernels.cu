@@ -112,6 +112,7 @@ struct Smem {
     DEVI uint32_t* seed() const { return at<uint32_t>(oSeed); }
     DEVI int* sxy() const { return at<int>(oSxy); }
     DEVI long long* cnt() const { return at<long long>(oCnt); }
+    DEVI int* strip_warp() const { return at<int>(oCnt + 40); }
     DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
 
@@ -134,6 +135,7 @@ struct Ctx {
     ChainScalars* sc;
     cplx* wg;   // HBM workspaces of an N > 36 chain (two NMAX x LD matrices)
     int n;
+    int sw0;    // first warp of the site strip
     DEVI const PointDev& P() const { return *s.P(); }
     DEVI Arena A() const { return make_arena(abase, n); }
     DEVI cplx* W1() const {
@@ -299,8 +301,8 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     for (int k0 = 0; k0 < n; k0 += KB) {
         const int kb = min(KB, n - k0);
         const int slo = LEFT ? n - k0 - kb : k0;   // block sites are slo .. slo+kb-1
-        if (tid < NB) {
-            const int t = tid;
+        const int t = tid - 32 * x.sw0;
+        if ((unsigned)t < (unsigned)NB) {
             const bool tv = t < n;
             const bool tin = (unsigned)(t - slo) < (unsigned)kb;
             // site of slot q
@@ -439,7 +441,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
-    if (tid == 0) {   // AccCounter%count, kept in shared memory for the sweep
+    if (tid == 32 * x.sw0) {   // the strip's first thread: AccCounter%count, kept in shared memory
         s.cnt()[ch] += nacc;
         s.cnt()[2 + ch] += n;
         *s.seed() = lcg_mul(c_apow[2 * n], s0);
@@ -1134,7 +1136,16 @@ COLD void wrap_R(Ctx<NMAX> x, int nt) {
 template <int NMAX>
 DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     const ChainDev cd = ka.chains[chain];
-    if (threadIdx.x == 0) *x.s.P() = ka.pts[cd.point];
+    if (threadIdx.x == 0) {
+        *x.s.P() = ka.pts[cd.point];
+        // The SM's schedulers take warps by slot modulo 4, so the site strips of
+        // two CTAs on one SM would share two schedulers if both used warps 0-1.
+        // A CTA whose warp slots start at an odd multiple of 8 runs its strip on
+        // warps 2-3.  Thread 0 decides for the whole CTA.
+        unsigned slot;
+        asm volatile("mov.u32 %0, %%warpid;" : "=r"(slot));
+        *x.s.strip_warp() = (Cfg<NMAX>::THREADS >= 192 && ((slot >> 3) & 1)) ? 2 : 0;
+    }
     __syncthreads();
     x.n = x.P().N;
     if (x.P().hasK)
@@ -1145,6 +1156,7 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     }
     x.abase = ka.arena + cd.arena_off;
     x.wg = x.abase + arena_base(x.n, x.P().Nst);
+    x.sw0 = *x.s.strip_warp();
     x.phi = ka.phi + cd.phi_off;
     x.sc = ka.sc + chain;
     return x.n <= NMAX;
