@@ -15,6 +15,7 @@ ERRORS = {-1: "BAFQMC_EARG", -2: "BAFQMC_ECUDA", -3: "BAFQMC_EUNSUPPORTED", -4: 
           -5: "BAFQMC_ENUMERIC"}
 OBS_SCALARS = 32
 COUNTERS = 14
+POLE_SCALARS = 5
 
 
 class BafqmcError(RuntimeError):
@@ -56,6 +57,7 @@ SIGNATURES = {
     "bafqmc_bin_point_obs": (C.c_int, [_P, _DP]),
     "bafqmc_get_green": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_log_weight": (C.c_int, [_P, _DP]),
+    "bafqmc_pole_diagnostics": (C.c_int, [_P, _DP, C.c_int, _DP]),
     "bafqmc_counters": (C.c_int, [_P, _DP]),
     "bafqmc_phase_timers": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_synchronize": (C.c_int, [_P]),

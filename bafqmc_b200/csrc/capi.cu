@@ -188,6 +188,8 @@ struct bafqmc_handle {
     int* d_plist = nullptr;
     double* d_pout = nullptr;
     double* d_tmp = nullptr;
+    double* d_pole = nullptr;   // pole diagnostics: [nchains][kPoleScalars] then [nchains][pole_n][2]
+    int pole_n = 0;
     PointDev* d_pts = nullptr;
     ChainDev* d_chains = nullptr;
     double2* d_mats = nullptr;
@@ -319,7 +321,7 @@ void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
-                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp};
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
@@ -625,6 +627,56 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out) {
     CK(cudaStreamSynchronize(h->stream));
     for (int c = 0; c < h->nchains; ++c)
         out[c] = h->pts[h->chain_point[c]].pairing ? std::nan("") : fn[c] - 2.0 * sc[c].logdetM;
+    return BAFQMC_OK;
+}
+
+int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars) {
+    if (!h || !scalars) return fail(BAFQMC_EARG, "null argument");
+    if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
+    int nmax = 0;
+    for (int c = 0; c < h->nchains; ++c) {
+        const PointHost& p = h->pts[h->chain_point[c]];
+        if (!p.pairing) nmax = std::max(nmax, p.N);
+    }
+    if (z && zstride < nmax) return fail(BAFQMC_EARG, "zstride is below the largest Ndim of a number-conserving chain");
+    const double nan = std::nan("");
+    for (size_t k = 0; k < (size_t)h->nchains * BAFQMC_POLE_SCALARS; ++k) scalars[k] = nan;
+    if (z)
+        for (size_t k = 0; k < (size_t)h->nchains * zstride * 2; ++k) z[k] = nan;
+    if (nmax == 0) return BAFQMC_OK;
+    CK(cudaSetDevice(h->device));
+    const size_t per = bq::kPoleScalars + 2 * (size_t)nmax;
+    if (!h->d_pole) {
+        CK(cudaMalloc(&h->d_pole, sizeof(double) * per * h->nchains));
+        h->pole_n = nmax;
+    }
+    double* d_s = h->d_pole;
+    double* d_z = h->d_pole + (size_t)bq::kPoleScalars * h->nchains;
+    CK(bq::launch_pole(h->args(), nmax, h->pole_n, d_z, d_s, h->stream));
+    CK(bq::launch_field_norm(h->args(), h->d_tmp, h->stream));
+    std::vector<double> hs((size_t)bq::kPoleScalars * h->nchains), hz(2 * (size_t)h->pole_n * h->nchains),
+        fn(h->nchains);
+    std::vector<ChainScalars> sc(h->nchains);
+    CK(cudaMemcpyAsync(hs.data(), d_s, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, h->stream));
+    if (z) CK(cudaMemcpyAsync(hz.data(), d_z, sizeof(double) * hz.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(fn.data(), h->d_tmp, sizeof(double) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(sc.data(), h->d_sc, sizeof(ChainScalars) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int bad = -1;
+    for (int c = 0; c < h->nchains; ++c) {
+        const PointHost& p = h->pts[h->chain_point[c]];
+        if (p.pairing) continue;
+        const double* s = hs.data() + (size_t)c * bq::kPoleScalars;
+        double* o = scalars + (size_t)c * BAFQMC_POLE_SCALARS;
+        for (int k = 0; k < 4; ++k) o[k] = s[k];
+        o[4] = fn[c] - 2.0 * sc[c].logdetM;
+        if (s[4] != 0.0 && bad < 0) bad = c;
+        if (z)
+            for (int i = 0; i < 2 * p.N; ++i) z[(size_t)c * zstride * 2 + i] = hz[(size_t)c * h->pole_n * 2 + i];
+    }
+    if (bad >= 0)
+        return fail(BAFQMC_ENUMERIC, "eigenvalue iteration of the pole diagnostics did not converge for chain " +
+                                         std::to_string(bad));
     return BAFQMC_OK;
 }
 

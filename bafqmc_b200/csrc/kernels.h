@@ -40,4 +40,12 @@ cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* star
                                  cudaStream_t st);
 cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st);
 
+// pole diagnostics of the number-conserving chains' G: per chain kPoleScalars
+// doubles (pole_distance, pole_x, spectral radius, largest singular value,
+// status) at sout, the poles 1/lambda at zout (zstride complex per chain);
+// nmax bounds N over those chains
+constexpr int kPoleScalars = 5;
+size_t pole_smem_bytes(int n);
+cudaError_t launch_pole(const KernelArgs& ka, int nmax, int zstride, double* zout, double* sout, cudaStream_t st);
+
 }  // namespace bq

@@ -165,6 +165,28 @@ class Ensemble:
         _lib.check(self.lib.bafqmc_log_weight(self.h, _dptr(out)))
         return out
 
+    POLE_NAMES = ("pole_distance", "pole_x", "green_spectral_radius", "green_smax", "log_weight")
+
+    def pole_diagnostics(self) -> list[dict | None]:
+        """PoleDiagnostics (pole_diagnostics.f90:91-123) of every chain's current G,
+        computed on the device: the poles z = 1/lambda (the chain's pole_z row)
+        and the five scalar files.  None for a Nambu chain."""
+        zs = max([self.dims[self.chain_point[c]][0] for c in range(self.nchains)] + [1])
+        z = np.zeros((self.nchains, zs, 2))
+        sc = np.zeros((self.nchains, _lib.POLE_SCALARS))
+        _lib.check(self.lib.bafqmc_pole_diagnostics(self.h, _dptr(z), zs, _dptr(sc)))
+        out = []
+        for c in range(self.nchains):
+            p = self.chain_point[c]
+            if self.points[p].sector == 1:
+                out.append(None)
+                continue
+            nd = self.dims[p][0]
+            d = {k: float(sc[c, i]) for i, k in enumerate(self.POLE_NAMES)}
+            d["pole_z"] = z[c, :nd, 0] + 1j * z[c, :nd, 1]
+            out.append(d)
+        return out
+
     def phase_timers(self, enable: bool = True) -> np.ndarray:
         """Enable per-phase cycle counting; returns the [nchains, 4] cycles so far."""
         out = np.zeros((self.nchains, 4))
@@ -191,21 +213,6 @@ def nambu_green(block: np.ndarray) -> np.ndarray:
     g[np.ix_(one, one)] = block
     g[np.ix_(two, two)] = np.conj(block)
     return g
-
-
-# ---------------------------------------------------------------------------
-# per-bin diagnostics of G (pole_diagnostics.f90:91-123).  log_weight comes from
-# the device (stabilised factorisation of I - B); the eigen/singular values are
-# taken on the host from the device-computed G.
-def pole_diagnostics(G: np.ndarray, log_weight: float) -> dict:
-    small = np.finfo(float).tiny
-    ev = np.linalg.eigvals(G)
-    sv = np.linalg.svd(G, compute_uv=False)
-    z = np.where(np.abs(ev) <= small, complex(1.0 / small, 0.0), 1.0 / np.where(ev == 0, 1, ev))
-    pd = max(float(np.min(np.abs(z))), small)
-    return {"pole_z": z, "pole_distance": pd, "pole_x": -math.log10(pd),
-            "green_spectral_radius": float(np.max(np.abs(ev))), "green_smax": float(np.max(sv)),
-            "log_weight": float(log_weight)}
 
 
 # ---------------------------------------------------------------------------
@@ -333,8 +340,7 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
         ens.sweep(p.Nsweep)
         append_bin(run_dir, ens.point_obs()[0], pairing=pairing)
         if pole and not pairing:
-            lw = ens.log_weight()
-            append_pole(run_dir, [pole_diagnostics(ens.green(c), lw[c]) for c in range(nchains)])
+            append_pole(run_dir, ens.pole_diagnostics())
     cnt = ens.counters()
     for ch, name in ((0, "U1"), (1, "U2")):
         if abs((p.U1, p.U2)[ch]) > 1e-10:

@@ -117,6 +117,23 @@ int bafqmc_get_green(bafqmc_handle* h, int chain, double* G);
  * NaN for Nambu chains. */
 int bafqmc_log_weight(bafqmc_handle* h, double* out);
 
+/* PoleDiagnostics (pole_diagnostics.f90:91-123) of each number-conserving
+ * chain's current G, computed on the device.
+ *   z        optional, [nchains][zstride][2] doubles: the Ndim poles
+ *            z = 1/lambda over the eigenvalues lambda of G (1/tiny where
+ *            |lambda| <= tiny), the chain's row of the pole_z file; zstride >=
+ *            Ndim of every number-conserving chain.  Eigenvalues come in the
+ *            order of the diagonal of this library's Schur form, which need
+ *            not be ZGEEV's order.
+ *   scalars  [nchains][BAFQMC_POLE_SCALARS]: pole_distance, pole_x,
+ *            green_spectral_radius, green_smax, log_weight (the five
+ *            one-column files).
+ * Nambu chains (the pairing program writes no pole files) get NaN.  Returns
+ * BAFQMC_ENUMERIC if a chain's eigenvalue iteration did not converge (the
+ * reference stops on ZGEEV info != 0, pole_diagnostics.f90:41-46). */
+#define BAFQMC_POLE_SCALARS 5
+int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars);
+
 /* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
  * status, seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
  * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and

@@ -50,6 +50,20 @@ def compare_bin(gpu: dict, ora: dict, label=""):
                                    err_msg=f"{label} {k}")
 
 
+def compare_pole(gpu: dict, ora: dict, label=""):
+    """Device pole diagnostics against the oracle's (ZGEEV/ZGESVD through NumPy).
+    The poles are matched as sets: eigenvalue order is solver-specific."""
+    for k in ("log_weight", "pole_distance", "pole_x", "green_spectral_radius", "green_smax"):
+        np.testing.assert_allclose(gpu[k], ora[k], rtol=RTOL, atol=ATOL, err_msg=f"{label} {k}")
+    zg, zo = list(gpu["pole_z"]), list(ora["pole_z"])
+    assert len(zg) == len(zo)
+    scale = max(abs(z) for z in zo)
+    for z in zg:
+        j = int(np.argmin([abs(z - w) for w in zo]))
+        assert abs(z - zo[j]) <= RTOL * scale, f"{label} pole {z} vs {zo[j]}"
+        zo.pop(j)
+
+
 def assert_green_close(Gg, Go, label=""):
     err = np.max(np.abs(Gg - Go)) / np.max(np.abs(Go))
     assert err < RTOL, f"{label} G rel err {err:.3e}"
@@ -74,7 +88,7 @@ def test_fixed_field_matches_reference_dense(solver_mod, root, nwrap):
                       "onsite_n2_do", "interaction_energy_density", "energy_density"):
                 np.testing.assert_allclose(np.atleast_1d(b[k]), np.atleast_1d(exp[k]), rtol=tol, atol=tol,
                                            err_msg=k)
-            d = solver_mod.pole_diagnostics(ens.green(0), ens.log_weight()[0])
+            d = ens.pole_diagnostics()[0]
             for k in ("log_weight", "pole_distance", "pole_x", "green_spectral_radius", "green_smax"):
                 np.testing.assert_allclose(d[k], exp[k], rtol=tol, atol=tol, err_msg=k)
         seeds, phis = ens.get_state()
@@ -130,6 +144,7 @@ def _run_both(op, sp, seeds, nbins, nwarm=0):
         cobs = ens.chain_obs()
         cnt = ens.counters()
         lw = ens.log_weight()
+        pole = ens.pole_diagnostics()
         for c, ch in enumerate(chains):
             assert int(seeds_g[c]) == ch.seed, f"bin {b} chain {c} seed"
             np.testing.assert_array_equal(phis_g[c], ch.phi, err_msg=f"bin {b} chain {c} fields")
@@ -137,6 +152,7 @@ def _run_both(op, sp, seeds, nbins, nwarm=0):
             compare_bin(cobs[c], ch.obs.as_dict(latt), f"bin {b} chain {c}")
             np.testing.assert_allclose(cnt[c, 0:2], ch.acc_sum, rtol=0, atol=0)
             np.testing.assert_allclose(lw[c], ch.pole_diagnostics()["log_weight"], rtol=RTOL)
+            compare_pole(pole[c], ch.pole_diagnostics(), f"bin {b} chain {c}")
         avg = O.chain_average(chains)
         compare_bin(ens.point_obs()[0], avg, f"bin {b} average")
     ens.close()
@@ -195,3 +211,45 @@ def test_n72_class_against_oracle(solver_mod, lx, ly):
     the two workspaces in HBM, one CTA per SM; 6x7 has no K point."""
     op, sp = both_params(U2=-0.5, Nlx=lx, Nly=ly, Ltrot=20, Beta=1.0, Nwrap=5)
     _run_both(op, sp, [31, 32], nbins=1)
+
+
+def test_pole_diagnostics_near_the_band_edge(solver_mod):
+    """4x4 (lowest free level at -2) at mu = -2.05, beta = 8 and weak coupling:
+    G is far from the identity (largest singular values about 3.2 and 1.6,
+    condition numbers 4.8 and 2.5), so the device eigenvalue and
+    singular-value routines are checked on a non-trivial spectrum against
+    ZGEEV/ZGESVD of the oracle's G."""
+    op, sp = both_params(U1=0.2, U2=-0.05, mu=-2.05, Nlx=4, Nly=4, Ltrot=80, Beta=8.0, Nwrap=10)
+    chains = _run_both(op, sp, [5, 6], nbins=1)
+    assert max(ch.pole_diagnostics()["green_smax"] for ch in chains) > 2.0
+
+
+def test_run_directory_number_conserving_program(solver_mod, tmp_path):
+    """The run-directory contract of src/number_conserving: every per-bin file,
+    including the pole files (one row per chain per bin), against the oracle."""
+    op, sp = both_params(U2=-0.5, Nlx=4, Nly=4, Ltrot=40, Beta=4.0, Nbin=2)
+    (tmp_path / "paramC_sets.txt").write_text(sp.to_text())
+    (tmp_path / "confin.txt").write_text("0\n")
+    (tmp_path / "seeds.txt").write_text("4099\n777\n")
+    solver_mod.run_directory(tmp_path, nchains=2)
+    bins, chains = O.run(op, seeds=[4099, 777])
+    from bafqmc_b200.observables import FILE_ORDER
+    for name in FILE_ORDER:
+        rows = [ln.split() for ln in (tmp_path / name).read_text().splitlines() if ln.strip()]
+        assert len(rows) == sp.Nbin, name
+        for b, row in enumerate(rows):
+            got = np.array([float(t) for t in row])
+            want = bins[b][name]
+            if isinstance(want, complex):
+                want = np.array([want.real, want.imag])
+            np.testing.assert_allclose(got, np.atleast_1d(want), rtol=1e-9, atol=1e-12, err_msg=f"{name} bin {b}")
+    for k in ("pole_distance", "pole_x", "green_spectral_radius", "green_smax", "log_weight"):
+        vals = [float(t) for t in (tmp_path / k).read_text().split()]
+        want = [bins[b]["pole"][c][k] for b in range(sp.Nbin) for c in range(2)]
+        np.testing.assert_allclose(vals, want, rtol=1e-9, err_msg=k)
+    rows = [ln.split() for ln in (tmp_path / "pole_z").read_text().splitlines() if ln.strip()]
+    assert len(rows) == 2 * sp.Nbin
+    for r, row in enumerate(rows):
+        v = np.array([float(t) for t in row])
+        got = v[0::2] + 1j * v[1::2]
+        compare_pole({**bins[r // 2]["pole"][r % 2], "pole_z": got}, bins[r // 2]["pole"][r % 2], f"pole_z row {r}")
