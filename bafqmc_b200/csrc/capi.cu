@@ -199,6 +199,10 @@ struct bafqmc_handle {
     ChainScalars* d_sc = nullptr;
     bool have_fields = false, pre_done = false, bin_done = false;
     int timers = 0;
+    // the launches of one bin (reset, nsweep sweeps of every class, finish),
+    // captured once per (nsweep, timers) and replayed as one graph launch
+    cudaGraphExec_t bin_graph = nullptr;
+    int graph_nsweep = 0, graph_timers = 0;
 
     bq::KernelArgs args() const {
         bq::KernelArgs ka;
@@ -326,6 +330,7 @@ void free_handle(bafqmc_handle* h) {
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
         if (h->d_cls[c]) cudaFree(h->d_cls[c]);
+    if (h->bin_graph) cudaGraphExecDestroy(h->bin_graph);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -571,16 +576,47 @@ int bafqmc_pre(bafqmc_handle* h) {
     return BAFQMC_OK;
 }
 
+namespace {
+// The launches of one bin: accumulator reset, nsweep persistent sweep launches
+// per kernel class, bin averages.
+cudaError_t record_bin(bafqmc_handle* h, int nsweep) {
+    const bq::KernelArgs ka = h->args();
+    cudaError_t e = bq::launch_bin_reset(ka, h->stream);
+    for (int s = 0; s < nsweep && e == cudaSuccess; ++s)
+        for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+            e = bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
+    if (e == cudaSuccess) e = bq::launch_bin_finish(ka, h->stream);
+    return e;
+}
+}  // namespace
+
 int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
     if (!h || nsweep < 1) return fail(BAFQMC_EARG, "bad sweep arguments");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     CK(cudaSetDevice(h->device));
-    const bq::KernelArgs ka = h->args();
-    CK(bq::launch_bin_reset(ka, h->stream));
-    for (int s = 0; s < nsweep; ++s)
-        for (int c = 0; c < bq::kNumClasses; ++c)
-            CK(bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
-    CK(bq::launch_bin_finish(ka, h->stream));
+    if (!h->bin_graph || h->graph_nsweep != nsweep || h->graph_timers != h->timers) {
+        if (h->bin_graph) {
+            CK(cudaGraphExecDestroy(h->bin_graph));
+            h->bin_graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+        const cudaError_t e = record_bin(h, nsweep);
+        const cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e != cudaSuccess ? e : e2, "capture of the bin launches");
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&h->bin_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            h->bin_graph = nullptr;
+            return cuda_fail(e3, "cudaGraphInstantiate");
+        }
+        h->graph_nsweep = nsweep;
+        h->graph_timers = h->timers;
+    }
+    CK(cudaGraphLaunch(h->bin_graph, h->stream));
     h->bin_done = true;
     return BAFQMC_OK;
 }

@@ -92,7 +92,11 @@ int bafqmc_warmup_prior(bafqmc_handle* h, int nwarm);
 int bafqmc_pre(bafqmc_handle* h);
 
 /* One measurement bin: Local_sweep%sweep (local_sweep.f90:136-161) with
- * nsweep left+right sweeps, then Obs_equal_ave and the acceptance ratio. */
+ * nsweep left+right sweeps, then Obs_equal_ave and the acceptance ratio.
+ * The bin's launches (accumulator reset, one persistent sweep launch per
+ * kernel class and sweep, bin averages) are captured into a CUDA graph on the
+ * first call and replayed by later calls with the same nsweep and timer
+ * setting. */
 int bafqmc_sweep(bafqmc_handle* h, int nsweep);
 
 /* Observables of the last bin.  chain_obs: [nchains][stride] (per chain, the

@@ -253,3 +253,31 @@ def test_run_directory_number_conserving_program(solver_mod, tmp_path):
         v = np.array([float(t) for t in row])
         got = v[0::2] + 1j * v[1::2]
         compare_pole({**bins[r // 2]["pole"][r % 2], "pole_z": got}, bins[r // 2]["pole"][r % 2], f"pole_z row {r}")
+
+
+def test_bin_graph_replay_and_recapture(solver_mod):
+    """A bin is one CUDA graph launch (reset, Nsweep sweeps per kernel class,
+    finish), captured on the first bin, replayed on the second and captured
+    again when the phase timers change the kernel arguments on the third; every
+    bin matches the oracle's Nsweep = 2 bins."""
+    op, sp = both_params(U2=-0.5, Nsweep=2)
+    latt, opT, chains = O.init_chains(op, seeds=[77, 78])
+    with solver_mod.Ensemble([sp], [0, 0]) as ens:
+        ens.fields_from_seeds([77, 78])
+        ens.pre()
+        for ch in chains:
+            ch.pre()
+        for b in range(3):
+            if b == 2:
+                ens.phase_timers(True)
+            for ch in chains:
+                ch.sweep_bin()
+            ens.sweep(2)
+            seeds, phis = ens.get_state()
+            cobs = ens.chain_obs()
+            for c, ch in enumerate(chains):
+                assert int(seeds[c]) == ch.seed, f"bin {b} chain {c} seed"
+                np.testing.assert_array_equal(phis[c], ch.phi, err_msg=f"bin {b} chain {c} fields")
+                assert_green_close(ens.green(c), ch.prop.Gr, f"bin {b} chain {c}")
+                compare_bin(cobs[c], ch.obs.as_dict(latt), f"bin {b} chain {c}")
+        assert ens.phase_timers(False).sum() > 0
