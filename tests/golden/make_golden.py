@@ -16,6 +16,11 @@ the Fortran solver against:
 * ``benchmarks/paper/data/number_conserving/ed/*.json`` and
   ``benchmarks/paper/data/pairing/ed/triangle_pairing_delta_3x3_D0_mum5_b4.json``:
   stored ED chain averages for 3x3 points -> ``ed_3x3.json`` (observables only)
+* ``benchmarks/paper/data/index.json`` and ``benchmarks/paper/data/*/inputs/*/
+  paramC_sets.txt``: for each paper case (number-conserving and pairing 3x3
+  points), the run parameters and, per observable (density_total,
+  energy_density, S_SF_K, S_DW_K), the ED value and the reference solver's
+  own DQMC mean and standard error -> ``paper_3x3.json``
 """
 
 from __future__ import annotations
@@ -77,6 +82,20 @@ def main(ref_root: str) -> None:
     d = json.loads(p.read_text())
     ed[p.stem] = {k: d[k] for k in ("parameters", "observables") if k in d}
     (HERE / "ed_3x3.json").write_text(json.dumps(ed, indent=1) + "\n")
+
+    data = root / "benchmarks/paper/data"
+    index = json.loads((data / "index.json").read_text())
+    cases = {}
+    for c in index["cases"]:
+        lines = (data / c["model"] / "inputs" / c["id"] / "paramC_sets.txt").read_text().splitlines()
+        cases[c["id"]] = {
+            "model": c["model"],
+            "paramC_sets": [ln.split() for ln in lines[:7]],
+            "samples": c["samples"],
+            "observables": {k: {f: v[f] for f in ("ed", "dqmc", "stderr")} for k, v in c["observables"].items()},
+        }
+    (HERE / "paper_3x3.json").write_text(json.dumps({"source": "benchmarks/paper/data/index.json", "cases": cases},
+                                                    indent=1) + "\n")
 
 
 if __name__ == "__main__":
