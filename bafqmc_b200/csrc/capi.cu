@@ -189,6 +189,7 @@ struct bafqmc_handle {
     double* d_pout = nullptr;
     double* d_tmp = nullptr;
     double* d_pole = nullptr;   // pole diagnostics: [nchains][kPoleScalars] then [nchains][pole_n][2]
+    double2* d_pole_mat = nullptr;   // per-chain matrices of the pole kernel above its shared-memory size
     int pole_n = 0;
     PointDev* d_pts = nullptr;
     ChainDev* d_chains = nullptr;
@@ -239,7 +240,7 @@ int setup_point(const bafqmc_point& p, PointHost& out) {
     out.Nst = p.Ltrot / p.Nwrap;
     out.dtau = p.beta / (double)p.Ltrot;
     if (bq::class_of(out.N, out.pairing) < 0)
-        return fail(BAFQMC_EUNSUPPORTED, "Ndim above the largest shared-memory class of this build");
+        return fail(BAFQMC_EUNSUPPORTED, "Ndim above the largest size class of this build (144 number-conserving, 72 Nambu)");
     HostLattice lat(p.Lx, p.Ly);
     const int ns = out.Lq, n = out.N;
     zmat H(n);   // def_hamT (non_interact.f90:33-72), t = 1
@@ -325,7 +326,7 @@ void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
-                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole};
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
@@ -685,10 +686,12 @@ int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* sc
     if (!h->d_pole) {
         CK(cudaMalloc(&h->d_pole, sizeof(double) * per * h->nchains));
         h->pole_n = nmax;
+        const long long hm = bq::pole_hbm_elems(nmax);
+        if (hm > 0) CK(cudaMalloc(&h->d_pole_mat, sizeof(double2) * (size_t)hm * h->nchains));
     }
     double* d_s = h->d_pole;
     double* d_z = h->d_pole + (size_t)bq::kPoleScalars * h->nchains;
-    CK(bq::launch_pole(h->args(), nmax, h->pole_n, d_z, d_s, h->stream));
+    CK(bq::launch_pole(h->args(), nmax, h->pole_n, d_z, d_s, h->d_pole_mat, h->stream));
     CK(bq::launch_field_norm(h->args(), h->d_tmp, h->stream));
     std::vector<double> hs((size_t)bq::kPoleScalars * h->nchains), hz(2 * (size_t)h->pole_n * h->nchains),
         fn(h->nchains);

@@ -23,8 +23,8 @@ struct KernelArgs {
 };
 
 // kernel classes of the fused sweep: size (N <= 16, N <= 36, N <= 72) + 3 * sector
-// (0 number-conserving, 1 Nambu)
-constexpr int kNumClasses = 6;
+// (0 number-conserving, 1 Nambu), and class 6: number-conserving N <= 144
+constexpr int kNumClasses = 7;
 int class_nmax(int cls);
 size_t smem_bytes(int cls);
 int class_of(int n, int pairing);   // -1 if no class holds n
@@ -44,8 +44,12 @@ cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st
 // doubles (pole_distance, pole_x, spectral radius, largest singular value,
 // status) at sout, the poles 1/lambda at zout (zstride complex per chain);
 // nmax bounds N over those chains
+// above kPoleSmemMaxN the matrix lives in hmat: pole_hbm_elems(nmax) complex
+// values per chain
 constexpr int kPoleScalars = 5;
-size_t pole_smem_bytes(int n);
-cudaError_t launch_pole(const KernelArgs& ka, int nmax, int zstride, double* zout, double* sout, cudaStream_t st);
+constexpr int kPoleSmemMaxN = 112;
+long long pole_hbm_elems(int nmax);
+cudaError_t launch_pole(const KernelArgs& ka, int nmax, int zstride, double* zout, double* sout, double2* hmat,
+                        cudaStream_t st);
 
 }  // namespace bq

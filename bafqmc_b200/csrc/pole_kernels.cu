@@ -12,7 +12,8 @@
 // last stabilised factorisation and is assembled by the host call.
 //
 // One warp per chain (one CTA of 32 threads), with the matrix in shared memory
-// at an odd leading dimension.  The eigenvalues come from a diagonal balancing
+// at an odd leading dimension (in a per-chain HBM scratch above n = 112, whose
+// matrix does not fit in shared memory).  The eigenvalues come from a diagonal balancing
 // (Parlett and Reinsch, radix 2), a Householder reduction to Hessenberg form
 // and the complex single-shift QR iteration with Wilkinson shifts and
 // deflation on negligible subdiagonals (Golub and Van Loan, Matrix
@@ -275,16 +276,17 @@ DEVI int hqr_warp(int n, int ld, cplx* H, cplx* ev) {
 
 // out per chain: kPoleScalars doubles (pole_distance, pole_x, spectral radius,
 // smax, status) and zstride complex poles.
-__global__ void __launch_bounds__(32) pole_kernel(KernelArgs ka, int zstride, double* zout, double* sout) {
+__global__ void __launch_bounds__(32) pole_kernel(KernelArgs ka, int zstride, double* zout, double* sout, cplx* hmat,
+                                                   long long hstride) {
     const int chain = blockIdx.x;
     if (chain >= ka.nchains) return;
     const ChainDev cd = ka.chains[chain];
     const PointDev* P = ka.pts + cd.point;
     if (P->pairing) return;
     const int n = P->N, ld = n | 1, lane = threadIdx.x;
-    cplx* H = reinterpret_cast<cplx*>(pole_smem);
-    cplx* v = H + n * ld;
+    cplx* v = reinterpret_cast<cplx*>(pole_smem);
     cplx* ev = v + n;
+    cplx* H = hmat ? hmat + (long long)chain * hstride : ev + n;
     const cplx* G = reinterpret_cast<const cplx*>(ka.arena) + cd.arena_off;
 
     for (int e = lane; e < n * n; e += 32) {
@@ -344,14 +346,17 @@ __global__ void __launch_bounds__(32) pole_kernel(KernelArgs ka, int zstride, do
 
 }  // namespace
 
-size_t pole_smem_bytes(int n) { return sizeof(cplx) * ((size_t)n * (n | 1) + 2 * (size_t)n); }
+long long pole_hbm_elems(int nmax) { return nmax > kPoleSmemMaxN ? (long long)nmax * (nmax | 1) : 0; }
 
-cudaError_t launch_pole(const KernelArgs& ka, int nmax, int zstride, double* zout, double* sout, cudaStream_t st) {
+cudaError_t launch_pole(const KernelArgs& ka, int nmax, int zstride, double* zout, double* sout, double2* hmat,
+                        cudaStream_t st) {
     if (ka.nchains <= 0) return cudaSuccess;
-    const size_t sm = pole_smem_bytes(nmax);
+    const long long hs = pole_hbm_elems(nmax);
+    if (hs > 0 && !hmat) return cudaErrorInvalidValue;
+    const size_t sm = sizeof(cplx) * (2 * (size_t)nmax + (hs > 0 ? 0 : (size_t)nmax * (nmax | 1)));
     cudaError_t e = cudaFuncSetAttribute(pole_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    pole_kernel<<<ka.nchains, 32, sm, st>>>(ka, zstride, zout, sout);
+    pole_kernel<<<ka.nchains, 32, sm, st>>>(ka, zstride, zout, sout, hs > 0 ? hmat : nullptr, hs);
     return cudaGetLastError();
 }
 

@@ -10,6 +10,7 @@
 // shared-memory size class and per sector (PAIR: Nambu chains).
 #include "sweep.cuh"
 #include "kernels.h"
+#include "linalg_big.cuh"
 
 namespace bq {
 
@@ -25,7 +26,8 @@ template <int NMAX> struct Cfg;
 // only G and U in shared memory.
 template <> struct Cfg<16> {
     static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, NB = 64, MINB = 2;
-    static constexpr bool GW = false;
+    static constexpr bool GW = false, GG = false;
+    static constexpr int RW = 1, CPW = 1;
 };
 static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
 // N <= 36: two CTAs per SM, all four matrices in shared memory.  (Three CTAs
@@ -33,21 +35,37 @@ static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
 // slice products and wraps slow down more than the third chain adds.)
 template <> struct Cfg<36> {
     static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, NB = 64, MINB = 2;
-    static constexpr bool GW = false;
+    static constexpr bool GW = false, GG = false;
+    static constexpr int RW = 2, CPW = 1;
 };
 // N <= 72: G and U in shared memory, the workspaces in HBM (one CTA per SM)
 template <> struct Cfg<72> {
     static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = 73, NB = 96, MINB = 1;
-    static constexpr bool GW = true;
+    static constexpr bool GW = true, GG = false;
+    static constexpr int RW = 3, CPW = 1;
+};
+// N <= 144 (up to the 12x12 lattice, number-conserving): G, U, both
+// workspaces and a product scratch in HBM after the chain's arena (L2-resident
+// while the chain runs), one CTA of 512 threads per SM.  Neither shared memory
+// nor the register file holds these n x n matrices, so products loop over
+// TR x TC tiles out of place and the factorisations use linalg_big.cuh (one
+// warp per column, RW rows per lane, CPW columns at a time).
+template <> struct Cfg<144> {
+    static constexpr int THREADS = 512, TR = 2, TC = 3, MAXE = 41, KB = 4, R8 = 18, CPS = 3, LD = 145, NB = 160,
+                         MINB = 1;
+    static constexpr bool GW = true, GG = true;
+    static constexpr int RW = 5, CPW = 2;
 };
 template <int NMAX>
 constexpr bool cfg_ok() {
     using C = Cfg<NMAX>;
-    return NMAX % C::TR == 0 && NMAX % C::TC == 0 && (NMAX / C::TR) * (NMAX / C::TC) <= C::THREADS &&
+    return NMAX % C::TR == 0 && NMAX % C::TC == 0 && (C::GG || (NMAX / C::TR) * (NMAX / C::TC) <= C::THREADS) &&
+           (!C::GG || (C::RW * 32 >= NMAX && C::THREADS >= NMAX && C::GW)) &&
            C::MAXE * C::THREADS >= NMAX * NMAX && C::R8 * 8 >= NMAX && C::CPS * (C::THREADS / 8) >= NMAX &&
            C::NB >= NMAX && C::NB % 32 == 0 && C::NB <= C::THREADS && (C::LD & 1) == 1 && C::LD >= NMAX;
 }
-static_assert(cfg_ok<16>() && cfg_ok<36>() && cfg_ok<72>(), "class tiles and register layouts must cover NMAX");
+static_assert(cfg_ok<16>() && cfg_ok<36>() && cfg_ok<72>() && cfg_ok<144>(),
+              "class tiles and register layouts must cover NMAX");
 static_assert(36 % 2 == 0 && 36 % 3 == 0, "tile must divide NMAX");
 static_assert(Cfg<16>::R8 * 8 >= 16 && Cfg<16>::CPS * (Cfg<16>::THREADS / 8) >= 16, "register layout must cover NMAX");
 static_assert(Cfg<36>::R8 * 8 >= 36 && Cfg<36>::CPS * (Cfg<36>::THREADS / 8) >= 36, "register layout must cover NMAX");
@@ -61,9 +79,10 @@ struct Smem {
     static constexpr int kRed = 32 * (Cfg<NMAX>::THREADS / 32);
     static constexpr size_t MM = sizeof(cplx) * NMAX * Cfg<NMAX>::LD, VC = sizeof(cplx) * NMAX, VD = sizeof(double) * NMAX;
     static constexpr bool GW = Cfg<NMAX>::GW;   // workspaces in HBM
+    static constexpr bool GG = Cfg<NMAX>::GG;   // G and U in HBM as well
     static constexpr size_t oG = 0, oU = MM, oW1 = 2 * MM, oW2 = 3 * MM;
     static constexpr int KB = Cfg<NMAX>::KB;
-    static constexpr size_t oTau = (GW ? 2 : 4) * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
+    static constexpr size_t oTau = (GG ? 0 : (GW ? 2 : 4)) * MM, oCol = oTau + VC, oRow = oCol + KB * VC, oDelta = oRow + KB * VC;
     static constexpr size_t oDelta2 = oDelta + VC;
     static constexpr size_t oEao = oDelta2 + VC, oEan = oEao + VC, oEbo = oEan + VC, oEbn = oEbo + VC;
     static constexpr size_t oPh = oEbn + VC, oCoef = oPh + VC, oCbc = oCoef + KB * sizeof(cplx);
@@ -118,12 +137,14 @@ struct Smem {
 
 // green_from_M keeps n complex reciprocals in vn1 | vn2
 static_assert(Smem<16>::oVn1 % 16 == 0 && Smem<36>::oVn1 % 16 == 0 && Smem<72>::oVn1 % 16 == 0 &&
+                  Smem<144>::oVn1 % 16 == 0 &&
                   Smem<16>::oVn2 == Smem<16>::oVn1 + 8 * 16 && Smem<36>::oVn2 == Smem<36>::oVn1 + 8 * 36 &&
-                  Smem<72>::oVn2 == Smem<72>::oVn1 + 8 * 72,
+                  Smem<72>::oVn2 == Smem<72>::oVn1 + 8 * 72 && Smem<144>::oVn2 == Smem<144>::oVn1 + 8 * 144,
               "vn1 | vn2 must hold NMAX aligned complex values");
 template <int NMAX>
 constexpr bool smem_fits() { return Cfg<NMAX>::MINB * (Smem<NMAX>::bytes() + 1024) <= 228 * 1024; }
-static_assert(smem_fits<16>() && smem_fits<36>() && smem_fits<72>(), "shared memory per SM for MINB CTAs");
+static_assert(smem_fits<16>() && smem_fits<36>() && smem_fits<72>() && smem_fits<144>(),
+              "shared memory per SM for MINB CTAs");
 
 // Per-chain view: the chain's arena base and fields in registers, the point
 // parameters in shared memory.
@@ -133,7 +154,7 @@ struct Ctx {
     cplx* abase;
     double* phi;
     ChainScalars* sc;
-    cplx* wg;   // HBM workspaces of an N > 36 chain (two NMAX x LD matrices)
+    cplx* wg;   // HBM region after the arena: W1, W2 (N > 36), then G, U and a product scratch (N > 72)
     int n;
     int sw0;    // first warp of the site strip
     DEVI const PointDev& P() const { return *s.P(); }
@@ -146,7 +167,95 @@ struct Ctx {
         if constexpr (Smem<NMAX>::GW) return wg + NMAX * Cfg<NMAX>::LD;
         else return s.W2();
     }
+    DEVI cplx* G() const {
+        if constexpr (Smem<NMAX>::GG) return wg + 2 * NMAX * Cfg<NMAX>::LD;
+        else return s.G();
+    }
+    DEVI cplx* U() const {
+        if constexpr (Smem<NMAX>::GG) return wg + 3 * NMAX * Cfg<NMAX>::LD;
+        else return s.U();
+    }
+    DEVI cplx* S() const { return wg + 4 * NMAX * Cfg<NMAX>::LD; }   // product scratch (HBM-resident classes)
 };
+
+// ---------------------------------------------------------------------------
+// Linear algebra per size class: the register-resident 8-lane-segment
+// routines of linalg.cuh for the shared-memory classes, the warp-per-column
+// routines of linalg_big.cuh (out of place through x.S()) for the HBM class.
+template <int NMAX>
+DEVI void gemm_any(Ctx<NMAX>& x, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) {
+        gemm_big<C_::TR, C_::TC>(x.n, C_::LD, x.S(), A, B, tri);
+        copy_mat(x.n, C_::LD, C, x.S());
+    } else {
+        gemm_rs<C_::TR, C_::TC>(x.n, C_::LD, C, A, B, tri);
+    }
+}
+template <int NMAX, bool RIGHT_REAL>
+DEVI void gemm_real_any(Ctx<NMAX>& x, cplx* C, const void* A, const void* B) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) {
+        gemm_big_real<C_::TR, C_::TC, RIGHT_REAL>(x.n, C_::LD, x.S(), A, B);
+        copy_mat(x.n, C_::LD, C, x.S());
+    } else {
+        gemm_smem_real<C_::TR, C_::TC, RIGHT_REAL>(x.n, C_::LD, C, A, B);
+    }
+}
+template <int NMAX>
+DEVI void qrp_any(Ctx<NMAX>& x, cplx* A) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) qrp_big<C_::RW>(x.n, C_::LD, A, x.s.qr());
+    else qrp_inplace<C_::R8, C_::CPS>(x.n, C_::LD, A, x.s.qr());
+}
+template <int NMAX>
+DEVI void form_q_any(Ctx<NMAX>& x, const cplx* F, cplx* Q, bool conjT) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) form_q_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), Q, conjT);
+    else form_q<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), Q, conjT);
+}
+template <int NMAX>
+DEVI void apply_qh_left_any(Ctx<NMAX>& x, const cplx* F, cplx* C) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) apply_qh_left_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), C);
+    else apply_qh_left<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
+}
+template <int NMAX>
+DEVI void apply_q_right_any(Ctx<NMAX>& x, const cplx* F, cplx* C) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) apply_q_right_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), C);
+    else apply_q_right<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
+}
+template <int NMAX>
+DEVI void trsm_left_any(Ctx<NMAX>& x, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) trsm_left_upper_big<C_::RW, C_::CPW>(x.n, C_::LD, F, rinv, rs, C);
+    else trsm_left_upper<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, rs, C);
+}
+template <int NMAX>
+DEVI void trsm_right_any(Ctx<NMAX>& x, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) trsm_right_upperH_big<C_::RW, C_::CPW>(x.n, C_::LD, F, rinv, cs, C);
+    else trsm_right_upperH<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, cs, C);
+}
+template <int NMAX>
+DEVI void permute_rows_any(Ctx<NMAX>& x, cplx* C, bool forward) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) permute_rows_big(x.n, C_::LD, C, x.s.piv(), x.s.ipiv(), forward, x.S());
+    else permute_rows<C_::MAXE>(x.n, C_::LD, C, x.s.piv(), x.s.ipiv(), forward);
+}
+template <int NMAX>
+DEVI void permute_cols_any(Ctx<NMAX>& x, cplx* C, bool forward) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) permute_cols_big(x.n, C_::LD, C, x.s.piv(), x.s.ipiv(), forward, x.S());
+    else permute_cols<C_::MAXE>(x.n, C_::LD, C, x.s.piv(), x.s.ipiv(), forward);
+}
+template <int NMAX>
+DEVI void conj_transpose_any(Ctx<NMAX>& x, cplx* A) {
+    using C_ = Cfg<NMAX>;
+    if constexpr (C_::GG) conj_transpose_big(x.n, C_::LD, A, x.S());
+    else conj_transpose_inplace<C_::MAXE>(x.n, C_::LD, A);
+}
 
 // ---------------------------------------------------------------------------
 // small CTA helpers
@@ -247,6 +356,48 @@ DEVI bool metro_ratio(cplx d, double rg, double u, cplx gjj, cplx& coef) {
     return accept;
 }
 
+// The deferred rank-KB pass of prop_channel on one TR x TC tile at (r0, c0):
+// the block's rank-1 terms (coefficients, rows and columns staged in shared
+// memory) on the tile's elements outside the block's rows and columns.
+template <int NMAX>
+DEVI void rank_block_tile(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb, int r0, int c0) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
+    const auto& s = x.s;
+    cplx g[TR][TC];
+    bool own[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+            const int r = r0 + a, c = c0 + b;
+            own[a][b] = r < n && c < n && (unsigned)(r - slo) >= (unsigned)kb &&
+                        (unsigned)(c - slo) >= (unsigned)kb;
+            g[a][b] = G[min(r, n - 1) * LD + min(c, n - 1)];
+        }
+#pragma unroll
+    for (int m = 0; m < KB; ++m) {
+        if (m >= kb) break;
+        const cplx cf = s.coef()[m];
+        cplx cr[TR], y[TC];
+#pragma unroll
+        for (int a = 0; a < TR; ++a) cr[a] = cmul(cf, s.col(m)[min(r0 + a, n - 1)]);
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+            const cplx yv = s.row(m)[min(c0 + b, n - 1)];
+            y[b] = cmk(-yv.x, -yv.y);
+        }
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+            for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b)
+            if (own[a][b]) G[(r0 + a) * LD + c0 + b] = g[a][b];
+}
+
 template <int NMAX, bool LEFT>
 COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
@@ -256,7 +407,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     const double shift = fabs(x.P().shiftLoc);
     const uint32_t s0 = *s.seed();
     double* phis = x.phi + (long)slice * n * 2;
-    cplx* G = s.G();
+    cplx* G = x.G();
 
     // per-site proposals; draw order follows the visiting order of the sites
     for (int i = tid; i < n; i += blockDim.x) {
@@ -401,40 +552,11 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
         }
         __syncthreads();
         // the block's rank-1 terms on the elements outside its rows and columns
-        if (act) {
-            cplx g[TR][TC];
-            bool own[TR][TC];
-#pragma unroll
-            for (int a = 0; a < TR; ++a)
-#pragma unroll
-                for (int b = 0; b < TC; ++b) {
-                    const int r = r0 + a, c = c0 + b;
-                    own[a][b] = r < n && c < n && (unsigned)(r - slo) >= (unsigned)kb &&
-                                (unsigned)(c - slo) >= (unsigned)kb;
-                    g[a][b] = G[min(r, n - 1) * LD + min(c, n - 1)];
-                }
-#pragma unroll
-            for (int m = 0; m < KB; ++m) {
-                if (m >= kb) break;
-                const cplx cf = s.coef()[m];
-                cplx cr[TR], y[TC];
-#pragma unroll
-                for (int a = 0; a < TR; ++a) cr[a] = cmul(cf, s.col(m)[min(r0 + a, n - 1)]);
-#pragma unroll
-                for (int b = 0; b < TC; ++b) {
-                    const cplx yv = s.row(m)[min(c0 + b, n - 1)];
-                    y[b] = cmk(-yv.x, -yv.y);
-                }
-#pragma unroll
-                for (int a = 0; a < TR; ++a)
-#pragma unroll
-                    for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
-            }
-#pragma unroll
-            for (int a = 0; a < TR; ++a)
-#pragma unroll
-                for (int b = 0; b < TC; ++b)
-                    if (own[a][b]) G[(r0 + a) * LD + c0 + b] = g[a][b];
+        if constexpr (Cfg<NMAX>::GG) {
+            for (int tile = tid; tile < ncg * nrg; tile += blockDim.x)
+                rank_block_tile<NMAX>(x, G, n, slo, kb, (tile / ncg) * TR, (tile % ncg) * TC);
+        } else if (act) {
+            rank_block_tile<NMAX>(x, G, n, slo, kb, r0, c0);
         }
         __syncthreads();
     }
@@ -456,7 +578,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
             if (e < n * n) {
                 const int site = LEFT ? c : r;
                 const cplx f = s.accf()[site] ? s.ean()[site] : s.eao()[site];
-                s.U()[r * LD + c] = cmul(s.U()[r * LD + c], f);
+                x.U()[r * LD + c] = cmul(x.U()[r * LD + c], f);
             }
             c += dc;
             r += dr;
@@ -500,7 +622,7 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
     const bool total = (ch == 1);
     const uint32_t s0 = *s.seed();
     double* phis = x.phi + (long)slice * ns * 2;
-    cplx* G = s.G();
+    cplx* G = x.G();
 
     // per-site proposals (opU_get_delta, src/pairing/src/operator_Hubbard.f90:100-137)
     for (int i = tid; i < ns; i += blockDim.x) {
@@ -632,7 +754,7 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
             const cplx ep = acc ? s.ean()[site] : s.eao()[site];
             const cplx em = acc ? s.ebn()[site] : s.ebo()[site];
             const cplx f = (idx >= ns && flip) ? em : ep;
-            cplx* u = s.U() + er[k] * LD + ec[k];
+            cplx* u = x.U() + er[k] * LD + ec[k];
             *u = LEFT ? cmul(*u, f) : cmul(f, *u);
         }
     }
@@ -645,19 +767,18 @@ COLD void prop_channel_pair(Ctx<NMAX> x, int ch, int slice) {
 // right.  e^{-dtau K} is in W1, e^{+dtau K} in W2.
 template <int NMAX, bool LEFT>
 COLD void slice_products(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     const double* P = reinterpret_cast<const double*>(x.W1());   // e^{-dtau K}, real
     const double* M = reinterpret_cast<const double*>(x.W2());   // e^{+dtau K}, real
     if (LEFT) {
-        gemm_smem_real<TR, TC, true>(n, LD, s.G(), s.G(), P);
-        gemm_smem_real<TR, TC, false>(n, LD, s.G(), M, s.G());
-        gemm_smem_real<TR, TC, true>(n, LD, s.U(), s.U(), P);
+        gemm_real_any<NMAX, true>(x, x.G(), x.G(), P);
+        gemm_real_any<NMAX, false>(x, x.G(), M, x.G());
+        gemm_real_any<NMAX, true>(x, x.U(), x.U(), P);
     } else {
-        gemm_smem_real<TR, TC, false>(n, LD, s.G(), P, s.G());
-        gemm_smem_real<TR, TC, true>(n, LD, s.G(), s.G(), M);
-        gemm_smem_real<TR, TC, false>(n, LD, s.U(), P, s.U());
+        gemm_real_any<NMAX, false>(x, x.G(), P, x.G());
+        gemm_real_any<NMAX, true>(x, x.G(), x.G(), M);
+        gemm_real_any<NMAX, false>(x, x.U(), P, x.U());
     }
 }
 
@@ -674,7 +795,7 @@ COLD void measure(Ctx<NMAX> x) {
     const PointDev& P = x.P();
     const int n = x.n, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
     const double lq = (double)P.Lq, lq2 = lq * lq;
-    const cplx* G = s.G();
+    const cplx* G = x.G();
     const cplx* ph = s.ph();
     const bool hasK = P.hasK;
     // v: 0 sum Re(t_up), 1 sum |Gc|^2, 2-3 sf_K, 4-5 dw_K, 6-7 sum t_up, 8-9 sum du_i conj(du_j),
@@ -789,7 +910,7 @@ COLD void measure_pair(Ctx<NMAX> x) {
     const PointDev& P = x.P();
     const int n = x.n, ns = P.Ns, tid = threadIdx.x, lx = P.Lx, ly = P.Ly;
     const double lq = (double)P.Lq, lq2 = lq * lq, dns = (double)ns;
-    const cplx* G = s.G();
+    const cplx* G = x.G();
     const cplx* ph = s.ph();
     const bool hasK = P.hasK;
     // v: 0-1 sum Dbb, 2-3 sum Dbc, 4 sum |D_ij|^2, 5-6 sf_K, 7-8 dw_K, 9 kinetic bonds,
@@ -911,26 +1032,26 @@ COLD void measure_pair(Ctx<NMAX> x) {
 // stabilisation (stabilization.f90:69-190)
 
 // stab_UR: (U_R D_R) P = Q R;  D_R <- |diag R|;  V_R <- R P^T V_R;  U_R <- Q.
-// U_R is s.U(); on exit the new V_R is in x.W2() and in A.VRc, D_R in A.DRc.
+// U_R is x.U(); on exit the new V_R is in x.W2() and in A.VRc, D_R in A.DRc.
 template <int NMAX>
 COLD void stab_UR(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        x.W1()[r * LD + c] = cmul(s.U()[r * LD + c], x.A().DRc[c]);
+        x.W1()[r * LD + c] = cmul(x.U()[r * LD + c], x.A().DRc[c]);
     }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.qr());
+    qrp_any(x, x.W1());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DRc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
         x.W2()[r * LD + c] = x.A().VRc[s.piv()[r] * n + c];
     }
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), op_n(x.W2(), LD), TRI_A_UPPER);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.tau(), s.U(), false);
+    gemm_any(x, x.W2(), op_n(x.W1(), LD), op_n(x.W2(), LD), TRI_A_UPPER);
+    form_q_any(x, x.W1(), x.U(), false);
     sstore(n, LD, x.A().VRc, x.W2());
     __syncthreads();
 }
@@ -938,23 +1059,23 @@ COLD void stab_UR(Ctx<NMAX> x) {
 // stab_UL: (U_L^H D_L) P = Q R;  D_L <- |diag R|;  V_L <- V_L P R^H;  U_L <- Q^H.
 template <int NMAX>
 COLD void stab_UL(Ctx<NMAX> x) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        x.W1()[r * LD + c] = cmul(cconj(s.U()[c * LD + r]), x.A().DLc[c]);
+        x.W1()[r * LD + c] = cmul(cconj(x.U()[c * LD + r]), x.A().DLc[c]);
     }
     __syncthreads();
-    qrp_inplace<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.qr());
+    qrp_any(x, x.W1());
     for (int i = threadIdx.x; i < n; i += blockDim.x) x.A().DLc[i] = cmk(s.d()[i], 0.0);
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
         x.W2()[r * LD + c] = x.A().VLc[r * n + s.piv()[c]];
     }
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W2(), LD), op_c(x.W1(), LD), TRI_B_LOWER_FROM_C);
-    form_q<Cfg<NMAX>::R8, Cfg<NMAX>::CPS>(n, LD, x.W1(), s.tau(), s.U(), true);
+    gemm_any(x, x.W2(), op_n(x.W2(), LD), op_c(x.W1(), LD), TRI_B_LOWER_FROM_C);
+    form_q_any(x, x.W1(), x.U(), true);
     sstore(n, LD, x.A().VLc, x.W2());
     __syncthreads();
 }
@@ -971,42 +1092,41 @@ COLD void stab_UL(Ctx<NMAX> x) {
 // triangular solve) so that every product runs on shared memory.
 template <int NMAX>
 COLD void green_from_M(Ctx<NMAX> x, int nt, bool right_local, bool want_logdet) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, R8 = Cfg<NMAX>::R8, CPS = Cfg<NMAX>::CPS;
     constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
     cplx* rinv = reinterpret_cast<cplx*>(s.vn1());   // vn1 | vn2, n complex
     double* dinv = s.u2();
-    const MatOp Uloc = op_c(s.U(), LD);
+    const MatOp Uloc = op_c(x.U(), LD);
     const MatOp URh = right_local ? Uloc : op_c(x.A().URc, n);
     const MatOp ULh = right_local ? op_c(x.A().ULc, n) : Uloc;
-    if (nt > L / 2) conj_transpose_inplace<Cfg<NMAX>::MAXE>(n, LD, x.W2());
-    qrp_inplace<R8, CPS>(n, LD, x.W2(), s.qr());
+    if (nt > L / 2) conj_transpose_any(x, x.W2());
+    qrp_any(x, x.W2());
     if (nt < L / 2 + 1) {
         copy_op(n, LD, x.W1(), URh);
-        apply_qh_left<R8, CPS>(n, LD, x.W2(), s.tau(), x.W1());
+        apply_qh_left_any(x, x.W2(), x.W1());
         diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
-        trsm_left_upper<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
-        permute_rows<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
+        trsm_left_any(x, x.W2(), rinv, dinv, x.W1());
+        permute_rows_any(x, x.W1(), false);
         if (right_local) {   // U_L^H from HBM, staged
             sload(n, LD, x.W2(), x.A().ULc);
             __syncthreads();
-            gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.W2(), LD), op_n(x.W1(), LD));
+            gemm_any(x, x.W2(), op_c(x.W2(), LD), op_n(x.W1(), LD));
         } else {
-            gemm_rs<TR, TC>(n, LD, x.W2(), Uloc, op_n(x.W1(), LD));
+            gemm_any(x, x.W2(), Uloc, op_n(x.W1(), LD));
         }
     } else {
         copy_op(n, LD, x.W1(), ULh);
-        apply_q_right<R8, CPS>(n, LD, x.W2(), s.tau(), x.W1());
+        apply_q_right_any(x, x.W2(), x.W1());
         diag_inverse(n, LD, x.W2(), s.d(), rinv, dinv);
-        trsm_right_upperH<R8, CPS>(n, LD, x.W2(), rinv, dinv, x.W1());
-        permute_cols<Cfg<NMAX>::MAXE>(n, LD, x.W1(), s.piv(), s.ipiv(), false);
+        trsm_right_any(x, x.W2(), rinv, dinv, x.W1());
+        permute_cols_any(x, x.W1(), false);
         if (right_local) {
-            gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), Uloc);
+            gemm_any(x, x.W2(), op_n(x.W1(), LD), Uloc);
         } else {             // U_R^H from HBM, staged
             sload(n, LD, x.W2(), x.A().URc);
             __syncthreads();
-            gemm_rs<TR, TC>(n, LD, x.W2(), op_n(x.W1(), LD), op_c(x.W2(), LD));
+            gemm_any(x, x.W2(), op_n(x.W1(), LD), op_c(x.W2(), LD));
         }
     }
     if (want_logdet) {
@@ -1040,7 +1160,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
     constexpr int LD = Cfg<NMAX>::LD;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - (e / n) * n;
-        v[0] += cabsv(csub(x.W2()[r * LD + c], s.G()[r * LD + c]));
+        v[0] += cabsv(csub(x.W2()[r * LD + c], x.G()[r * LD + c]));
     }
     block_sum<1>(v, s.red());
     if (threadIdx.x == 0) {
@@ -1049,7 +1169,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
         x.sc->xmean += dif;
         if (!(dif == dif) || dif > 1.0e300) x.sc->status |= 1;
     }
-    scopy(n, LD, s.G(), x.W2());
+    scopy(n, LD, x.G(), x.W2());
     __syncthreads();
 }
 
@@ -1057,7 +1177,7 @@ DEVI void drift_and_replace(Ctx<NMAX>& x) {
 // and the left side in HBM (A.ULc, A.VLc, A.DLc).
 template <int NMAX>
 COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     // HBM operands are staged into the workspace the product overwrites (the
@@ -1065,10 +1185,10 @@ COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
     // V_R in W2 is no longer needed after the first product (VRc holds it).
     sload(n, LD, x.W1(), x.A().VLc);
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W2(), LD), op_n(x.W1(), LD));   // V_R V_L
+    gemm_any(x, x.W1(), op_n(x.W2(), LD), op_n(x.W1(), LD));   // V_R V_L
     sload(n, LD, x.W2(), x.A().ULc);
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(s.U(), LD), op_c(x.W2(), LD));    // U_R^H U_L^H
+    gemm_any(x, x.W2(), op_c(x.U(), LD), op_c(x.W2(), LD));    // U_R^H U_L^H
     form_M(x);
     green_from_M(x, nt, true, want_logdet);
 }
@@ -1077,15 +1197,15 @@ COLD void stab_green_right_local(Ctx<NMAX> x, int nt, bool want_logdet) {
 // right side in HBM.
 template <int NMAX>
 COLD void stab_green_left_local(Ctx<NMAX> x, int nt) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
+    constexpr int LD = Cfg<NMAX>::LD;
     auto& s = x.s;
     const int n = x.n;
     sload(n, LD, x.W1(), x.A().VRc);
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W1(), op_n(x.W1(), LD), op_n(x.W2(), LD));   // V_R V_L
+    gemm_any(x, x.W1(), op_n(x.W1(), LD), op_n(x.W2(), LD));   // V_R V_L
     sload(n, LD, x.W2(), x.A().URc);
     __syncthreads();
-    gemm_rs<TR, TC>(n, LD, x.W2(), op_c(x.W2(), LD), op_c(s.U(), LD));    // U_R^H U_L^H
+    gemm_any(x, x.W2(), op_c(x.W2(), LD), op_c(x.U(), LD));    // U_R^H U_L^H
     form_M(x);
     green_from_M(x, nt, false, false);
 }
@@ -1104,7 +1224,7 @@ COLD void wrap_L(Ctx<NMAX> x, int nt) {
         stab_green_left_local(x, nt);
         drift_and_replace(x);
     }
-    sstore(n, Cfg<NMAX>::LD, x.A().ULs(st), s.U());
+    sstore(n, Cfg<NMAX>::LD, x.A().ULs(st), x.U());
     gcopy(x.A().VLs(st), x.A().VLc, n * n);
     gcopy(x.A().DLs(st), x.A().DLc, n);
     __syncthreads();
@@ -1125,7 +1245,7 @@ COLD void wrap_R(Ctx<NMAX> x, int nt) {
         stab_green_right_local(x, nt, nt == x.P().L);
         drift_and_replace(x);
     }
-    sstore(n, Cfg<NMAX>::LD, x.A().URs(st), s.U());
+    sstore(n, Cfg<NMAX>::LD, x.A().URs(st), x.U());
     gcopy(x.A().VRs(st), x.A().VRc, n * n);
     gcopy(x.A().DRs(st), x.A().DRc, n);
     __syncthreads();
@@ -1173,12 +1293,12 @@ DEVI void flush_obs(Ctx<NMAX>& x, double* gobs) {
 
 template <int NMAX, bool PAIR, bool LEFT>
 DEVI void prop_any(Ctx<NMAX>& x, int ch, int slice) {
-    if (PAIR) prop_channel_pair<NMAX, LEFT>(x, ch, slice);
+    if constexpr (PAIR) prop_channel_pair<NMAX, LEFT>(x, ch, slice);
     else prop_channel<NMAX, LEFT>(x, ch, slice);
 }
 template <int NMAX, bool PAIR>
 DEVI void measure_any(Ctx<NMAX>& x) {
-    if (PAIR) measure_pair<NMAX>(x);
+    if constexpr (PAIR) measure_pair<NMAX>(x);
     else measure<NMAX>(x);
 }
 
@@ -1206,8 +1326,8 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
         for (int k = 0; k < 5; ++k) s.cnt()[k] = 0;
     }
     load_obs(x);
-    sload(n, Cfg<NMAX>::LD, s.G(), x.A().G);
-    sload(n, Cfg<NMAX>::LD, s.U(), x.A().ULc);
+    sload(n, Cfg<NMAX>::LD, x.G(), x.A().G);
+    sload(n, Cfg<NMAX>::LD, x.U(), x.A().ULc);
     __syncthreads();
     load_expT(x);
     lap(3);
@@ -1226,10 +1346,10 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
         lap(0);
     }
     wrap_L(x, 0);
-    sstore(n, Cfg<NMAX>::LD, x.A().ULc, s.U());
+    sstore(n, Cfg<NMAX>::LD, x.A().ULc, x.U());
     __syncthreads();
     // ---- right traversal
-    sload(n, Cfg<NMAX>::LD, s.U(), x.A().URc);
+    sload(n, Cfg<NMAX>::LD, x.U(), x.A().URc);
     __syncthreads();
     wrap_R(x, 0);
     lap(3);
@@ -1246,8 +1366,8 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
         measure_any<NMAX, PAIR>(x);
         lap(2);
     }
-    sstore(n, Cfg<NMAX>::LD, x.A().URc, s.U());
-    sstore(n, Cfg<NMAX>::LD, x.A().G, s.G());
+    sstore(n, Cfg<NMAX>::LD, x.A().URc, x.U());
+    sstore(n, Cfg<NMAX>::LD, x.A().G, x.G());
     flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
     if (threadIdx.x == 0) {
         x.sc->seed = *s.seed();
@@ -1267,15 +1387,15 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
 // e^{-alpha phi} in the U2 channel (src/pairing/src/operator_Hubbard.f90:155-166).
 template <int NMAX, bool PAIR>
 __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kernel(KernelArgs ka, const int* idx, int count) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, LD = Cfg<NMAX>::LD;
+    constexpr int LD = Cfg<NMAX>::LD;
     if ((int)blockIdx.x >= count) return;
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
     if (!setup_ctx(x, ka, chain)) return;
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
-    set_identity(n, LD, s.U());
-    set_identity(n, LD, s.G());
+    set_identity(n, LD, x.U());
+    set_identity(n, LD, x.G());
     set_identity(n, n, x.A().VRc);
     set_identity(n, n, x.A().ULc);
     set_identity(n, n, x.A().VLc);
@@ -1284,7 +1404,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
         x.A().DLc[i] = cmk(1.0, 0.0);
     }
     __syncthreads();
-    sstore(n, LD, x.A().URs(0), s.U());
+    sstore(n, LD, x.A().URs(0), x.U());
     gcopy(x.A().VRs(0), x.A().VRc, n * n);
     gcopy(x.A().DRs(0), x.A().DRc, n);
     sload_real(n, LD, reinterpret_cast<double*>(x.W1()), x.P().expP);
@@ -1302,29 +1422,29 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
                 const double p = ph[site * 2 + ch];
                 const bool neg = PAIR && r >= ns && flip;
                 const cplx f = neg ? cexpz(cmk(-(ar * p), -(ai * p))) : cexpz(cmk(ar * p, ai * p));
-                s.U()[r * LD + c] = cmul(f, s.U()[r * LD + c]);
+                x.U()[r * LD + c] = cmul(f, x.U()[r * LD + c]);
             }
             __syncthreads();
         }
-        gemm_smem_real<TR, TC, false>(n, LD, s.U(), reinterpret_cast<const double*>(x.W1()), s.U());
+        gemm_real_any<NMAX, false>(x, x.U(), reinterpret_cast<const double*>(x.W1()), x.U());
         if (nt % x.P().Nwrap == 0) {
             const int st = nt / x.P().Nwrap;
             stab_UR(x);
-            sstore(n, LD, x.A().URs(st), s.U());
+            sstore(n, LD, x.A().URs(st), x.U());
             gcopy(x.A().VRs(st), x.A().VRc, n * n);
             gcopy(x.A().DRs(st), x.A().DRc, n);
             __syncthreads();
             if (nt == L) {
                 stab_green_right_local(x, nt, true);
-                scopy(n, LD, s.G(), x.W2());
+                scopy(n, LD, x.G(), x.W2());
                 __syncthreads();
             }
             sload_real(n, LD, reinterpret_cast<double*>(x.W1()), x.P().expP);
             __syncthreads();
         }
     }
-    sstore(n, LD, x.A().URc, s.U());
-    sstore(n, LD, x.A().G, s.G());
+    sstore(n, LD, x.A().URc, x.U());
+    sstore(n, LD, x.A().G, x.G());
 }
 
 // LocalU_prop_therm / LocalU_metro_therm over the whole field, nwarm sweeps
@@ -1462,7 +1582,7 @@ static cudaError_t launch_cls(int which, const KernelArgs& ka, const int* idx, i
     return cudaGetLastError();
 }
 
-// class index: size class (NMAX 16 / 36 / 72) + 3 * Nambu sector
+// class index: size class (NMAX 16 / 36 / 72) + 3 * Nambu sector; 6 = NMAX 144, number-conserving
 static cudaError_t launch_any(int which, int cls, const KernelArgs& ka, const int* idx, int count, cudaStream_t st) {
     switch (cls) {
         case 0: return launch_cls<16, false>(which, ka, idx, count, st);
@@ -1471,6 +1591,7 @@ static cudaError_t launch_any(int which, int cls, const KernelArgs& ka, const in
         case 3: return launch_cls<16, true>(which, ka, idx, count, st);
         case 4: return launch_cls<36, true>(which, ka, idx, count, st);
         case 5: return launch_cls<72, true>(which, ka, idx, count, st);
+        case 6: return launch_cls<144, false>(which, ka, idx, count, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1508,22 +1629,26 @@ cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st
     return cudaGetLastError();
 }
 long long class_work_elems(int cls) {
+    if (cls == 6) return 5LL * 144 * Cfg<144>::LD;   // W1, W2, G, U, product scratch
     const int sz = cls % 3;
     auto w = [](int nmax, int ld, bool gw) { return gw ? 2LL * nmax * ld : 0LL; };
     return sz == 0 ? w(16, Cfg<16>::LD, Cfg<16>::GW)
                    : (sz == 1 ? w(36, Cfg<36>::LD, Cfg<36>::GW) : w(72, Cfg<72>::LD, Cfg<72>::GW));
 }
 size_t smem_bytes(int cls) {
+    if (cls == 6) return Smem<144>::bytes();
     const int sz = cls % 3;
     return sz == 0 ? Smem<16>::bytes() : (sz == 1 ? Smem<36>::bytes() : Smem<72>::bytes());
 }
 int class_nmax(int cls) {
+    if (cls == 6) return 144;
     const int sz = cls % 3;
     return sz == 0 ? 16 : (sz == 1 ? 36 : 72);
 }
 int class_of(int n, int pairing) {
     for (int c = 0; c < 3; ++c)
         if (n <= class_nmax(c)) return c + (pairing ? 3 : 0);
+    if (!pairing && n <= 144) return 6;
     return -1;
 }
 

@@ -281,3 +281,19 @@ def test_bin_graph_replay_and_recapture(solver_mod):
                 assert_green_close(ens.green(c), ch.prop.Gr, f"bin {b} chain {c}")
                 compare_bin(cobs[c], ch.obs.as_dict(latt), f"bin {b} chain {c}")
         assert ens.phase_timers(False).sum() > 0
+
+
+@pytest.mark.parametrize("lx,ly", [(12, 12), (9, 9), (10, 11)])
+def test_n144_class_against_oracle(solver_mod, lx, ly):
+    """N = 144, 81 and 110 sites: the class whose G, U, workspaces and product
+    scratch live in a per-chain HBM region (warp-per-column factorisations,
+    tiled out-of-place products); 10x11 has no K point."""
+    op, sp = both_params(U2=-0.5, Nlx=lx, Nly=ly, Ltrot=20, Beta=1.0, Nwrap=5)
+    _run_both(op, sp, [41, 42], nbins=1)
+
+
+def test_12x12_beta10_point(solver_mod):
+    """The 12x12 point: U1 = 1, U2 = -0.5, mu = -5, beta = 10, dtau = 0.05
+    (L = 200), Nwrap = 10, one chain, one bin."""
+    op, sp = both_params(U2=-0.5, Nlx=12, Nly=12, Ltrot=200, Beta=10.0, Nwrap=10)
+    _run_both(op, sp, [20241203], nbins=1)
