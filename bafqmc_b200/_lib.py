@@ -16,6 +16,7 @@ ERRORS = {-1: "BAFQMC_EARG", -2: "BAFQMC_ECUDA", -3: "BAFQMC_EUNSUPPORTED", -4: 
 OBS_SCALARS = 32
 COUNTERS = 14
 POLE_SCALARS = 5
+PRECISION = {"fp64": 0, "mixed": 1}
 
 
 class BafqmcError(RuntimeError):
@@ -58,6 +59,7 @@ SIGNATURES = {
     "bafqmc_get_green": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_log_weight": (C.c_int, [_P, _DP]),
     "bafqmc_pole_diagnostics": (C.c_int, [_P, _DP, C.c_int, _DP]),
+    "bafqmc_set_precision": (C.c_int, [_P, C.c_int]),
     "bafqmc_counters": (C.c_int, [_P, _DP]),
     "bafqmc_phase_timers": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_synchronize": (C.c_int, [_P]),

@@ -200,10 +200,11 @@ struct bafqmc_handle {
     ChainScalars* d_sc = nullptr;
     bool have_fields = false, pre_done = false, bin_done = false;
     int timers = 0;
+    int mixed = 0;   // bafqmc_set_precision
     // the launches of one bin (reset, nsweep sweeps of every class, finish),
     // captured once per (nsweep, timers) and replayed as one graph launch
     cudaGraphExec_t bin_graph = nullptr;
-    int graph_nsweep = 0, graph_timers = 0;
+    int graph_nsweep = 0, graph_timers = 0, graph_mixed = 0;
 
     bq::KernelArgs args() const {
         bq::KernelArgs ka;
@@ -216,6 +217,7 @@ struct bafqmc_handle {
         ka.obs = d_obs;
         ka.sc = d_sc;
         ka.timers = timers;
+        ka.mixed = mixed;
         return ka;
     }
 };
@@ -595,7 +597,7 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
     if (!h || nsweep < 1) return fail(BAFQMC_EARG, "bad sweep arguments");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     CK(cudaSetDevice(h->device));
-    if (!h->bin_graph || h->graph_nsweep != nsweep || h->graph_timers != h->timers) {
+    if (!h->bin_graph || h->graph_nsweep != nsweep || h->graph_timers != h->timers || h->graph_mixed != h->mixed) {
         if (h->bin_graph) {
             CK(cudaGraphExecDestroy(h->bin_graph));
             h->bin_graph = nullptr;
@@ -616,6 +618,7 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
         }
         h->graph_nsweep = nsweep;
         h->graph_timers = h->timers;
+        h->graph_mixed = h->mixed;
     }
     CK(cudaGraphLaunch(h->bin_graph, h->stream));
     h->bin_done = true;
@@ -742,6 +745,14 @@ int bafqmc_counters(bafqmc_handle* h, double* out) {
         o[12] = sc[c].acc_tot[0];
         o[13] = sc[c].acc_tot[1];
     }
+    return BAFQMC_OK;
+}
+
+int bafqmc_set_precision(bafqmc_handle* h, int mode) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    if (mode != BAFQMC_PRECISION_FP64 && mode != BAFQMC_PRECISION_MIXED)
+        return fail(BAFQMC_EARG, "precision must be BAFQMC_PRECISION_FP64 or BAFQMC_PRECISION_MIXED");
+    h->mixed = mode == BAFQMC_PRECISION_MIXED ? 1 : 0;
     return BAFQMC_OK;
 }
 
@@ -890,6 +901,7 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     ka.obs = reinterpret_cast<double*>(base + o_ob);
     ka.sc = sc;
     ka.timers = 0;
+    ka.mixed = 0;
     const int* d_ix = reinterpret_cast<const int*>(base + o_ix);
     CK(bq::launch_pre(cls, ka, d_ix, nchains, st));
     CK(bq::launch_bin_reset(ka, st));

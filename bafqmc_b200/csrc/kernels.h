@@ -20,6 +20,7 @@ struct KernelArgs {
     double* obs;
     ChainScalars* sc;
     int timers;   // nonzero: accumulate per-phase SM cycles into ChainScalars::cyc
+    int mixed;    // nonzero: slice products of the N <= 144 class on the tensor cores (3xTF32)
 };
 
 // kernel classes of the fused sweep: size (N <= 16, N <= 36, N <= 72) + 3 * sector

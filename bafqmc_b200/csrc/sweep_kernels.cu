@@ -11,6 +11,7 @@
 #include "sweep.cuh"
 #include "kernels.h"
 #include "linalg_big.cuh"
+#include "tc.cuh"
 
 namespace bq {
 
@@ -25,6 +26,7 @@ template <int NMAX> struct Cfg;
 // budget.  GW: the two workspaces live in HBM (after the chain's arena) and
 // only G and U in shared memory.
 template <> struct Cfg<16> {
+    static constexpr bool TCORE = false;
     static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, NB = 64, MINB = 2;
     static constexpr bool GW = false, GG = false;
     static constexpr int RW = 1, CPW = 1;
@@ -34,12 +36,14 @@ static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
 // per SM at 192 threads with the workspaces in HBM measured 42% slower: the
 // slice products and wraps slow down more than the third chain adds.)
 template <> struct Cfg<36> {
+    static constexpr bool TCORE = false;
     static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, NB = 64, MINB = 2;
     static constexpr bool GW = false, GG = false;
     static constexpr int RW = 2, CPW = 1;
 };
 // N <= 72: G and U in shared memory, the workspaces in HBM (one CTA per SM)
 template <> struct Cfg<72> {
+    static constexpr bool TCORE = false;
     static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = 73, NB = 96, MINB = 1;
     static constexpr bool GW = true, GG = false;
     static constexpr int RW = 3, CPW = 1;
@@ -51,6 +55,7 @@ template <> struct Cfg<72> {
 // TR x TC tiles out of place and the factorisations use linalg_big.cuh (one
 // warp per column, RW rows per lane, CPW columns at a time).
 template <> struct Cfg<144> {
+    static constexpr bool TCORE = true;   // slice products may run on the tensor cores (tc.cuh)
     static constexpr int THREADS = 512, TR = 2, TC = 3, MAXE = 41, KB = 4, R8 = 18, CPS = 3, LD = 145, NB = 160,
                          MINB = 1;
     static constexpr bool GW = true, GG = true;
@@ -95,7 +100,12 @@ struct Smem {
     static constexpr size_t oIbc = oAccf + sizeof(int) * NMAX, oSeed = oIbc + 4 * sizeof(int);
     static constexpr size_t oSxy = oSeed + 16;   // site coordinates x | y << 16
     static constexpr size_t oCnt = oSxy + ((sizeof(int) * NMAX + 15) / 16) * 16;   // nacc[2], nc[2], nobs of the sweep
-    static constexpr size_t bytes() { return oCnt + 48; }
+    // tensor-core staging (classes with Cfg::TCORE): A hi | A lo | B hi | B lo, then
+    // the MMA barrier, the tensor-memory base, the barrier parity and the on flag
+    static constexpr bool TCORE = Cfg<NMAX>::TCORE;
+    static constexpr size_t oTc = ((oCnt + 48 + 127) / 128) * 128;
+    static constexpr size_t oTcBar = oTc + 2 * kTcABytes + 2 * kTcBBytes;
+    static constexpr size_t bytes() { return TCORE ? oTcBar + 32 : oCnt + 48; }
 
     template <class T>
     static DEVI T* at(size_t off) { return reinterpret_cast<T*>(bq_smem + off); }
@@ -132,6 +142,14 @@ struct Smem {
     DEVI int* sxy() const { return at<int>(oSxy); }
     DEVI long long* cnt() const { return at<long long>(oCnt); }
     DEVI int* strip_warp() const { return at<int>(oCnt + 40); }
+    DEVI uint64_t* tc_mbar() const { return at<uint64_t>(oTcBar); }
+    DEVI uint32_t* tc_slot() const { return at<uint32_t>(oTcBar + 8); }
+    DEVI uint32_t* tc_phase() const { return at<uint32_t>(oTcBar + 12); }
+    DEVI int* tc_on() const { return at<int>(oTcBar + 16); }
+    DEVI TcBufs tcb() const {
+        return TcBufs{at<uint32_t>(oTc), at<uint32_t>(oTc + kTcABytes), at<uint32_t>(oTc + 2 * kTcABytes),
+                      at<uint32_t>(oTc + 2 * kTcABytes + kTcBBytes), tc_mbar(), *tc_slot()};
+    }
     DEVI QRScratch qr() const { return QRScratch{tau(), piv(), ipiv(), vn1(), vn2(), d(), cbc(), ibc()}; }
 };
 
@@ -255,6 +273,57 @@ DEVI void conj_transpose_any(Ctx<NMAX>& x, cplx* A) {
     using C_ = Cfg<NMAX>;
     if constexpr (C_::GG) conj_transpose_big(x.n, C_::LD, A, x.S());
     else conj_transpose_inplace<C_::MAXE>(x.n, C_::LD, A);
+}
+
+// One slice product in place: X <- X R (RIGHT) or X <- R X, R = e^{-+dtau K}
+// real.  With the mixed-precision option on, classes with tensor-core staging
+// run it as tc_product; a product that did not complete within its wait bound
+// leaves X unchanged, flags the chain (status bit 2) and the kernel continues
+// in FP64.
+template <int NMAX, bool RIGHT>
+DEVI void slice_mult(Ctx<NMAX>& x, cplx* X, const double* R) {
+    if constexpr (Cfg<NMAX>::TCORE) {
+        if (*x.s.tc_on()) {
+            if (tc_product(x.n, Cfg<NMAX>::LD, X, R, RIGHT, x.s.tcb(), x.s.tc_phase())) return;
+            if (threadIdx.x == 0) {
+                *x.s.tc_on() = 0;
+                x.sc->status |= 4;
+            }
+            __syncthreads();
+        }
+    }
+    if constexpr (RIGHT) gemm_real_any<NMAX, true>(x, X, X, R);
+    else gemm_real_any<NMAX, false>(x, X, R, X);
+}
+
+// Tensor memory and the MMA barrier of a CTA that runs mixed-precision products
+// (one CTA per SM in the classes with Cfg::TCORE): allocated after set-up, freed at exit.
+template <int NMAX>
+DEVI void tc_begin(Ctx<NMAX>& x, const KernelArgs& ka) {
+    if constexpr (Cfg<NMAX>::TCORE) {
+        if (threadIdx.x == 0) {
+            *x.s.tc_on() = ka.mixed ? 1 : 0;
+            *x.s.tc_phase() = 0;
+        }
+        if (ka.mixed) {
+            if (threadIdx.x < 32) tmem_alloc(smem_u32(x.s.tc_slot()), kTcCols);
+            if (threadIdx.x == 0) mbar_init(smem_u32(x.s.tc_mbar()), 1);
+            tc_fence_before();
+        }
+        __syncthreads();
+        if (ka.mixed) tc_fence_after();
+    }
+}
+template <int NMAX>
+DEVI void tc_end(Ctx<NMAX>& x, const KernelArgs& ka) {
+    if constexpr (Cfg<NMAX>::TCORE) {
+        if (ka.mixed) {
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (threadIdx.x < 32) tmem_dealloc(*x.s.tc_slot(), kTcCols);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -772,13 +841,13 @@ COLD void slice_products(Ctx<NMAX> x) {
     const double* P = reinterpret_cast<const double*>(x.W1());   // e^{-dtau K}, real
     const double* M = reinterpret_cast<const double*>(x.W2());   // e^{+dtau K}, real
     if (LEFT) {
-        gemm_real_any<NMAX, true>(x, x.G(), x.G(), P);
-        gemm_real_any<NMAX, false>(x, x.G(), M, x.G());
-        gemm_real_any<NMAX, true>(x, x.U(), x.U(), P);
+        slice_mult<NMAX, true>(x, x.G(), P);
+        slice_mult<NMAX, false>(x, x.G(), M);
+        slice_mult<NMAX, true>(x, x.U(), P);
     } else {
-        gemm_real_any<NMAX, false>(x, x.G(), P, x.G());
-        gemm_real_any<NMAX, true>(x, x.G(), x.G(), M);
-        gemm_real_any<NMAX, false>(x, x.U(), P, x.U());
+        slice_mult<NMAX, false>(x, x.G(), P);
+        slice_mult<NMAX, true>(x, x.G(), M);
+        slice_mult<NMAX, false>(x, x.U(), P);
     }
 }
 
@@ -1309,6 +1378,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
     if (!setup_ctx(x, ka, chain)) return;
+    tc_begin(x, ka);
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
     const bool tm = ka.timers && threadIdx.x == 0;
@@ -1379,6 +1449,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
     }
     lap(3);
 #undef lap
+    tc_end(x, ka);
 }
 
 // Local_sweep_pre (local_sweep.f90:80-94) with Prop_make's identities
@@ -1392,6 +1463,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
     if (!setup_ctx(x, ka, chain)) return;
+    tc_begin(x, ka);
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
     set_identity(n, LD, x.U());
@@ -1426,7 +1498,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
             }
             __syncthreads();
         }
-        gemm_real_any<NMAX, false>(x, x.U(), reinterpret_cast<const double*>(x.W1()), x.U());
+        slice_mult<NMAX, false>(x, x.U(), reinterpret_cast<const double*>(x.W1()));
         if (nt % x.P().Nwrap == 0) {
             const int st = nt / x.P().Nwrap;
             stab_UR(x);
@@ -1445,6 +1517,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
     }
     sstore(n, LD, x.A().URc, x.U());
     sstore(n, LD, x.A().G, x.G());
+    tc_end(x, ka);
 }
 
 // LocalU_prop_therm / LocalU_metro_therm over the whole field, nwarm sweeps

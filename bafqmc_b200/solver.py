@@ -165,6 +165,11 @@ class Ensemble:
         _lib.check(self.lib.bafqmc_log_weight(self.h, _dptr(out)))
         return out
 
+    def set_precision(self, mode: str):
+        """"fp64" (default) or "mixed": slice products of chains with 72 < Ndim <= 144
+        on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision)."""
+        _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
+
     POLE_NAMES = ("pole_distance", "pole_x", "green_spectral_radius", "green_smax", "log_weight")
 
     def pole_diagnostics(self) -> list[dict | None]:

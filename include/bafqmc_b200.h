@@ -139,13 +139,27 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out);
 int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars);
 
 /* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
- * status, seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
+ * status (bit 0: non-finite drift; bit 2: a tensor-core product did not
+ * complete within its wait bound and the chain continued in FP64), seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
  * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and
  * %count_accepted over all bins, src/pairing/src/operator_Hubbard.f90:269-284.
  * The Nambu weight ratio is real and positive here, so PhaseCounter's phase
  * sums are zero). */
 #define BAFQMC_COUNTERS 14
 int bafqmc_counters(bafqmc_handle* h, double* out);
+
+/* Arithmetic of the slice propagation (multiply.f90:72-86, propT_L/R; the
+ * reference computes it in FP64 with ZGEMM).  BAFQMC_PRECISION_MIXED runs the
+ * slice products of chains with 72 < Ndim <= 144 (number-conserving, up to
+ * 12x12) on the tensor cores in 3xTF32-compensated FP32 (the products
+ * X e^{-+dtau K} and e^{-+dtau K} X with FP32 accumulation), in bafqmc_pre and
+ * the sweeps; the stabilisation, (I - B)^{-1}, ratios and acceptance stay
+ * FP64, and chains of the other size classes always run FP64.  Decisions of
+ * a mixed chain are not bit-identical to the FP64 chain's.  Takes effect from
+ * the next bafqmc_pre / bafqmc_sweep.  Default BAFQMC_PRECISION_FP64. */
+#define BAFQMC_PRECISION_FP64 0
+#define BAFQMC_PRECISION_MIXED 1
+int bafqmc_set_precision(bafqmc_handle* h, int mode);
 
 /* Per-phase SM cycle counters of the sweep kernel (the reference has only a
  * total wall time, main.f90:26-27,67-71).  enable switches counting for the
