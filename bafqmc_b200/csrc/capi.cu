@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/bafqmc_b200.h"
 #include "kernels.h"
 #include "sweep.cuh"
@@ -24,6 +26,13 @@ int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
+// NVTX range over one C-ABI call, so that a profiler timeline shows the
+// host-side phases (set-up, pre, bins, diagnostics) around the kernels.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 int cuda_fail(cudaError_t e, const char* where) {
     return fail(BAFQMC_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
@@ -346,6 +355,7 @@ const char* bafqmc_last_error(void) { return g_err.c_str(); }
 
 int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
                   bafqmc_handle** out) {
+    NvtxRange nvtx_("bafqmc_create");
     if (!out || !pts || npts < 1 || nchains < 1 || !chain_point) return fail(BAFQMC_EARG, "bad create arguments");
     *out = nullptr;
     bafqmc_handle* h = new bafqmc_handle();
@@ -491,14 +501,25 @@ static int upload_state(bafqmc_handle* h, const int32_t* seeds, const double* ph
     std::memset(sc.data(), 0, sizeof(ChainScalars) * h->nchains);
     for (int c = 0; c < h->nchains; ++c) sc[c].seed = (uint32_t)seeds[c];
     CK(cudaMemcpyAsync(h->d_sc, sc.data(), sizeof(ChainScalars) * h->nchains, cudaMemcpyHostToDevice, h->stream));
+    // fields must be finite (the reference would carry a NaN into every weight)
+    int* d_bad = reinterpret_cast<int*>(h->d_tmp);
+    CK(bq::launch_field_check(h->args(), d_bad, h->stream));
+    std::vector<int> bad(h->nchains);
+    CK(cudaMemcpyAsync(bad.data(), d_bad, sizeof(int) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    h->have_fields = true;
     h->pre_done = false;
     h->bin_done = false;
+    for (int c = 0; c < h->nchains; ++c)
+        if (bad[c]) {
+            h->have_fields = false;
+            return fail(BAFQMC_EARG, "non-finite field value (NaN or Inf) in chain " + std::to_string(c));
+        }
+    h->have_fields = true;
     return BAFQMC_OK;
 }
 
 int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds) {
+    NvtxRange nvtx_("bafqmc_fields_from_seeds");
     if (!h || !seeds) return fail(BAFQMC_EARG, "null argument");
     std::vector<double> phi(h->phi_total);
     std::vector<int32_t> adv(h->nchains);
@@ -543,11 +564,13 @@ int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds) {
 }
 
 int bafqmc_set_state(bafqmc_handle* h, const int32_t* seeds, const double* phi) {
+    NvtxRange nvtx_("bafqmc_set_state");
     if (!h || !seeds || !phi) return fail(BAFQMC_EARG, "null argument");
     return upload_state(h, seeds, phi);
 }
 
 int bafqmc_get_state(bafqmc_handle* h, int32_t* seeds, double* phi) {
+    NvtxRange nvtx_("bafqmc_get_state");
     if (!h) return fail(BAFQMC_EARG, "null handle");
     CK(cudaSetDevice(h->device));
     if (phi) CK(cudaMemcpyAsync(phi, h->d_phi, sizeof(double) * h->phi_total, cudaMemcpyDeviceToHost, h->stream));
@@ -560,6 +583,7 @@ int bafqmc_get_state(bafqmc_handle* h, int32_t* seeds, double* phi) {
 }
 
 int bafqmc_warmup_prior(bafqmc_handle* h, int nwarm) {
+    NvtxRange nvtx_("bafqmc_warmup_prior");
     if (!h || nwarm < 0) return fail(BAFQMC_EARG, "bad warm-up arguments");
     if (!h->have_fields) return fail(BAFQMC_ESTATE, "fields not initialised");
     if (nwarm == 0) return BAFQMC_OK;
@@ -570,6 +594,7 @@ int bafqmc_warmup_prior(bafqmc_handle* h, int nwarm) {
 }
 
 int bafqmc_pre(bafqmc_handle* h) {
+    NvtxRange nvtx_("bafqmc_pre");
     if (!h) return fail(BAFQMC_EARG, "null handle");
     if (!h->have_fields) return fail(BAFQMC_ESTATE, "fields not initialised");
     CK(cudaSetDevice(h->device));
@@ -594,6 +619,7 @@ cudaError_t record_bin(bafqmc_handle* h, int nsweep) {
 }  // namespace
 
 int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
+    NvtxRange nvtx_("bafqmc_sweep");
     if (!h || nsweep < 1) return fail(BAFQMC_EARG, "bad sweep arguments");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     CK(cudaSetDevice(h->device));
@@ -626,6 +652,7 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
 }
 
 int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs) {
+    NvtxRange nvtx_("bafqmc_bin_chain_obs");
     if (!h || !chain_obs) return fail(BAFQMC_EARG, "null argument");
     if (!h->bin_done) return fail(BAFQMC_ESTATE, "no bin has been measured");
     CK(cudaSetDevice(h->device));
@@ -636,6 +663,7 @@ int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs) {
 }
 
 int bafqmc_bin_point_obs(bafqmc_handle* h, double* point_obs) {
+    NvtxRange nvtx_("bafqmc_bin_point_obs");
     if (!h || !point_obs) return fail(BAFQMC_EARG, "null argument");
     if (!h->bin_done) return fail(BAFQMC_ESTATE, "no bin has been measured");
     CK(cudaSetDevice(h->device));
@@ -671,6 +699,7 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out) {
 }
 
 int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars) {
+    NvtxRange nvtx_("bafqmc_pole_diagnostics");
     if (!h || !scalars) return fail(BAFQMC_EARG, "null argument");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     int nmax = 0;
@@ -707,7 +736,7 @@ int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* sc
     int bad = -1;
     for (int c = 0; c < h->nchains; ++c) {
         const PointHost& p = h->pts[h->chain_point[c]];
-        if (p.pairing) continue;
+        if (p.pairing || (sc[c].status & 1)) continue;   // NaN rows for quarantined chains
         const double* s = hs.data() + (size_t)c * bq::kPoleScalars;
         double* o = scalars + (size_t)c * BAFQMC_POLE_SCALARS;
         for (int k = 0; k < 4; ++k) o[k] = s[k];

@@ -40,6 +40,7 @@ cudaError_t launch_bin_finish(const KernelArgs& ka, cudaStream_t st);
 cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* start, const int* list, double* out,
                                  cudaStream_t st);
 cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st);
+cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st);   // bad[chain]: non-finite field
 
 // pole diagnostics of the number-conserving chains' G: per chain kPoleScalars
 // doubles (pole_distance, pole_x, spectral radius, largest singular value,

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(32) pole_kernel(KernelArgs ka, int zstride, do
     if (chain >= ka.nchains) return;
     const ChainDev cd = ka.chains[chain];
     const PointDev* P = ka.pts + cd.point;
-    if (P->pairing) return;
+    if (P->pairing || (ka.sc[chain].status & 1)) return;   // no pole files for Nambu chains; quarantined chains
     const int n = P->N, ld = n | 1, lane = threadIdx.x;
     cplx* v = reinterpret_cast<cplx*>(pole_smem);
     cplx* ev = v + n;

@@ -1378,6 +1378,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
     const int chain = idx[blockIdx.x];
     Ctx<NMAX> x;
     if (!setup_ctx(x, ka, chain)) return;
+    if (x.sc->status & 1) return;   // quarantined: non-finite G, skipped until its state is set again
     tc_begin(x, ka);
     auto& s = x.s;
     const int n = x.n, L = x.P().L;
@@ -1517,6 +1518,16 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) pre_kerne
     }
     sstore(n, LD, x.A().URc, x.U());
     sstore(n, LD, x.A().G, x.G());
+    // a chain whose G(beta) is not finite (overflowing fields) is quarantined
+    {
+        double v[1] = {0.0};
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const cplx g = x.A().G[e];
+            if (!isfinite(g.x) || !isfinite(g.y)) v[0] += 1.0;
+        }
+        block_sum<1>(v, x.s.red());
+        if (threadIdx.x == 0 && v[0] > 0.0) x.sc->status |= 1;
+    }
     tc_end(x, ka);
 }
 
@@ -1610,16 +1621,37 @@ __global__ void bin_finish_kernel(KernelArgs ka) {
 }
 
 // Chain average per point (m_process_obs_equal, fourier_trans.f90:350-457):
-// out[p][k] = sum over chains of point p of obs[chain][k] / (chains of p).
+// out[p][k] = sum over the chains of point p of obs[chain][k] / (chains of p),
+// over the chains that are not quarantined (NaN if none is left).
 __global__ void point_average_kernel(KernelArgs ka, const int* point_chain_start, const int* point_chain_list,
                                      double* out) {
     const int p = blockIdx.x;
     const int b = point_chain_start[p], e = point_chain_start[p + 1];
     for (int k = threadIdx.x; k < ka.obs_stride; k += blockDim.x) {
         double s = 0.0;
-        for (int c = b; c < e; ++c) s += ka.obs[(long)point_chain_list[c] * ka.obs_stride + k];
-        out[(long)p * ka.obs_stride + k] = (e > b) ? s / (double)(e - b) : 0.0;
+        int m = 0;
+        for (int c = b; c < e; ++c) {
+            const int ch = point_chain_list[c];
+            if (ka.sc[ch].status & 1) continue;   // quarantined chains leave the average
+            s += ka.obs[(long)ch * ka.obs_stride + k];
+            ++m;
+        }
+        out[(long)p * ka.obs_stride + k] = m > 0 ? s / (double)m : __longlong_as_double(0x7ff8000000000000LL);
     }
+}
+
+// bad[chain] = 1 if any field value of the chain is NaN or infinite
+__global__ void field_check_kernel(KernelArgs ka, int* bad) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    const ChainDev cd = ka.chains[chain];
+    const PointDev& P = ka.pts[cd.point];
+    const double* phi = ka.phi + cd.phi_off;
+    const long long tot = (long long)P.L * P.Ns * 2;
+    int any = 0;
+    for (long long k = threadIdx.x; k < tot; k += blockDim.x) any |= !isfinite(phi[k]);
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) bad[chain] = any;
 }
 
 // -0.5 * sum(phi^2) per chain (AuxConf_log_weight, fields.f90:29-33)
@@ -1695,6 +1727,10 @@ cudaError_t launch_bin_finish(const KernelArgs& ka, cudaStream_t st) {
 cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* start, const int* list, double* out,
                                  cudaStream_t st) {
     point_average_kernel<<<npts, 64, 0, st>>>(ka, start, list, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st) {
+    field_check_kernel<<<ka.nchains, 256, 0, st>>>(ka, bad);
     return cudaGetLastError();
 }
 cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st) {

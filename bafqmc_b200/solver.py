@@ -11,6 +11,7 @@ appends the same per-bin files, info.txt and confout.txt.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
 import time
 from pathlib import Path
@@ -170,6 +171,12 @@ class Ensemble:
         on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision)."""
         _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
 
+    def quarantined(self) -> list[int]:
+        """Chains whose Green's function became non-finite (status bit 0): later
+        sweeps skip them and the point averages leave them out."""
+        st = self.counters()[:, 6].astype(np.int64)
+        return [int(c) for c in np.nonzero(st & 1)[0]]
+
     POLE_NAMES = ("pole_distance", "pole_x", "green_spectral_radius", "green_smax", "log_weight")
 
     def pole_diagnostics(self) -> list[dict | None]:
@@ -233,6 +240,9 @@ def _lst(*vals) -> str:
 
 
 def _es(v: float, width: int = 24, digits: int = 16, expdigits: int = 2) -> str:
+    """Fortran ESw.dEe; a non-finite value is written as gfortran does (NaN, Infinity)."""
+    if not math.isfinite(v):
+        return ("NaN" if v != v else ("-Infinity" if v < 0 else "Infinity")).rjust(width)
     m, e = f"{v:.{digits}E}".split("E")
     ei = int(e)
     s = f"{m}E{'-' if ei < 0 else '+'}{abs(ei):0{expdigits}d}"
@@ -277,17 +287,38 @@ def append_pole(run_dir: Path, diags: list[dict]) -> None:
                 f.write(_es(d[name], expdigits=3) + "\n")
 
 
+def _fortran_float(tok: str, path, pos: int) -> float:
+    try:
+        return float(tok.replace("D", "E").replace("d", "e"))
+    except ValueError:
+        raise ValueError(f"{path}: value {pos + 1} ({tok!r}) is not a number") from None
+
+
 def read_confin(path: Path, p: SolverParams, nchains: int):
+    """conf_therm_in's confin.txt (fields.f90:64-103): 0, or per chain a seed and
+    LtrotTherm*NlxTherm*NlyTherm*2 field values.  A truncated or corrupt file
+    raises ValueError naming the chain and position (the reference would read
+    past the end or stop)."""
     toks = Path(path).read_text().split()
-    if int(float(toks[0].replace("D", "E"))) == 0:
+    if not toks:
+        raise ValueError(f"{path}: empty")
+    if int(_fortran_float(toks[0], path, 0)) == 0:
         return None
     per = p.LtrotTherm * p.NlxTherm * p.NlyTherm * NAUX
+    need = nchains * (per + 1)
+    if len(toks) < need:
+        raise ValueError(f"{path}: {len(toks)} values, {need} needed for {nchains} chains of {per} fields")
     out, pos = [], 0
-    for _ in range(nchains):
-        seed = int(float(toks[pos])); pos += 1
-        vals = np.array([float(t.replace("D", "E").replace("d", "e")) for t in toks[pos:pos + per]])
+    for c in range(nchains):
+        seed = _fortran_float(toks[pos], path, pos)
+        if seed != int(seed):
+            raise ValueError(f"{path}: seed of chain {c} ({toks[pos]!r}) is not an integer")
+        pos += 1
+        vals = np.array([_fortran_float(t, path, pos + i) for i, t in enumerate(toks[pos:pos + per])])
+        if not np.all(np.isfinite(vals)):
+            raise ValueError(f"{path}: non-finite field value in chain {c}")
         pos += per
-        out.append((seed, conf_transfer(p, vals)))
+        out.append((int(seed), conf_transfer(p, vals)))
     return out
 
 
@@ -341,8 +372,13 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     else:
         info.write(" Skipping Bosonic warm-up\n")
     ens.pre()
+    seen = set()
     for nbc in range(p.Nbin):
         ens.sweep(p.Nsweep)
+        for c in ens.quarantined():
+            if c not in seen:   # the reference has no counterpart: it would carry the NaN on
+                seen.add(c)
+                log(f" WARNING: chain {c} quarantined after bin {nbc + 1}: non-finite Green's function")
         append_bin(run_dir, ens.point_obs()[0], pairing=pairing)
         if pole and not pairing:
             append_pole(run_dir, ens.pole_diagnostics())
@@ -359,13 +395,24 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
                 if nprop > 0:
                     w(f"Phase_{name}_branch_pi_fraction", 0.0)
                 w(f"Phase_{name}_local_proposals", nprop)
-    if np.any(cnt[:, 6] != 0):
-        info.write(" non-finite Green's function detected in chains: "
-                   + " ".join(str(i) for i in np.nonzero(cnt[:, 6])[0]) + "\n")
+    quarantined = ens.quarantined()
+    if quarantined:
+        info.write(" non-finite Green's function, chains quarantined: "
+                   + " ".join(str(i) for i in quarantined) + "\n")
     w("Max diff Matrix", float(cnt[:, 4].max()))
     w("Mean diff Matrix", float(cnt[:, 5].sum() / (2 * nchains * p.Nbin * p.Nst * p.Nsweep)))
-    w("Tot CPU time", time.time() - t0)
+    elapsed = time.time() - t0
+    w("Tot CPU time", elapsed)
     info.close()
+    record = {   # machine-readable summary of the run (no counterpart in the reference)
+        "program": "pairing" if pairing else "number_conserving", "chains": nchains, "bins": p.Nbin,
+        "sweeps_per_bin": p.Nsweep, "Ndim": p.Ndim, "Ltrot": p.Ltrot, "wall_s": elapsed,
+        "chain_sweeps_per_s": nchains * p.Nbin * p.Nsweep / elapsed,
+        "acceptance": [float(cnt[:, ch].sum() / (nchains * p.Nbin)) for ch in (0, 1)],
+        "drift_max": float(cnt[:, 4].max()), "quarantined_chains": quarantined,
+        "status": [int(v) for v in cnt[:, 6]],
+    }
+    (run_dir / "run_record.json").write_text(json.dumps(record, indent=1) + "\n")
     seeds, phis = ens.get_state()
     with open(run_dir / "confout.txt", "w") as f:   # conf_out (fields.f90:236-278)
         for c in range(nchains):

@@ -81,7 +81,9 @@ int bafqmc_fields_from_seeds(bafqmc_handle* h, const int32_t* seeds);
 
 /* confin path of conf_therm_in (fields.f90:81-103): explicit seed and field
  * (already of the full Ltrot x Ns size) per chain.  get_state is conf_out's
- * payload (fields.f90:236-278). */
+ * payload (fields.f90:236-278).  Setting a state clears every chain's counters
+ * and status; a NaN or infinite field value returns BAFQMC_EARG naming the
+ * chain (and leaves the handle without fields). */
 int bafqmc_set_state(bafqmc_handle* h, const int32_t* seeds, const double* phi);
 int bafqmc_get_state(bafqmc_handle* h, int32_t* seeds, double* phi);
 
@@ -132,15 +134,19 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out);
  *   scalars  [nchains][BAFQMC_POLE_SCALARS]: pole_distance, pole_x,
  *            green_spectral_radius, green_smax, log_weight (the five
  *            one-column files).
- * Nambu chains (the pairing program writes no pole files) get NaN.  Returns
+ * Nambu chains (the pairing program writes no pole files) and quarantined
+ * chains (status bit 0, see bafqmc_counters) get NaN.  Returns
  * BAFQMC_ENUMERIC if a chain's eigenvalue iteration did not converge (the
  * reference stops on ZGEEV info != 0, pole_diagnostics.f90:41-46). */
 #define BAFQMC_POLE_SCALARS 5
 int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars);
 
 /* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
- * status (bit 0: non-finite drift; bit 2: a tensor-core product did not
- * complete within its wait bound and the chain continued in FP64), seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
+ * status (bit 0: the chain's Green's function became non-finite, at a
+ * stabilisation or in bafqmc_pre: the chain is quarantined, i.e. later sweeps
+ * skip it and bafqmc_bin_point_obs averages over the other chains, until its
+ * state is set again; bit 2: a tensor-core product did not complete within
+ * its wait bound and the chain continued in FP64), seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
  * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and
  * %count_accepted over all bins, src/pairing/src/operator_Hubbard.f90:269-284.
  * The Nambu weight ratio is real and positive here, so PhaseCounter's phase
