@@ -16,6 +16,7 @@ ERRORS = {-1: "BAFQMC_EARG", -2: "BAFQMC_ECUDA", -3: "BAFQMC_EUNSUPPORTED", -4: 
 OBS_SCALARS = 32
 COUNTERS = 14
 POLE_SCALARS = 5
+NUM_CLASSES = 7
 PRECISION = {"fp64": 0, "mixed": 1}
 
 
@@ -42,6 +43,8 @@ _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int32)
 SIGNATURES = {
     "bafqmc_create": (C.c_int, [C.POINTER(Point), C.c_int, _IP, C.c_int, C.c_int, C.POINTER(_P)]),
+    "bafqmc_create_tuned": (C.c_int, [C.POINTER(Point), C.c_int, _IP, C.c_int, C.c_int, _IP, C.POINTER(_P)]),
+    "bafqmc_autotune": (C.c_int, [C.POINTER(Point), C.c_int, C.c_int, C.c_int, _IP, _DP]),
     "bafqmc_destroy": (None, [_P]),
     "bafqmc_last_error": (C.c_char_p, []),
     "bafqmc_point_dim": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),

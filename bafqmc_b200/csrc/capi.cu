@@ -168,6 +168,7 @@ struct PointHost {
     double alpha_re[2], alpha_im[2];
     int active[2];
     int flip[2];
+    int cls = -1;   // kernel class of the point's chains (default: the smallest that holds N)
 };
 
 double ranf(int32_t& seed) {   // src/common/random.f90:1-11
@@ -298,7 +299,14 @@ int setup_point(const bafqmc_point& p, PointHost& out) {
     return BAFQMC_OK;
 }
 
-int point_class(const PointHost& ph) { return bq::class_of(ph.N, ph.pairing); }
+int point_class(const PointHost& ph) { return ph.cls >= 0 ? ph.cls : bq::class_of(ph.N, ph.pairing); }
+
+// Whether kernel class cls can run a point of dimension n and the given sector.
+bool class_holds(int cls, int n, int pairing) {
+    if (cls < 0 || cls >= bq::kNumClasses || n > bq::class_nmax(cls)) return false;
+    const int cls_pair = (cls >= 3 && cls < 6) ? 1 : 0;
+    return cls_pair == pairing;
+}
 
 // Device descriptor of a point whose expP | expM | phase table start at mats.
 PointDev point_dev(const PointHost& ph, const double2* mats) {
@@ -355,6 +363,11 @@ const char* bafqmc_last_error(void) { return g_err.c_str(); }
 
 int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
                   bafqmc_handle** out) {
+    return bafqmc_create_tuned(pts, npts, chain_point, nchains, device, nullptr, out);
+}
+
+int bafqmc_create_tuned(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
+                        const int* classes, bafqmc_handle** out) {
     NvtxRange nvtx_("bafqmc_create");
     if (!out || !pts || npts < 1 || nchains < 1 || !chain_point) return fail(BAFQMC_EARG, "bad create arguments");
     *out = nullptr;
@@ -369,6 +382,14 @@ int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point,
         if (rc != BAFQMC_OK) {
             delete h;
             return rc;
+        }
+        if (classes && classes[i] >= 0) {
+            if (!class_holds(classes[i], h->pts[i].N, h->pts[i].pairing)) {
+                delete h;
+                return fail(BAFQMC_EARG, "kernel class " + std::to_string(classes[i]) + " cannot run point " +
+                                             std::to_string(i));
+            }
+            h->pts[i].cls = classes[i];
         }
         maxlq = std::max(maxlq, h->pts[i].Lq);
     }
@@ -773,6 +794,71 @@ int bafqmc_counters(bafqmc_handle* h, double* out) {
         o[11] = sc[c].prop_tot[1];
         o[12] = sc[c].acc_tot[0];
         o[13] = sc[c].acc_tot[1];
+    }
+    return BAFQMC_OK;
+}
+
+int bafqmc_autotune(const bafqmc_point* pts, int npts, int device, int trial_chains, int* classes,
+                    double* ms_per_chain_sweep) {
+    NvtxRange nvtx_("bafqmc_autotune");
+    if (!pts || npts < 1 || !classes) return fail(BAFQMC_EARG, "bad autotune arguments");
+    std::vector<PointHost> ph(npts);
+    for (int i = 0; i < npts; ++i) {
+        int rc = setup_point(pts[i], ph[i]);
+        if (rc != BAFQMC_OK) return rc;
+    }
+    CK(cudaSetDevice(device));
+    if (trial_chains <= 0) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        trial_chains = 4 * sms;   // whole waves at one, two and four CTAs per SM
+    }
+    if (ms_per_chain_sweep)
+        for (int k = 0; k < npts * bq::kNumClasses; ++k) ms_per_chain_sweep[k] = std::nan("");
+    // one trial per distinct (Ndim, sector), on the first point that has it
+    std::vector<int> done(npts, 0);
+    for (int i = 0; i < npts; ++i) {
+        if (done[i]) continue;
+        int best = -1;
+        double best_t = 0.0;
+        std::vector<int32_t> cp(trial_chains, 0), seeds(trial_chains);
+        for (int c = 0; c < trial_chains; ++c) seeds[c] = 1000003 + 7919 * c;
+        for (int cls = 0; cls < bq::kNumClasses; ++cls) {
+            if (!class_holds(cls, ph[i].N, ph[i].pairing)) continue;
+            bafqmc_handle* t = nullptr;
+            int rc = bafqmc_create_tuned(&pts[i], 1, cp.data(), trial_chains, device, &cls, &t);
+            if (rc == BAFQMC_OK) rc = bafqmc_fields_from_seeds(t, seeds.data());
+            if (rc == BAFQMC_OK) rc = bafqmc_pre(t);
+            if (rc == BAFQMC_OK) rc = bafqmc_sweep(t, 1);   // warm-up (captures the bin graph)
+            float ms = 0.0f;
+            if (rc == BAFQMC_OK) {
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, t->stream);
+                rc = bafqmc_sweep(t, 1);
+                cudaEventRecord(e1, t->stream);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+            }
+            if (t) bafqmc_destroy(t);
+            if (rc != BAFQMC_OK) return rc;
+            const double per = (double)ms / trial_chains;
+            for (int j = i; j < npts; ++j)
+                if (ph[j].N == ph[i].N && ph[j].pairing == ph[i].pairing && ms_per_chain_sweep)
+                    ms_per_chain_sweep[(size_t)j * bq::kNumClasses + cls] = per;
+            if (best < 0 || per < best_t) {
+                best = cls;
+                best_t = per;
+            }
+        }
+        for (int j = i; j < npts; ++j)
+            if (ph[j].N == ph[i].N && ph[j].pairing == ph[i].pairing) {
+                classes[j] = best;
+                done[j] = 1;
+            }
     }
     return BAFQMC_OK;
 }

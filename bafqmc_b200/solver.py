@@ -42,15 +42,21 @@ def point_struct(p: SolverParams) -> _lib.Point:
 class Ensemble:
     """Independent Markov chains (the reference's MPI ranks) on one GPU."""
 
-    def __init__(self, points: list[SolverParams], chain_point, device: int = 0):
+    def __init__(self, points: list[SolverParams], chain_point, device: int = 0, classes=None):
+        """classes: optional kernel class per point (from autotune), -1 for the default."""
         self.lib = _lib.load()
         self.points = list(points)
         self.chain_point = np.ascontiguousarray(chain_point, dtype=np.int32)
         self.nchains = int(self.chain_point.size)
         arr = (_lib.Point * len(points))(*[point_struct(p) for p in points])
         h = C.c_void_p()
-        _lib.check(self.lib.bafqmc_create(arr, len(points), _iptr(self.chain_point), self.nchains, device,
-                                          C.byref(h)))
+        if classes is None:
+            _lib.check(self.lib.bafqmc_create(arr, len(points), _iptr(self.chain_point), self.nchains, device,
+                                              C.byref(h)))
+        else:
+            cls = np.ascontiguousarray(classes, dtype=np.int32)
+            _lib.check(self.lib.bafqmc_create_tuned(arr, len(points), _iptr(self.chain_point), self.nchains, device,
+                                                    _iptr(cls), C.byref(h)))
         self.h = h
         self.stride = self.lib.bafqmc_obs_stride(h)
         self.dims = []
@@ -209,6 +215,18 @@ class Ensemble:
         out = np.zeros((self.nchains, _lib.COUNTERS))
         _lib.check(self.lib.bafqmc_counters(self.h, _dptr(out)))
         return out
+
+
+def autotune(points: list[SolverParams], trial_chains: int = 0, device: int = 0):
+    """bafqmc_autotune: the fastest kernel class per point, and the measured
+    milliseconds per chain-sweep of every candidate class ([npts, 7], NaN where
+    a class cannot hold the point)."""
+    lib = _lib.load()
+    arr = (_lib.Point * len(points))(*[point_struct(p) for p in points])
+    classes = np.full(len(points), -1, dtype=np.int32)
+    table = np.full((len(points), _lib.NUM_CLASSES), np.nan)
+    _lib.check(lib.bafqmc_autotune(arr, len(points), device, int(trial_chains), _iptr(classes), _dptr(table)))
+    return classes, table
 
 
 def nambu_green(block: np.ndarray) -> np.ndarray:

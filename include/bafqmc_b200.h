@@ -66,6 +66,25 @@ typedef struct bafqmc_handle bafqmc_handle;
 int bafqmc_create(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
                   bafqmc_handle** out);
 void bafqmc_destroy(bafqmc_handle* h);
+
+/* Kernel classes and their autotuner (no counterpart in the reference).  A
+ * kernel class is one tile configuration of the sweep kernels: threads per
+ * CTA, CTAs per SM, GEMM micro-tile, register layout of the factorisations and
+ * where the workspaces live.  Classes 0-2 hold Ndim <= 16 / 36 / 72
+ * (number-conserving), 3-5 the same sizes for Nambu points, 6 number-
+ * conserving Ndim <= 144.  bafqmc_create gives every point the smallest class
+ * that holds it.  bafqmc_autotune times one sweep of trial_chains chains (0:
+ * four per SM) of each distinct (Ndim, sector) among pts in every class that
+ * can hold it, on scratch handles (nothing of a later run is touched), and
+ * writes the fastest class per point to classes[npts]; ms_per_chain_sweep
+ * (optional, [npts][7]) receives the measured time per chain-sweep of each
+ * candidate (NaN where a class does not apply).  bafqmc_create_tuned takes
+ * such a table (or -1 per point for the default). */
+#define BAFQMC_NUM_CLASSES 7
+int bafqmc_autotune(const bafqmc_point* pts, int npts, int device, int trial_chains, int* classes,
+                    double* ms_per_chain_sweep);
+int bafqmc_create_tuned(const bafqmc_point* pts, int npts, const int32_t* chain_point, int nchains, int device,
+                        const int* classes, bafqmc_handle** out);
 const char* bafqmc_last_error(void);
 
 /* Sizes: dimension of a point's stored Green's function (Lx*Ly, or 2*Lx*Ly
