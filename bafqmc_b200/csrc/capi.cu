@@ -2,6 +2,7 @@
 // up (lattice tables, kinetic propagators, HS factors, initial fields) and the
 // device state of a batch of chains of the number-conserving and Nambu
 // pairing solvers.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -411,6 +412,17 @@ int bafqmc_create_tuned(const bafqmc_point* pts, int npts, const int32_t* chain_
         h->phi_total += (long long)ph.p.Ltrot * ph.Lq * 2;
         h->cls_list[point_class(ph)].push_back(c);
         per_point[p].push_back(c);
+    }
+    // Within a class launch, CTAs start in list order: longest chains first
+    // (cost ~ Ltrot * N^3 * active channels), so that a ragged batch does not end
+    // on a tail of long chains started last.  Results do not depend on the order.
+    for (int k = 0; k < bq::kNumClasses; ++k) {
+        auto cost = [&](int c) {
+            const PointHost& q = h->pts[h->chain_point[c]];
+            return (double)q.p.Ltrot * q.N * q.N * q.N * (q.active[0] + q.active[1]);
+        };
+        std::stable_sort(h->cls_list[k].begin(), h->cls_list[k].end(),
+                         [&](int a, int b) { return cost(a) > cost(b); });
     }
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {

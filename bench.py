@@ -207,6 +207,70 @@ def run_reference(args, rank: int, world: int):
 
 
 # ---------------------------------------------------------------------------
+def run_ragged(args):
+    """The ragged batch: 216 parameter points (3x3, 4x4, 6x6; beta 2, 4, 8;
+    number-conserving and Nambu) x 32 chains in one handle, kernel classes from
+    the autotuner, one persistent launch per class and sweep; against the same
+    points run one handle at a time (the sequential plain path)."""
+    import torch
+    from bafqmc_b200.solver import Ensemble, autotune
+    from bafqmc_b200.workloads import ragged_grid
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    pts = ragged_grid()
+    per = 32
+    classes, _ = autotune(pts)
+    chain_point = np.repeat(np.arange(len(pts)), per).astype(np.int32)
+    seeds = 4242 + 7919 * np.arange(chain_point.size)
+    ens = Ensemble(pts, chain_point, classes=classes)
+    ens.fields_from_seeds(seeds)
+    ens.pre()
+    for _ in range(max(args.warmup, 3)):
+        ens.sweep(1)
+    ens.synchronize()
+    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ens.sweep(1)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ragged_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    ens.close()
+    # the same chains, one point per handle, each timed alone
+    seq_s = 0.0
+    for k, p in enumerate(pts):
+        with Ensemble([p], np.zeros(per, dtype=np.int32), classes=[int(classes[k])]) as one:
+            one.fields_from_seeds(seeds[k * per:(k + 1) * per])
+            one.pre()
+            one.sweep(1)
+            one.synchronize()
+            st = torch.cuda.ExternalStream(one.stream, device=dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            one.sweep(1)
+            b.record(st)
+            b.synchronize()
+            seq_s += a.elapsed_time(b) / 1e3
+    n = int(chain_point.size)
+    print(json.dumps({
+        "metric": "chain-sweeps/s per B200, ragged batch (216 points x 32 chains, FP64)", "value": n / ragged_s,
+        "unit": "chain-sweeps/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": 1e3 * ragged_s, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded N(0,1) HS fields)",
+        "config": {"workload": "ragged grid: Lx=Ly in {3,4,6}, beta in {2,4,8}, U2 in {0,-0.5}, mu in {-6,-5,-4}, "
+                               "number-conserving and Nambu Delta in {0.25,0.5,1}", "points": len(pts),
+                   "chains_per_point": per, "chains": n,
+                   "classes": {str(c): int(np.sum(classes == c)) for c in np.unique(classes)},
+                   "sequential_ms_per_sweep": 1e3 * seq_s, "sequential_chain_sweeps_per_s": n / seq_s,
+                   "speedup_vs_sequential": seq_s / ragged_s},
+        "clocks": clk,
+    }), flush=True)
+
+
 def run_12x12(args):
     """12x12 (N = 144), U1 = 1, U2 = -0.5, mu = -5, beta = 10, dtau = 0.05 (L = 200),
     Nwrap = 10, 512 chains: the size class whose matrices live in HBM.  One
@@ -283,11 +347,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="12x12 workload: FP64 slice products, or 3xTF32 on the tensor cores")
-    ap.add_argument("--workload", choices=["6x6", "12x12"], default="6x6",
-                    help="6x6: the headline line; 12x12: the beta=10 point (512 chains, device time only)")
+    ap.add_argument("--workload", choices=["6x6", "12x12", "ragged"], default="6x6",
+                    help="6x6: the headline line; 12x12: the beta=10 point (512 chains, device time only); "
+                         "ragged: 216 points x 32 chains in one launch per kernel class")
     args = ap.parse_args()
     if args.workload == "12x12":
         run_12x12(args)
+        return
+    if args.workload == "ragged":
+        run_ragged(args)
         return
 
     rank = int(os.environ.get("RANK", "0"))

@@ -9,28 +9,12 @@ points, two chains each, shares one handle; each point then runs in a handle
 of its own from the same seeds.  Every chain's CTA does the same work whatever
 else is in the launch, so fields, seeds and bin records agree bit for bit.
 """
-import itertools
-
 import numpy as np
 import pytest
 
-from bafqmc_b200.params import SolverParams
+from bafqmc_b200.workloads import ragged_grid
 
 pytestmark = pytest.mark.gpu
-
-
-def ragged_grid():
-    pts = []
-    for lx, beta, u2, mu, delta in itertools.product((3, 4, 6), (2.0, 4.0, 8.0), (0.0, -0.5), (-6.0, -5.0, -4.0),
-                                                     (None, 0.25, 0.5, 1.0)):
-        L = int(round(beta / 0.05))
-        kw = dict(U1=1.0, U2=u2, mu=mu, Nlx=lx, Nly=lx, Ltrot=L, Beta=beta, NlxTherm=lx, NlyTherm=lx, LtrotTherm=L,
-                  Nwrap=10, Nbin=1, Nsweep=1, iniType=2, iniAmpl=1.0)
-        if delta is None:
-            pts.append(SolverParams(**kw, shiftLoc=1.5))
-        else:
-            pts.append(SolverParams(**kw, shiftLoc=1.0, delta=delta, sector=1))
-    return pts
 
 
 def test_grid_has_216_points_in_three_size_classes():
