@@ -63,6 +63,8 @@ SIGNATURES = {
     "bafqmc_log_weight": (C.c_int, [_P, _DP]),
     "bafqmc_pole_diagnostics": (C.c_int, [_P, _DP, C.c_int, _DP]),
     "bafqmc_set_precision": (C.c_int, [_P, C.c_int]),
+    "bafqmc_stats_reset": (C.c_int, [_P, C.c_int, C.c_int]),
+    "bafqmc_stats": (C.c_int, [_P, _DP, _DP, _IP]),
     "bafqmc_counters": (C.c_int, [_P, _DP]),
     "bafqmc_phase_timers": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_synchronize": (C.c_int, [_P]),

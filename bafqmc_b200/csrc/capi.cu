@@ -214,6 +214,9 @@ struct bafqmc_handle {
     int mixed = 0;   // bafqmc_set_precision
     // the launches of one bin (reset, nsweep sweeps of every class, finish),
     // captured once per (nsweep, timers) and replayed as one graph launch
+    // on-device block statistics of the per-bin point averages (bafqmc_stats_reset)
+    int stats_block = 0, stats_max = 0, stats_in_block = 0, stats_blocks = 0;
+    double* d_stats = nullptr;   // [npts*stride] x (current block sum, mean, sem, then stats_max block means)
     cudaGraphExec_t bin_graph = nullptr;
     int graph_nsweep = 0, graph_timers = 0, graph_mixed = 0;
 
@@ -346,7 +349,7 @@ void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
-                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat};
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat, h->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
@@ -681,6 +684,49 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
     }
     CK(cudaGraphLaunch(h->bin_graph, h->stream));
     h->bin_done = true;
+    if (h->stats_block > 0 && h->stats_blocks < h->stats_max) {
+        const int n = h->npts * h->obs_stride;
+        const bool finish = h->stats_in_block + 1 == h->stats_block;
+        CK(bq::launch_point_average(h->args(), h->npts, h->d_pstart, h->d_plist, h->d_pout, h->stream));
+        CK(bq::launch_stats_add(h->d_pout, h->d_stats, h->d_stats + (size_t)(3 + h->stats_blocks) * n, n,
+                                finish ? 1 : 0, h->stats_block, h->stream));
+        h->stats_in_block = finish ? 0 : h->stats_in_block + 1;
+        if (finish) ++h->stats_blocks;
+    }
+    return BAFQMC_OK;
+}
+
+int bafqmc_stats_reset(bafqmc_handle* h, int block_size, int max_blocks) {
+    if (!h || block_size < 1 || max_blocks < 2) return fail(BAFQMC_EARG, "block_size >= 1 and max_blocks >= 2");
+    CK(cudaSetDevice(h->device));
+    const size_t n = (size_t)h->npts * h->obs_stride;
+    if (h->d_stats && max_blocks > h->stats_max) {
+        CK(cudaFree(h->d_stats));
+        h->d_stats = nullptr;
+    }
+    if (!h->d_stats) {
+        CK(cudaMalloc(&h->d_stats, sizeof(double) * n * (3 + (size_t)max_blocks)));
+        h->stats_max = max_blocks;
+    }
+    CK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * n, h->stream));
+    h->stats_block = block_size;
+    h->stats_in_block = 0;
+    h->stats_blocks = 0;
+    return BAFQMC_OK;
+}
+
+int bafqmc_stats(bafqmc_handle* h, double* mean, double* sem, int* nblocks) {
+    if (!h || !mean || !sem) return fail(BAFQMC_EARG, "null argument");
+    if (h->stats_block < 1) return fail(BAFQMC_ESTATE, "bafqmc_stats_reset has not run");
+    if (nblocks) *nblocks = h->stats_blocks;
+    CK(cudaSetDevice(h->device));
+    const size_t n = (size_t)h->npts * h->obs_stride;
+    double* d_mean = h->d_stats + n;
+    double* d_sem = h->d_stats + 2 * n;
+    CK(bq::launch_stats_final(h->d_stats + 3 * n, h->stats_blocks, (int)n, d_mean, d_sem, h->stream));
+    CK(cudaMemcpyAsync(mean, d_mean, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(sem, d_sem, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return BAFQMC_OK;
 }
 

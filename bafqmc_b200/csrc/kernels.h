@@ -41,6 +41,10 @@ cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* star
                                  cudaStream_t st);
 cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st);
 cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st);   // bad[chain]: non-finite field
+// block statistics over n = npts * obs_stride values: accumulate one bin, finish blocks, final mean / sem
+cudaError_t launch_stats_add(const double* pout, double* cur, double* blk, int n, int finish, int block_size,
+                             cudaStream_t st);
+cudaError_t launch_stats_final(const double* blk, int nb, int n, double* mean, double* sem, cudaStream_t st);
 
 // pole diagnostics of the number-conserving chains' G: per chain kPoleScalars
 // doubles (pole_distance, pole_x, spectral radius, largest singular value,

@@ -1640,6 +1640,36 @@ __global__ void point_average_kernel(KernelArgs ka, const int* point_chain_start
     }
 }
 
+// Block statistics of the per-bin point averages: cur += pout (bins summed in
+// order); when a block completes, blk = cur / block_size and cur restarts.
+__global__ void stats_add_kernel(const double* pout, double* cur, double* blk, int n, int finish, int block_size) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double v = cur[k] + pout[k];
+        if (finish) {
+            blk[k] = v / (double)block_size;
+            cur[k] = 0.0;
+        } else {
+            cur[k] = v;
+        }
+    }
+}
+// mean and standard error over nb block means, each element summed over the
+// blocks in order: mean = sum / nb, sem = sqrt(sum (m - mean)^2 / (nb - 1) / nb)
+__global__ void stats_final_kernel(const double* blk, int nb, int n, double* mean, double* sem) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += blk[(long)b * n + k];
+        const double m = s / (double)nb;
+        double v = 0.0;
+        for (int b = 0; b < nb; ++b) {   // square rounded, then added (no fused multiply-add)
+            const double d = blk[(long)b * n + k] - m;
+            v = __dadd_rn(v, __dmul_rn(d, d));
+        }
+        mean[k] = m;
+        sem[k] = nb > 1 ? sqrt(v / (double)(nb - 1) / (double)nb) : __longlong_as_double(0x7ff8000000000000LL);
+    }
+}
+
 // bad[chain] = 1 if any field value of the chain is NaN or infinite
 __global__ void field_check_kernel(KernelArgs ka, int* bad) {
     const int chain = blockIdx.x;
@@ -1727,6 +1757,15 @@ cudaError_t launch_bin_finish(const KernelArgs& ka, cudaStream_t st) {
 cudaError_t launch_point_average(const KernelArgs& ka, int npts, const int* start, const int* list, double* out,
                                  cudaStream_t st) {
     point_average_kernel<<<npts, 64, 0, st>>>(ka, start, list, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_stats_add(const double* pout, double* cur, double* blk, int n, int finish, int block_size,
+                             cudaStream_t st) {
+    stats_add_kernel<<<(n + 255) / 256, 256, 0, st>>>(pout, cur, blk, n, finish, block_size);
+    return cudaGetLastError();
+}
+cudaError_t launch_stats_final(const double* blk, int nb, int n, double* mean, double* sem, cudaStream_t st) {
+    stats_final_kernel<<<(n + 255) / 256, 256, 0, st>>>(blk, nb, n, mean, sem);
     return cudaGetLastError();
 }
 cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st) {

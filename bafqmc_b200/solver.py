@@ -177,6 +177,29 @@ class Ensemble:
         on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision)."""
         _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
 
+    def stats_reset(self, block_size: int, max_blocks: int = 1024):
+        """Start on-device block statistics of the per-bin point averages (bafqmc_stats_reset)."""
+        _lib.check(self.lib.bafqmc_stats_reset(self.h, int(block_size), int(max_blocks)))
+
+    def stats_raw(self):
+        """(mean, sem) as [npts, stride] arrays over the completed blocks, and the block count."""
+        mean = np.zeros((len(self.points), self.stride))
+        sem = np.zeros_like(mean)
+        nb = np.zeros(1, dtype=np.int32)
+        _lib.check(self.lib.bafqmc_stats(self.h, _dptr(mean), _dptr(sem), _iptr(nb)))
+        return mean, sem, int(nb[0])
+
+    def stats(self) -> list[dict]:
+        """Per point: {observable: (mean, sem)}; complex observables give complex mean and
+        complex sem (the SEM of the real and of the imaginary part)."""
+        mean, sem, _ = self.stats_raw()
+        out = []
+        for p in range(len(self.points)):
+            pair = self.points[p].sector == 1
+            m, e = decode(mean[p], self.dims[p][1], pair), decode(sem[p], self.dims[p][1], pair)
+            out.append({k: (m[k], e[k]) for k in m})
+        return out
+
     def quarantined(self) -> list[int]:
         """Chains whose Green's function became non-finite (status bit 0): later
         sweeps skip them and the point averages leave them out."""
@@ -340,6 +363,20 @@ def read_confin(path: Path, p: SolverParams, nchains: int):
     return out
 
 
+def read_confin_npz(path: Path, p: SolverParams, nchains: int):
+    """The binary checkpoint confout.npz written by run_directory (seeds
+    [nchains] int32, phi [nchains][Ltrot][Lq][2] float64), read back as
+    read_confin's (seed, fields) list."""
+    with np.load(path) as z:
+        seeds, phi = z["seeds"], z["phi"]
+    if seeds.shape != (nchains,) or phi.shape != (nchains, p.Ltrot, p.Lq, NAUX):
+        raise ValueError(f"{path}: seeds {seeds.shape} and fields {phi.shape} do not match {nchains} chains of "
+                         f"({p.Ltrot}, {p.Lq}, {NAUX})")
+    if not np.all(np.isfinite(phi)):
+        raise ValueError(f"{path}: non-finite field value")
+    return [(int(seeds[c]), phi[c]) for c in range(nchains)]
+
+
 def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print,
                   pairing: bool = False) -> dict:
     """The reference program for `mpirun -np nchains` in run_dir, on one GPU.
@@ -373,7 +410,10 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     w("Beta", p.Beta); w("Trotter number", p.Ltrot); w("=>Dtau", p.Dtau); w("N_Ortho", p.Nwrap)
     w("# Bins", p.Nbin); w("# Nsweep in one bin", p.Nsweep); w("# Cores", nchains)
     ens = Ensemble([p], np.zeros(nchains, dtype=np.int32), device=device)
-    confin = read_confin(run_dir / "confin.txt", p, nchains)
+    if (run_dir / "confin.npz").exists():   # binary checkpoint, read in place of confin.txt
+        confin = read_confin_npz(run_dir / "confin.npz", p, nchains)
+    else:
+        confin = read_confin(run_dir / "confin.txt", p, nchains)
     if confin is None:
         seeds = [int(r.split()[0]) for r in (run_dir / "seeds.txt").read_text().split("\n") if r.strip()][:nchains]
         if len(seeds) < nchains:
@@ -432,6 +472,9 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     }
     (run_dir / "run_record.json").write_text(json.dumps(record, indent=1) + "\n")
     seeds, phis = ens.get_state()
+    # binary checkpoint beside confout.txt: the same seeds and fields, exact and compact
+    np.savez(run_dir / "confout.npz", seeds=np.asarray(seeds, dtype=np.int32),
+             phi=np.stack([np.asarray(x, dtype=np.float64).reshape(p.Ltrot, p.Lq, NAUX) for x in phis]))
     with open(run_dir / "confout.txt", "w") as f:   # conf_out (fields.f90:236-278)
         for c in range(nchains):
             f.write(f" {int(seeds[c])}\n")

@@ -128,6 +128,18 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep);
 int bafqmc_bin_chain_obs(bafqmc_handle* h, double* chain_obs);
 int bafqmc_bin_point_obs(bafqmc_handle* h, double* point_obs);
 
+/* On-device block statistics of the per-bin chain averages.  The reference's
+ * solver has none; its analysis scripts block the appended per-bin files
+ * (benchmarks/paper/analysis.py:52-64).  After bafqmc_stats_reset, every bin's
+ * point averages (the values bafqmc_bin_point_obs returns) are summed in bin
+ * order into blocks of block_size bins, up to max_blocks blocks.  bafqmc_stats
+ * writes, per point and slot ([npts][stride]), the mean of the completed block
+ * means and its standard error sqrt(sum_b (m_b - mean)^2 / (nb - 1) / nb), each
+ * sum taken in order as the analysis script does; nblocks receives nb.  Bins
+ * of an unfinished block are not counted. */
+int bafqmc_stats_reset(bafqmc_handle* h, int block_size, int max_blocks);
+int bafqmc_stats(bafqmc_handle* h, double* mean, double* sem, int* nblocks);
+
 /* Prop%Gr of one chain (row-major complex, ndim x ndim as bafqmc_point_dim
  * reports).  For a Nambu chain this is the {b, c^dagger} block of the
  * reference's 4Ns Green's function, rows/columns b_1..b_Ns, c^dagger_1..
