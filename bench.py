@@ -140,58 +140,55 @@ def fp64_gemm_peak(dev) -> float:
 
 
 # ---------------------------------------------------------------------------
-# CPU arm: the oracle (CPU restatement of the reference) on the host cores
-def _oracle_chain_sweeps(args):
-    seed, nsweep = args
+# CPU arm: the C++ restatement of the reference's sweep (oracle/csweep.cpp,
+# checked against oracle.py) on the host cores, one chain per thread
+def _cport():
     sys.path.insert(0, str(ROOT))
+    from oracle import cport
+    if not cport.LIB.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
     from oracle import oracle as O
+    return cport, O
+
+
+def cpu_sweep_rate(cores: int, sweeps_per_chain: int, seed0: int = 1000):
+    """chain-sweeps/s of the C++ restatement, `cores` chains on `cores` threads
+    (after each chain's pre); returns (rate, wall seconds)."""
+    cport, O = _cport()
     p = workload()
     op = O.Params(U1=p.U1, U2=p.U2, mu=p.mu, Nlx=p.Nlx, Nly=p.Nly, Ltrot=p.Ltrot, Beta=p.Beta, NlxTherm=p.NlxTherm,
                   NlyTherm=p.NlyTherm, LtrotTherm=p.LtrotTherm, Nwrap=p.Nwrap, Nbin=1, Nsweep=1,
                   shiftLoc=p.shiftLoc, iniType=p.iniType, iniAmpl=p.iniAmpl)
-    _, _, chains = O.init_chains(op, seeds=[seed])
-    c = chains[0]
-    c.pre()
+    _, _, chains = O.init_chains(op, seeds=[seed0 + 17 * i for i in range(cores)])
+    seeds = np.array([c.seed for c in chains], dtype=np.int32)
+    phi = np.ascontiguousarray(np.stack([c.phi for c in chains]))
     t0 = time.perf_counter()
-    for _ in range(nsweep):
-        c.sweep_bin()
-    return time.perf_counter() - t0
-
-
-def cpu_sweep_rate(pool, cores: int, sweeps_per_core: int) -> tuple[float, float]:
-    """chain-sweeps/s of the oracle, one chain per core; returns (rate, wall)."""
-    t0 = time.perf_counter()
-    times = pool.map(_oracle_chain_sweeps, [(1000 + 17 * i, sweeps_per_core) for i in range(cores)])
+    out = cport.run(op, seeds, phi, sweeps_per_chain, nthreads=cores)
     wall = time.perf_counter() - t0
-    return cores * sweeps_per_core / max(times), wall
+    return cores * sweeps_per_chain / out["sweep_seconds"], wall
 
 
-def cpu_baseline(cores: int, sweeps_per_core: int = 2):
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        rate, wall = cpu_sweep_rate(pool, cores, sweeps_per_core)
+def cpu_baseline(cores: int, sweeps_per_chain: int = 4):
+    rate, wall = cpu_sweep_rate(cores, sweeps_per_chain)
     ess, _ = ess_rate(rate)
     return {"value": ess, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{cores} chains x {sweeps_per_core} sweeps of the 6x6 beta=8 workload, one chain per core "
-                      f"(oracle/oracle.py, NumPy + LAPACK), after pre; {rate:.3f} chain-sweeps/s"}
+            "sample": f"{cores} chains x {sweeps_per_chain} sweeps of the 6x6 beta=8 workload, one chain per thread "
+                      f"(oracle/csweep.cpp, the C++ restatement of the reference's sweep checked against "
+                      f"oracle.py), after pre; {rate:.2f} chain-sweeps/s"}
 
 
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    per = 1
-    with ctx.Pool(cores) as pool:
-        for _ in range(args.warmup):
-            cpu_sweep_rate(pool, cores, per)
-        rates, walls = [], []
-        for _ in range(args.steps):
-            r, w = cpu_sweep_rate(pool, cores, per)
-            rates.append(r)
-            walls.append(w)
+    per = 2
+    for k in range(args.warmup):
+        cpu_sweep_rate(cores, 1, seed0=500 + k)
+    rates, walls = [], []
+    for k in range(args.steps):
+        r, w = cpu_sweep_rate(cores, per, seed0=1000 + 100 * k)
+        rates.append(r)
+        walls.append(w)
     rate = float(np.mean(rates))
     ess, tau = ess_rate(rate)
     line = {"impl": "reference", "metric": METRIC, "value": ess, "unit": UNIT, "n_gpus": args.gpus,
@@ -199,9 +196,10 @@ def run_reference(args, rank: int, world: int):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded N(0,1) HS fields)",
             "config": {"workload": "6x6 beta=8 batched plain FP64 sweep", "sample_per_step":
-                       f"{cores} chains x {per} sweep on {cores} host cores", "chain_sweeps_per_s": rate, **tau},
+                       f"{cores} chains x {per} sweeps on {cores} host threads", "chain_sweeps_per_s": rate, **tau},
             "cpu_baseline": {"value": ess, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{cores} chains x {per} sweep per step, oracle/oracle.py"},
+                             "sample": f"{cores} chains x {per} sweeps per step, oracle/csweep.cpp (C++ "
+                                       f"restatement of the reference's sweep), one chain per thread"},
             "e2e": {"value": ess, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -365,7 +363,7 @@ def main():
         run_reference(args, rank, world)
         return
 
-    # the CPU pool is spawned before any CUDA call
+    # the CPU baseline runs before any CUDA call
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_cores or (os.cpu_count() or 1))
