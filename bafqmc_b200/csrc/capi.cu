@@ -214,6 +214,13 @@ struct bafqmc_handle {
     int mixed = 0;   // bafqmc_set_precision
     // the launches of one bin (reset, nsweep sweeps of every class, finish),
     // captured once per (nsweep, timers) and replayed as one graph launch
+    // proposal state of the global moves (bafqmc_global_shift): arena, fields,
+    // chain scalars and field norms, allocated on first use
+    double2* d_arena2 = nullptr;
+    double* d_phi2 = nullptr;
+    ChainScalars* d_sc2 = nullptr;
+    double* d_fn2 = nullptr;
+    int* d_acc = nullptr;
     // on-device block statistics of the per-bin point averages (bafqmc_stats_reset)
     int stats_block = 0, stats_max = 0, stats_in_block = 0, stats_blocks = 0;
     double* d_stats = nullptr;   // [npts*stride] x (current block sum, mean, sem, then stats_max block means)
@@ -232,6 +239,14 @@ struct bafqmc_handle {
         ka.sc = d_sc;
         ka.timers = timers;
         ka.mixed = mixed;
+        return ka;
+    }
+    bq::KernelArgs args2() const {   // the proposal state of the global moves
+        bq::KernelArgs ka = args();
+        ka.arena = d_arena2;
+        ka.phi = d_phi2;
+        ka.sc = d_sc2;
+        ka.timers = 0;
         return ka;
     }
 };
@@ -349,7 +364,8 @@ void free_handle(bafqmc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
-                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat, h->d_stats};
+                    h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat, h->d_stats,
+                    h->d_arena2, h->d_phi2, h->d_sc2, h->d_fn2, h->d_acc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
@@ -696,6 +712,33 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
     return BAFQMC_OK;
 }
 
+int bafqmc_global_shift(bafqmc_handle* h, const double* shift, int* accepted) {
+    NvtxRange nvtx_("bafqmc_global_shift");
+    if (!h || !shift) return fail(BAFQMC_EARG, "null argument");
+    if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
+    CK(cudaSetDevice(h->device));
+    if (!h->d_arena2) {
+        CK(cudaMalloc(&h->d_arena2, sizeof(double2) * h->arena_total));
+        CK(cudaMalloc(&h->d_phi2, sizeof(double) * h->phi_total));
+        CK(cudaMalloc(&h->d_sc2, sizeof(ChainScalars) * h->nchains));
+        CK(cudaMemset(h->d_sc2, 0, sizeof(ChainScalars) * h->nchains));
+        CK(cudaMalloc(&h->d_fn2, sizeof(double) * h->nchains));
+        CK(cudaMalloc(&h->d_acc, sizeof(int) * h->nchains));
+    }
+    const bq::KernelArgs ka = h->args(), kp = h->args2();
+    CK(bq::launch_global_propose(ka, kp, shift, h->stream));
+    for (int c = 0; c < bq::kNumClasses; ++c)
+        CK(bq::launch_pre(c, kp, h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
+    CK(bq::launch_field_norm(ka, h->d_tmp, h->stream));
+    CK(bq::launch_field_norm(kp, h->d_fn2, h->stream));
+    CK(bq::launch_global_accept(ka, kp, h->d_tmp, h->d_fn2, h->d_acc, h->stream));
+    if (accepted) {
+        CK(cudaMemcpyAsync(accepted, h->d_acc, sizeof(int) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return BAFQMC_OK;
+}
+
 int bafqmc_stats_reset(bafqmc_handle* h, int block_size, int max_blocks) {
     if (!h || block_size < 1 || max_blocks < 2) return fail(BAFQMC_EARG, "block_size >= 1 and max_blocks >= 2");
     CK(cudaSetDevice(h->device));
@@ -847,7 +890,7 @@ int bafqmc_counters(bafqmc_handle* h, double* out) {
         o[6] = (double)sc[c].status;
         o[7] = (double)sc[c].seed;
         o[8] = (double)sc[c].nobs;
-        o[9] = 0.0;
+        o[9] = sc[c].glb_acc;
         o[10] = sc[c].prop_tot[0];
         o[11] = sc[c].prop_tot[1];
         o[12] = sc[c].acc_tot[0];

@@ -68,6 +68,7 @@ struct ChainScalars {
     long long cyc[4];           // SM cycles per phase: local updates, slice products, measurement, wraps
     double prop_tot[2];         // proposals over all bins (PhaseCounter%count_proposed)
     double acc_tot[2];          // accepted over all bins (PhaseCounter%count_accepted)
+    double glb_prop, glb_acc;   // global moves proposed and accepted (bafqmc_global_shift)
 };
 
 struct ChainDev {

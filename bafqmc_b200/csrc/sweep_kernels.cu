@@ -1670,6 +1670,74 @@ __global__ void stats_final_kernel(const double* blk, int nb, int n, double* mea
     }
 }
 
+// Global shift move: the shift part of Global_flip (global_update.f90:193-208),
+// under this model's weight.  Per chain, two draws of the chain's LCG give a
+// uniform shift X_ns = (u - 1/2) |shift_ns| of every field of auxiliary channel
+// ns; the shifted field goes to the proposal state kp (same layout).
+__global__ void global_propose_kernel(KernelArgs ka, KernelArgs kp, double shift0, double shift1) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    const ChainDev cd = ka.chains[chain];
+    const PointDev& P = ka.pts[cd.point];
+    ChainScalars* sc = ka.sc + chain;
+    if (sc->status & 1) return;   // quarantined
+    __shared__ double X[2];
+    if (threadIdx.x == 0) {
+        uint32_t seed = sc->seed;
+        const double amp[2] = {fabs(shift0), fabs(shift1)};
+        for (int ns = 0; ns < 2; ++ns) {
+            seed = lcg_mul(kLcgA, seed);
+            X[ns] = (lcg_u(seed) - 0.5) * amp[ns];
+        }
+        sc->seed = seed;
+        kp.sc[chain].status = 0;
+    }
+    __syncthreads();
+    const long long tot = (long long)P.L * P.Ns * 2;
+    const double* phi = ka.phi + cd.phi_off;
+    double* phi2 = kp.phi + cd.phi_off;
+    for (long long k = threadIdx.x; k < tot; k += blockDim.x) phi2[k] = phi[k] + X[k & 1];
+}
+
+// Exact Metropolis-Hastings decision of a global move (global_update.f90:237-249:
+// accept if w'/w >= u, u the chain's next draw), with log w = -sum phi^2 / 2
+// - 2 log|det(I - B(beta,0))| from the two states' last factorisations at
+// tau = beta.  An accepted chain takes the proposal's fields and UDV arena.
+__global__ void global_accept_kernel(KernelArgs ka, KernelArgs kp, const double* fn, const double* fn2,
+                                     int* accepted) {
+    const int chain = blockIdx.x;
+    if (chain >= ka.nchains) return;
+    const ChainDev cd = ka.chains[chain];
+    const PointDev& P = ka.pts[cd.point];
+    ChainScalars* sc = ka.sc + chain;
+    __shared__ int acc;
+    if (threadIdx.x == 0) {
+        acc = 0;
+        if (!(sc->status & 1)) {
+            const double lw = fn[chain] - 2.0 * sc->logdetM;
+            const double lw2 = fn2[chain] - 2.0 * kp.sc[chain].logdetM;
+            const uint32_t seed = lcg_mul(kLcgA, sc->seed);
+            sc->seed = seed;
+            acc = !(kp.sc[chain].status & 1) && exp(lw2 - lw) >= lcg_u(seed);
+            sc->glb_prop += 1.0;
+            if (acc) {
+                sc->glb_acc += 1.0;
+                sc->logdetM = kp.sc[chain].logdetM;
+            }
+        }
+        if (accepted) accepted[chain] = acc;
+    }
+    __syncthreads();
+    if (!acc) return;
+    const long long na = arena_base(P.N, P.Nst), nphi = (long long)P.L * P.Ns * 2;
+    const double2* a2 = kp.arena + cd.arena_off;
+    double2* a = ka.arena + cd.arena_off;
+    for (long long k = threadIdx.x; k < na; k += blockDim.x) a[k] = a2[k];
+    const double* p2 = kp.phi + cd.phi_off;
+    double* p = ka.phi + cd.phi_off;
+    for (long long k = threadIdx.x; k < nphi; k += blockDim.x) p[k] = p2[k];
+}
+
 // bad[chain] = 1 if any field value of the chain is NaN or infinite
 __global__ void field_check_kernel(KernelArgs ka, int* bad) {
     const int chain = blockIdx.x;
@@ -1766,6 +1834,15 @@ cudaError_t launch_stats_add(const double* pout, double* cur, double* blk, int n
 }
 cudaError_t launch_stats_final(const double* blk, int nb, int n, double* mean, double* sem, cudaStream_t st) {
     stats_final_kernel<<<(n + 255) / 256, 256, 0, st>>>(blk, nb, n, mean, sem);
+    return cudaGetLastError();
+}
+cudaError_t launch_global_propose(const KernelArgs& ka, const KernelArgs& kp, const double* shift, cudaStream_t st) {
+    global_propose_kernel<<<ka.nchains, 256, 0, st>>>(ka, kp, shift[0], shift[1]);
+    return cudaGetLastError();
+}
+cudaError_t launch_global_accept(const KernelArgs& ka, const KernelArgs& kp, const double* fn, const double* fn2,
+                                 int* accepted, cudaStream_t st) {
+    global_accept_kernel<<<ka.nchains, 256, 0, st>>>(ka, kp, fn, fn2, accepted);
     return cudaGetLastError();
 }
 cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st) {

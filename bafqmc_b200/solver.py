@@ -177,6 +177,16 @@ class Ensemble:
         on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision)."""
         _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
 
+    def global_shift(self, shift) -> np.ndarray:
+        """One global shift move per chain (bafqmc_global_shift): every field of
+        channel ns shifted by (u - 1/2)|shift[ns]|, accepted by the exact weight
+        ratio; returns 0/1 per chain."""
+        sh = np.ascontiguousarray(shift, dtype=np.float64)
+        assert sh.size == 2
+        acc = np.zeros(self.nchains, dtype=np.int32)
+        _lib.check(self.lib.bafqmc_global_shift(self.h, _dptr(sh), _iptr(acc)))
+        return acc
+
     def stats_reset(self, block_size: int, max_blocks: int = 1024):
         """Start on-device block statistics of the per-bin point averages (bafqmc_stats_reset)."""
         _lib.check(self.lib.bafqmc_stats_reset(self.h, int(block_size), int(max_blocks)))

@@ -172,12 +172,28 @@ int bafqmc_log_weight(bafqmc_handle* h, double* out);
 #define BAFQMC_POLE_SCALARS 5
 int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* scalars);
 
+/* Global moves.  The reference's global update (global_update.f90, not in its
+ * build) pairs a Wolff cluster flip, built on neighbour couplings of an older
+ * field action, with a uniform shift of each auxiliary channel.  Under this
+ * model's weight w = exp(-sum phi^2 / 2) |det G|^2 (the exponent
+ * bafqmc_log_weight reports) the fields have no neighbour couplings, so the
+ * shift is the move that carries over.  bafqmc_global_shift proposes, per
+ * chain, phi' = phi + X_ns on every field of channel ns, X_ns = (u - 1/2)
+ * |shift[ns]| with u the chain's next two draws (ns = 0, 1), rebuilds G(beta)
+ * and log|det(I - B)| of the proposal from scratch (bafqmc_pre's work, in a
+ * second per-chain state allocated on first use), and accepts with
+ * w'/w >= u' for the chain's third draw u' (global_update.f90:237-249).  An
+ * accepted chain continues from the proposal's fields and UDV factors.
+ * accepted (optional, [nchains]) receives 0 or 1.  Quarantined chains are
+ * skipped.  Requires a built G (bafqmc_pre or a sweep). */
+int bafqmc_global_shift(bafqmc_handle* h, const double* shift, int* accepted);
+
 /* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
  * status (bit 0: the chain's Green's function became non-finite, at a
  * stabilisation or in bafqmc_pre: the chain is quarantined, i.e. later sweeps
  * skip it and bafqmc_bin_point_obs averages over the other chains, until its
  * state is set again; bit 2: a tensor-core product did not complete within
- * its wait bound and the chain continued in FP64), seed, nobs, reserved, proposals[2], accepted[2] (AccCounter,
+ * its wait bound and the chain continued in FP64), seed, nobs, accepted global moves, proposals[2], accepted[2] (AccCounter,
  * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and
  * %count_accepted over all bins, src/pairing/src/operator_Hubbard.f90:269-284.
  * The Nambu weight ratio is real and positive here, so PhaseCounter's phase
