@@ -135,3 +135,21 @@ def test_single_chain_config_against_ed(solver_mod, paper):
                      Nwrap=10, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0)
     got = ensemble_means(solver_mod, p, 64, ntherm=1000, nbins=20, nsweep=500, seed0=5005)
     check(got, case, False, "3x3 U1=1 mu=-5 beta=4 dtau=0.1")
+
+
+@pytest.mark.parametrize("mu,beta,seed0", [(-5.0, 2.0, 8008), (-4.0, 2.0, 9009), (-4.0, 4.0, 10010)])
+def test_ragged_grid_points_against_own_ed(solver_mod, mu, beta, seed0):
+    """3x3 points of the ragged grid (U1 = 1, U2 = 0, dtau = 0.05, Nwrap = 10,
+    shiftLoc 1.5) that the reference's stored ED does not cover, against
+    oracle/ed.py with up to 4 bosons (against 5: 1e-8, 4e-5 and 1e-10 relative
+    at these points, far below the standard errors).  U2 = 0: each boson costs
+    at least 2 above mu, so the truncated grand-canonical sum converges; at
+    U2 < 0 bosons bind on a site and it does not."""
+    from oracle import ed
+    L = int(round(beta / 0.05))
+    p = SolverParams(U1=1.0, U2=0.0, mu=mu, Nlx=3, Nly=3, Ltrot=L, Beta=beta, NlxTherm=3, NlyTherm=3, LtrotTherm=L,
+                     Nwrap=10, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0)
+    ref = ed.observables(3, 3, 1.0, 0.0, mu, beta, n_max_total=4)
+    case = {"observables": {k: {"ed": v, "dqmc": v, "stderr": 0.0} for k, v in ref.items()}}
+    got = ensemble_means(solver_mod, p, 256, ntherm=200, nbins=10, nsweep=100, seed0=seed0)
+    check(got, case, False, f"3x3 U1=1 U2=0 mu={mu} beta={beta}")
