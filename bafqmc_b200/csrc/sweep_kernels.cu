@@ -54,6 +54,7 @@ template <> struct Cfg<72> {
 // nor the register file holds these n x n matrices, so products loop over
 // TR x TC tiles out of place and the factorisations use linalg_big.cuh (one
 // warp per column, RW rows per lane, CPW columns at a time).
+static_assert(kTcPer * 512 >= 144 * kTcKC, "tensor-core staging: elements per thread must cover a chunk");
 template <> struct Cfg<144> {
     static constexpr bool TCORE = true;   // slice products may run on the tensor cores (tc.cuh)
     static constexpr int THREADS = 512, TR = 2, TC = 3, MAXE = 41, KB = 4, R8 = 18, CPS = 3, LD = 145, NB = 160,

@@ -37,6 +37,7 @@ constexpr int kTcCols = 512;   // tensor-memory columns allocated (3 tiles x 144
 constexpr size_t kTcABytes = sizeof(uint32_t) * kTcMT * kTcKC;   // one of A hi / A lo
 constexpr size_t kTcBBytes = sizeof(uint32_t) * kTcNB * kTcKC;   // one of B hi / B lo
 constexpr int kTcSpin = 1 << 22;   // bound on mbarrier polls before a product is declared failed
+constexpr int kTcPer = 9;          // staged elements per thread and chunk: 144 * 32 / 512
 
 DEVI uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -149,29 +150,76 @@ DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const 
     bool ok = true;
     for (int k0 = 0; k0 < kpad; k0 += kTcKC) {
         const int kc = min(kTcKC, kpad - k0);   // a multiple of 8
-        for (int e = tid; e < 2 * n * kc; e += T) {
-            const int m = e / kc, kk = e - m * kc, k = k0 + kk;
-            double v = 0.0;
-            if (k < n) {
-                const int r = m < n ? m : m - n;
-                const cplx z = right ? X[r * ld + k] : X[k * ld + r];
-                v = m < n ? z.x : z.y;
+        // A: one complex element of X per thread and step, consecutive threads on
+        // consecutive addresses (along k for right products, along the row index for
+        // left ones); its real part goes to row r, its imaginary part to row r + n.
+        // Every load of a thread is issued before the first split, so the L2
+        // latencies overlap (kTcPer >= n * kTcKC / blockDim.x).
+        {
+            cplx z[kTcPer];
+            int offs[kTcPer];
+#pragma unroll
+            for (int q = 0; q < kTcPer; ++q) {
+                const int e = tid + q * T;
+                offs[q] = -1;
+                z[q] = cmk(0.0, 0.0);
+                if (e < n * kc) {
+                    int r, kk;
+                    if (right) {
+                        r = e / kc;
+                        kk = e - r * kc;
+                    } else {
+                        kk = e / n;
+                        r = e - kk * n;
+                    }
+                    const int k = k0 + kk;
+                    if (k < n) z[q] = right ? X[r * ld + k] : X[k * ld + r];
+                    offs[q] = (kk >> 2) * (kTcMT * 4) + r * 4 + (kk & 3);
+                }
             }
-            uint32_t hi, lo;
-            split_tf32(v, hi, lo);
-            const int off = (kk >> 2) * (kTcMT * 4) + m * 4 + (kk & 3);
-            b.ahi[off] = hi;
-            b.alo[off] = lo;
+#pragma unroll
+            for (int q = 0; q < kTcPer; ++q) {
+                if (offs[q] < 0) continue;
+                uint32_t hr, lr, hi_, li_;
+                split_tf32(z[q].x, hr, lr);
+                split_tf32(z[q].y, hi_, li_);
+                b.ahi[offs[q]] = hr;
+                b.alo[offs[q]] = lr;
+                b.ahi[offs[q] + n * 4] = hi_;
+                b.alo[offs[q] + n * 4] = li_;
+            }
         }
-        for (int e = tid; e < nb * kc; e += T) {
-            const int j = e / kc, kk = e - j * kc, k = k0 + kk;
-            double v = 0.0;
-            if (k < n && j < n) v = (right ? R[k * ld + j] : R[j * ld + k]) - (j == k ? 1.0 : 0.0);
-            uint32_t hi, lo;
-            split_tf32(v, hi, lo);
-            const int off = (kk >> 2) * (kTcNB * 4) + j * 4 + (kk & 3);
-            b.bhi[off] = hi;
-            b.blo[off] = lo;
+        // B = (R - I) along the contiguous index: j for right products (R[k][j]), k for left ones
+        {
+            double v[kTcPer];
+            int offs[kTcPer];
+#pragma unroll
+            for (int q = 0; q < kTcPer; ++q) {
+                const int e = tid + q * T;
+                offs[q] = -1;
+                v[q] = 0.0;
+                if (e < nb * kc) {
+                    int j, kk;
+                    if (right) {
+                        kk = e / nb;
+                        j = e - kk * nb;
+                    } else {
+                        j = e / kc;
+                        kk = e - j * kc;
+                    }
+                    const int k = k0 + kk;
+                    if (k < n && j < n) v[q] = (right ? R[k * ld + j] : R[j * ld + k]) - (j == k ? 1.0 : 0.0);
+                    offs[q] = (kk >> 2) * (kTcNB * 4) + j * 4 + (kk & 3);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kTcPer; ++q) {
+                if (offs[q] < 0) continue;
+                uint32_t hi, lo;
+                split_tf32(v[q], hi, lo);
+                b.bhi[offs[q]] = hi;
+                b.blo[offs[q]] = lo;
+            }
         }
         fence_async_smem();
         tc_fence_before();
@@ -216,12 +264,19 @@ DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const 
             const int m = 128 * t + 32 * q + lane;
             if (m < 2 * n) {
                 const int row = m < n ? m : m - n, part = m < n ? 0 : 1;
+                double xv[16];
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) {   // all 16 loads in flight before the adds
+                    const int j = 16 * cc + jj;
+                    const long idx = right ? (long)row * ld + j : (long)j * ld + row;
+                    xv[jj] = j < n ? Cd[2 * idx + part] : 0.0;
+                }
 #pragma unroll
                 for (int jj = 0; jj < 16; ++jj) {
                     const int j = 16 * cc + jj;
                     if (j < n) {
                         const long idx = right ? (long)row * ld + j : (long)j * ld + row;
-                        Cd[2 * idx + part] += (double)__uint_as_float(r[jj]);
+                        Cd[2 * idx + part] = xv[jj] + (double)__uint_as_float(r[jj]);
                     }
                 }
             }
