@@ -13,7 +13,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libbafqmc_b200.so"
 SOURCES = ["sweep_kernels.cu", "pole_kernels.cu", "capi.cu"]
-HEADERS = ["cplx.cuh", "linalg.cuh", "sweep.cuh", "kernels.h"]
+HEADERS = ["cplx.cuh", "linalg.cuh", "linalg_big.cuh", "tc.cuh", "sweep.cuh", "kernels.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
