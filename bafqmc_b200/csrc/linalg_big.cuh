@@ -49,42 +49,96 @@ DEVI double warp_norm(int n, int ld, const cplx* A, int j, int r0) {
 }
 
 // C = op(A) op(B), C distinct from A and B; tri as in gemm_rs.
+// Work items are a warp's: with B untransposed (B.sc == 1) lanes take 32
+// consecutive columns of C over kGW rows, so each B(k, :) load is one coalesced
+// row segment and each A(r, k) load is the same address in every lane; with A
+// conjugate-transposed (A.sr == 1) lanes take 32 consecutive rows over kGW
+// columns, the mirror image.  The remaining case (A untransposed, B
+// transposed) keeps per-thread TR x TC tiles.  Every element of C takes the
+// same k-ordered cfma sequence in all three forms.
+constexpr int kGW = 9;
 template <int TR, int TC>
 COLD void gemm_big(int n, int ld, cplx* C, MatOp A, MatOp B, int tri = TRI_NONE) {
-    const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
-    for (int g = threadIdx.x; g < ncg * nrg; g += blockDim.x) {
-        const int r0 = (g / ncg) * TR, c0 = (g % ncg) * TC;
-        cplx acc[TR][TC];
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int nch = (n + 31) >> 5, items = nch * ((n + kGW - 1) / kGW);
+    if (B.sc == 1) {
+        for (int it = threadIdx.x >> 5; it < items; it += nw) {
+            const int c = (it % nch) * 32 + lane, rb = (it / nch) * kGW, cc = min(c, n - 1);
+            cplx acc[kGW];
 #pragma unroll
-        for (int i = 0; i < TR; ++i)
+            for (int i = 0; i < kGW; ++i) acc[i] = cmk(0.0, 0.0);
+            for (int k = 0; k < n; ++k) {
+                cplx bv = B.at(k, cc);
+                if (tri == TRI_B_LOWER_FROM_C && k < cc) bv = cmk(0.0, 0.0);
 #pragma unroll
-            for (int j = 0; j < TC; ++j) acc[i][j] = cmk(0.0, 0.0);
-        for (int k = 0; k < n; ++k) {
-            cplx a[TR], b[TC];
-#pragma unroll
-            for (int i = 0; i < TR; ++i) {
-                const int r = r0 + i;
-                a[i] = (r < n) ? A.at(r, k) : cmk(0.0, 0.0);
-                if (tri == TRI_A_UPPER && k < r) a[i] = cmk(0.0, 0.0);
+                for (int i = 0; i < kGW; ++i) {
+                    const int r = rb + i;
+                    cplx av = A.at(min(r, n - 1), k);
+                    if (tri == TRI_A_UPPER && k < r) av = cmk(0.0, 0.0);
+                    acc[i] = cfma(av, bv, acc[i]);
+                }
             }
 #pragma unroll
-            for (int j = 0; j < TC; ++j) {
-                const int c = c0 + j;
-                b[j] = (c < n) ? B.at(k, c) : cmk(0.0, 0.0);
-                if (tri == TRI_B_LOWER_FROM_C && k < c) b[j] = cmk(0.0, 0.0);
+            for (int i = 0; i < kGW; ++i)
+                if (c < n && rb + i < n) C[(rb + i) * ld + c] = acc[i];
+        }
+    } else if (A.sr == 1) {
+        for (int it = threadIdx.x >> 5; it < items; it += nw) {
+            const int r = (it % nch) * 32 + lane, cb = (it / nch) * kGW, rr = min(r, n - 1);
+            cplx acc[kGW];
+#pragma unroll
+            for (int j = 0; j < kGW; ++j) acc[j] = cmk(0.0, 0.0);
+            for (int k = 0; k < n; ++k) {
+                cplx av = A.at(rr, k);
+                if (tri == TRI_A_UPPER && k < rr) av = cmk(0.0, 0.0);
+#pragma unroll
+                for (int j = 0; j < kGW; ++j) {
+                    const int c = cb + j;
+                    cplx bv = B.at(k, min(c, n - 1));
+                    if (tri == TRI_B_LOWER_FROM_C && k < c) bv = cmk(0.0, 0.0);
+                    acc[j] = cfma(av, bv, acc[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kGW; ++j)
+                if (r < n && cb + j < n) C[r * ld + cb + j] = acc[j];
+        }
+    } else {
+        const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
+        for (int g = threadIdx.x; g < ncg * nrg; g += blockDim.x) {
+            const int r0 = (g / ncg) * TR, c0 = (g % ncg) * TC;
+            cplx acc[TR][TC];
+#pragma unroll
+            for (int i = 0; i < TR; ++i)
+#pragma unroll
+                for (int j = 0; j < TC; ++j) acc[i][j] = cmk(0.0, 0.0);
+            for (int k = 0; k < n; ++k) {
+                cplx a[TR], b[TC];
+#pragma unroll
+                for (int i = 0; i < TR; ++i) {
+                    const int r = r0 + i;
+                    a[i] = (r < n) ? A.at(r, k) : cmk(0.0, 0.0);
+                    if (tri == TRI_A_UPPER && k < r) a[i] = cmk(0.0, 0.0);
+                }
+#pragma unroll
+                for (int j = 0; j < TC; ++j) {
+                    const int c = c0 + j;
+                    b[j] = (c < n) ? B.at(k, c) : cmk(0.0, 0.0);
+                    if (tri == TRI_B_LOWER_FROM_C && k < c) b[j] = cmk(0.0, 0.0);
+                }
+#pragma unroll
+                for (int i = 0; i < TR; ++i)
+#pragma unroll
+                    for (int j = 0; j < TC; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
             }
 #pragma unroll
             for (int i = 0; i < TR; ++i)
 #pragma unroll
-                for (int j = 0; j < TC; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < TC; ++j) {
+                    const int r = r0 + i, c = c0 + j;
+                    if (r < n && c < n) C[r * ld + c] = acc[i][j];
+                }
         }
-#pragma unroll
-        for (int i = 0; i < TR; ++i)
-#pragma unroll
-            for (int j = 0; j < TC; ++j) {
-                const int r = r0 + i, c = c0 + j;
-                if (r < n && c < n) C[r * ld + c] = acc[i][j];
-            }
     }
     __syncthreads();
 }

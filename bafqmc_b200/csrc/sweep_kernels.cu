@@ -468,6 +468,50 @@ DEVI void rank_block_tile(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb, i
             if (own[a][b]) G[(r0 + a) * LD + c0 + b] = g[a][b];
 }
 
+// The deferred rank-KB pass of prop_channel for the classes whose G lives in
+// HBM/L2.  Items are (32-column chunk, PR-row block): a warp's load or store of
+// one row of an item is a coalesced 512-byte segment, where TR x TC tiles of
+// adjacent threads touched a dozen cache lines per load.  (Loading a warp's
+// next item before computing the current one measured slower.)  The block
+// columns are first scaled by their coefficients in place (the strip no longer
+// reads them), with the arithmetic of rank_block_tile, so every element takes
+// the same operations in the same order.
+template <int NMAX>
+DEVI void rank_pass_rows(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb) {
+    constexpr int KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD, PR = 9;
+    auto& s = x.s;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kb * n; e += blockDim.x) {
+        const int m = e / n, r = e - m * n;
+        s.col(m)[r] = cmul(s.coef()[m], s.col(m)[r]);
+    }
+    __syncthreads();
+    const int lane = tid & 31, nw = blockDim.x >> 5;
+    const int nch = (n + 31) >> 5, items = nch * ((n + PR - 1) / PR);
+    for (int it = tid >> 5; it < items; it += nw) {
+        const int c = (it % nch) * 32 + lane, rb = (it / nch) * PR;
+        if (c >= n) continue;
+        cplx g[PR];
+#pragma unroll
+        for (int a = 0; a < PR; ++a) g[a] = G[min(rb + a, n - 1) * LD + c];
+#pragma unroll
+        for (int m = 0; m < KB; ++m) {
+            if (m >= kb) break;
+            const cplx yv = s.row(m)[c];
+            const cplx y = cmk(-yv.x, -yv.y);
+            const cplx* cr = s.col(m);
+#pragma unroll
+            for (int a = 0; a < PR; ++a) g[a] = cfma(cr[min(rb + a, n - 1)], y, g[a]);
+        }
+        const bool cok = (unsigned)(c - slo) >= (unsigned)kb;
+#pragma unroll
+        for (int a = 0; a < PR; ++a) {
+            const int r = rb + a;
+            if (cok && r < n && (unsigned)(r - slo) >= (unsigned)kb) G[r * LD + c] = g[a];
+        }
+    }
+}
+
 template <int NMAX, bool LEFT>
 COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
@@ -623,8 +667,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
         __syncthreads();
         // the block's rank-1 terms on the elements outside its rows and columns
         if constexpr (Cfg<NMAX>::GG) {
-            for (int tile = tid; tile < ncg * nrg; tile += blockDim.x)
-                rank_block_tile<NMAX>(x, G, n, slo, kb, (tile / ncg) * TR, (tile % ncg) * TC);
+            rank_pass_rows<NMAX>(x, G, n, slo, kb);
         } else if (act) {
             rank_block_tile<NMAX>(x, G, n, slo, kb, r0, c0);
         }
