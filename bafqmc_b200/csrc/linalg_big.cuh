@@ -21,31 +21,34 @@ DEVI double warp_max(double v) {
     return v;
 }
 
-// Overflow-safe 2-norm of column j, rows [r0, n), by one warp.
+// Overflow-safe 2-norm of column j, rows [r0, n), by one warp (CM: A is stored
+// column-major, element (r, j) at A[j * ld + r]).
+template <bool CM = false>
 DEVI double warp_colnorm(int n, int ld, const cplx* A, int j, int r0) {
     const int lane = threadIdx.x & 31;
     double m = 0.0;
-    for (int r = r0 + lane; r < n; r += 32) m = fmax(m, fmax(fabs(A[r * ld + j].x), fabs(A[r * ld + j].y)));
+    for (int r = r0 + lane; r < n; r += 32) m = fmax(m, fmax(fabs(A[CM ? j * ld + r : r * ld + j].x), fabs(A[CM ? j * ld + r : r * ld + j].y)));
     m = warp_max(m);
     if (m == 0.0) return 0.0;
     double s = 0.0;
     for (int r = r0 + lane; r < n; r += 32) {
-        const double a = A[r * ld + j].x / m, b = A[r * ld + j].y / m;
+        const double a = A[CM ? j * ld + r : r * ld + j].x / m, b = A[CM ? j * ld + r : r * ld + j].y / m;
         s += a * a + b * b;
     }
     return m * sqrt(warp_sum(s));
 }
 
+template <bool CM = false>
 DEVI double warp_norm(int n, int ld, const cplx* A, int j, int r0) {
     const int lane = threadIdx.x & 31;
     double ss = 0.0;
     for (int r = r0 + lane; r < n; r += 32) {
-        const cplx a = A[r * ld + j];
+        const cplx a = A[CM ? j * ld + r : r * ld + j];
         ss = fma(a.x, a.x, fma(a.y, a.y, ss));
     }
     ss = warp_sum(ss);
     if (!sumsq_unsafe(ss)) return sqrt(ss);
-    return warp_colnorm(n, ld, A, j, r0);
+    return warp_colnorm<CM>(n, ld, A, j, r0);
 }
 
 // C = op(A) op(B), C distinct from A and B; tri as in gemm_rs.
@@ -239,12 +242,13 @@ COLD void permute_cols_big(int n, int ld, cplx* C, const int* piv, const int* ip
 // column pvt from the old column i, with ZLAQP2's norm downdate (barrier);
 // column i takes the reflector and beta, rows above i of columns i and pvt are
 // swapped (barrier).
-template <int RW>
+template <int RW, bool CM = false>
 COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
+#define QA(r, c) A[CM ? (c) * ld + (r) : (r) * ld + (c)]
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, nw = blockDim.x >> 5;
     const double tol3z = 1.0536712127723509e-08;   // sqrt(2^-53), LAPACK's sqrt(dlamch('E'))
     for (int j = wp; j < n; j += nw) {
-        const double v = warp_norm(n, ld, A, j, 0);
+        const double v = warp_norm<CM>(n, ld, A, j, 0);
         if (lane == 0) {
             s.vn1[j] = v;
             s.vn2[j] = v;
@@ -277,13 +281,13 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
 #pragma unroll
         for (int k = 0; k < RW; ++k) {
             const int r = lane + 32 * k;
-            v[k] = (r < n && r > i) ? A[r * ld + pvt] : cmk(0.0, 0.0);
+            v[k] = (r < n && r > i) ? QA(r, pvt) : cmk(0.0, 0.0);
             ss = fma(v[k].x, v[k].x, fma(v[k].y, v[k].y, ss));
         }
         ss = warp_sum(ss);
-        const cplx alpha = A[i * ld + pvt];
+        const cplx alpha = QA(i, pvt);
         double xn = sqrt(ss);
-        if (sumsq_unsafe(ss)) xn = warp_colnorm(n, ld, A, pvt, i + 1);
+        if (sumsq_unsafe(ss)) xn = warp_colnorm<CM>(n, ld, A, pvt, i + 1);
         cplx tau = cmk(0.0, 0.0), beta = alpha, scl = cmk(0.0, 0.0);
         if (!(xn == 0.0 && alpha.y == 0.0)) {
             const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn * xn);
@@ -309,7 +313,7 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
 #pragma unroll
             for (int k = 0; k < RW; ++k) {
                 const int r = lane + 32 * k;
-                a[k] = (r < n && r >= i) ? A[r * ld + src] : cmk(0.0, 0.0);
+                a[k] = (r < n && r >= i) ? QA(r, src) : cmk(0.0, 0.0);
             }
             const double t1 = s.vn1[src], t2 = s.vn2[src];
             cplx w = cmk(0.0, 0.0);
@@ -326,7 +330,7 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
                 const double m2 = a[k].x * a[k].x + a[k].y * a[k].y;
                 if (r == i) ai2 = m2;
                 if (r > i && r < n) rest += m2;
-                if (r < n && r >= i) A[r * ld + j] = a[k];
+                if (r < n && r >= i) QA(r, j) = a[k];
             }
             ai2 = warp_sum(ai2);
             rest = warp_sum(rest);
@@ -347,7 +351,7 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
                 if (recompute) {
                     if (sumsq_unsafe(rest)) {
                         __syncwarp();
-                        nv1 = (i + 1 < n) ? warp_colnorm(n, ld, A, j, i + 1) : 0.0;
+                        nv1 = (i + 1 < n) ? warp_colnorm<CM>(n, ld, A, j, i + 1) : 0.0;
                     } else {
                         nv1 = sqrt(rest);
                     }
@@ -365,17 +369,17 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
 #pragma unroll
             for (int k = 0; k < RW; ++k) {
                 const int r = lane + 32 * k;
-                if (r < n && r > i) A[r * ld + i] = v[k];
+                if (r < n && r > i) QA(r, i) = v[k];
             }
             if (lane == 0) {
-                A[i * ld + i] = beta;
+                QA(i, i) = beta;
                 s.tau[i] = tau;
             }
         }
         if (pvt != i && tid < i) {
-            const cplx ui = A[tid * ld + i], up = A[tid * ld + pvt];
-            A[tid * ld + i] = up;
-            A[tid * ld + pvt] = ui;
+            const cplx ui = QA(tid, i), up = QA(tid, pvt);
+            QA(tid, i) = up;
+            QA(tid, pvt) = ui;
         }
         if (tid == 0 && pvt != i) {
             const int t = s.piv[pvt];
@@ -385,22 +389,24 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
         __syncthreads();
     }
     for (int i = tid; i < n; i += blockDim.x) {
-        const cplx a = A[i * ld + i];
+        const cplx a = QA(i, i);
         const double d = hypot(a.x, a.y);
         s.d[i] = d;
         s.vn1[i] = 1.0 / d;
     }
     __syncthreads();
     for (int e = tid; e < n * n; e += blockDim.x) {
-        const int r = e / n, c = e - (e / n) * n;
+        const int q = e / n, t = e - q * n;   // consecutive threads walk the storage order
+        const int r = CM ? t : q, c = CM ? q : t;
         if (c >= r) {
             const double x = s.vn1[r];
-            const cplx a = A[r * ld + c];
-            A[r * ld + c] = cmk(a.x * x, a.y * x);
+            const cplx a = QA(r, c);
+            QA(r, c) = cmk(a.x * x, a.y * x);
         }
     }
     for (int k = tid; k < n; k += blockDim.x) s.ipiv[s.piv[k]] = k;
     __syncthreads();
+#undef QA
 }
 
 // v[k] = row lane+32k of reflector i (unit at i, zero above), from column i of F.

@@ -224,8 +224,25 @@ DEVI void gemm_real_any(Ctx<NMAX>& x, cplx* C, const void* A, const void* B) {
 template <int NMAX>
 DEVI void qrp_any(Ctx<NMAX>& x, cplx* A) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) qrp_big<C_::RW>(x.n, C_::LD, A, x.s.qr());
-    else qrp_inplace<C_::R8, C_::CPS>(x.n, C_::LD, A, x.s.qr());
+    if constexpr (C_::GG) {
+        // factorised in a column-major copy in S, so each warp's column walk is
+        // contiguous; the operations and their order are those of the row-major call
+        const int n = x.n;
+        cplx* S = x.S();
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const int r = e / n, c = e - r * n;
+            S[c * C_::LD + r] = A[r * C_::LD + c];
+        }
+        __syncthreads();
+        qrp_big<C_::RW, true>(n, C_::LD, S, x.s.qr());
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const int r = e / n, c = e - r * n;
+            A[r * C_::LD + c] = S[c * C_::LD + r];
+        }
+        __syncthreads();
+    } else {
+        qrp_inplace<C_::R8, C_::CPS>(x.n, C_::LD, A, x.s.qr());
+    }
 }
 template <int NMAX>
 DEVI void form_q_any(Ctx<NMAX>& x, const cplx* F, cplx* Q, bool conjT) {
