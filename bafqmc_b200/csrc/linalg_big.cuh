@@ -410,18 +410,29 @@ COLD void qrp_big(int n, int ld, cplx* A, QRScratch s) {
 }
 
 // v[k] = row lane+32k of reflector i (unit at i, zero above), from column i of F.
-template <int RW>
+// dst <- src stored column-major (dst[c * ld + r] = src[r * ld + c]).  The
+// reflector and triangular-solve routines below read F one column per warp;
+// with FCM they read such a copy, so each warp load is one contiguous segment.
+COLD void copy_col_major(int n, int ld, cplx* dst, const cplx* src) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        dst[c * ld + r] = src[r * ld + c];
+    }
+    __syncthreads();
+}
+
+template <int RW, bool FCM = false>
 DEVI void load_reflector_col(int n, int ld, const cplx* F, int i, cplx (&v)[RW]) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < RW; ++k) {
         const int r = lane + 32 * k;
-        v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[r * ld + i] : cmk(0.0, 0.0));
+        v[k] = (r == i) ? cmk(1.0, 0.0) : ((r > i && r < n) ? F[FCM ? i * ld + r : r * ld + i] : cmk(0.0, 0.0));
     }
 }
 
 // C <- Q^H C (ZUNMQR 'L','C'): columns of C are independent.
-template <int RW, int CPW>
+template <int RW, int CPW, bool FCM = false>
 COLD void apply_qh_left_big(int n, int ld, const cplx* F, const cplx* tau, cplx* C) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int j0 = wp * CPW; j0 < n; j0 += nw * CPW) {
@@ -436,7 +447,7 @@ COLD void apply_qh_left_big(int n, int ld, const cplx* F, const cplx* tau, cplx*
         for (int i = 0; i < n; ++i) {
             const cplx ct = cconj(tau[i]);
             cplx v[RW];
-            load_reflector_col<RW>(n, ld, F, i, v);
+            load_reflector_col<RW, FCM>(n, ld, F, i, v);
 #pragma unroll
             for (int q = 0; q < CPW; ++q) {
                 cplx w = cmk(0.0, 0.0);
@@ -461,7 +472,7 @@ COLD void apply_qh_left_big(int n, int ld, const cplx* F, const cplx* tau, cplx*
 }
 
 // C <- C Q (ZUNMQR 'R','N'): rows of C are independent.
-template <int RW, int CPW>
+template <int RW, int CPW, bool FCM = false>
 COLD void apply_q_right_big(int n, int ld, const cplx* F, const cplx* tau, cplx* C) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r0 = wp * CPW; r0 < n; r0 += nw * CPW) {
@@ -476,7 +487,7 @@ COLD void apply_q_right_big(int n, int ld, const cplx* F, const cplx* tau, cplx*
         for (int i = 0; i < n; ++i) {
             const cplx t = tau[i];
             cplx v[RW];
-            load_reflector_col<RW>(n, ld, F, i, v);
+            load_reflector_col<RW, FCM>(n, ld, F, i, v);
 #pragma unroll
             for (int q = 0; q < CPW; ++q) {
                 cplx w = cmk(0.0, 0.0);
@@ -502,7 +513,7 @@ COLD void apply_q_right_big(int n, int ld, const cplx* F, const cplx* tau, cplx*
 
 // Q = H_0 ... H_{n-1} (ZUNGQR), or Q^H with conjT, into Q (no alias with F).
 // Column j of Q is H_0 ... H_j e_j.
-template <int RW, int CPW>
+template <int RW, int CPW, bool FCM = false>
 COLD void form_q_big(int n, int ld, const cplx* F, const cplx* tau, cplx* Q, bool conjT) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int j0 = wp * CPW; j0 < n; j0 += nw * CPW) {
@@ -514,7 +525,7 @@ COLD void form_q_big(int n, int ld, const cplx* F, const cplx* tau, cplx* Q, boo
         for (int i = min(j0 + CPW - 1, n - 1); i >= 0; --i) {
             const cplx t = tau[i];
             cplx v[RW];
-            load_reflector_col<RW>(n, ld, F, i, v);
+            load_reflector_col<RW, FCM>(n, ld, F, i, v);
 #pragma unroll
             for (int q = 0; q < CPW; ++q) {
                 if (j0 + q < i) continue;   // H_i leaves e_j, j < i, unchanged (ZUNG2R); uniform in the warp
@@ -544,7 +555,7 @@ COLD void form_q_big(int n, int ld, const cplx* F, const cplx* tau, cplx* Q, boo
 
 // C <- R^{-1} diag(rs) C (as trsm_left_upper): columns independent; row i's
 // value comes from lane i % 32 by shuffle.
-template <int RW, int CPW>
+template <int RW, int CPW, bool FCM = false>
 COLD void trsm_left_upper_big(int n, int ld, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int j0 = wp * CPW; j0 < n; j0 += nw * CPW) {
@@ -572,7 +583,7 @@ COLD void trsm_left_upper_big(int n, int ld, const cplx* F, const cplx* rinv, co
 #pragma unroll
                 for (int k = 0; k < RW; ++k) {
                     const int r = lane + 32 * k;
-                    fcol[k] = (r < i) ? F[r * ld + i] : cmk(0.0, 0.0);
+                    fcol[k] = (r < i) ? F[FCM ? i * ld + r : r * ld + i] : cmk(0.0, 0.0);
                 }
 #pragma unroll
                 for (int q = 0; q < CPW; ++q) {
@@ -599,7 +610,7 @@ COLD void trsm_left_upper_big(int n, int ld, const cplx* F, const cplx* rinv, co
 
 // C <- C diag(cs) R^{-H} (as trsm_right_upperH): rows independent; column c's
 // value comes from lane c % 32.
-template <int RW, int CPW>
+template <int RW, int CPW, bool FCM = false>
 COLD void trsm_right_upperH_big(int n, int ld, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int r0 = wp * CPW; r0 < n; r0 += nw * CPW) {
@@ -627,7 +638,7 @@ COLD void trsm_right_upperH_big(int n, int ld, const cplx* F, const cplx* rinv, 
 #pragma unroll
                 for (int k = 0; k < RW; ++k) {
                     const int col = lane + 32 * k;
-                    frow[k] = (col < cc) ? F[col * ld + cc] : cmk(0.0, 0.0);
+                    frow[k] = (col < cc) ? F[FCM ? cc * ld + col : col * ld + cc] : cmk(0.0, 0.0);
                 }
 #pragma unroll
                 for (int q = 0; q < CPW; ++q) {

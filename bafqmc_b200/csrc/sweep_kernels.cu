@@ -247,32 +247,42 @@ DEVI void qrp_any(Ctx<NMAX>& x, cplx* A) {
 template <int NMAX>
 DEVI void form_q_any(Ctx<NMAX>& x, const cplx* F, cplx* Q, bool conjT) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) form_q_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), Q, conjT);
-    else form_q<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), Q, conjT);
+    if constexpr (C_::GG) {
+        copy_col_major(x.n, C_::LD, x.S(), F);
+        form_q_big<C_::RW, C_::CPW, true>(x.n, C_::LD, x.S(), x.s.tau(), Q, conjT);
+    } else form_q<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), Q, conjT);
 }
 template <int NMAX>
 DEVI void apply_qh_left_any(Ctx<NMAX>& x, const cplx* F, cplx* C) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) apply_qh_left_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), C);
-    else apply_qh_left<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
+    if constexpr (C_::GG) {
+        copy_col_major(x.n, C_::LD, x.S(), F);
+        apply_qh_left_big<C_::RW, C_::CPW, true>(x.n, C_::LD, x.S(), x.s.tau(), C);
+    } else apply_qh_left<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
 }
 template <int NMAX>
 DEVI void apply_q_right_any(Ctx<NMAX>& x, const cplx* F, cplx* C) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) apply_q_right_big<C_::RW, C_::CPW>(x.n, C_::LD, F, x.s.tau(), C);
-    else apply_q_right<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
+    if constexpr (C_::GG) {
+        copy_col_major(x.n, C_::LD, x.S(), F);
+        apply_q_right_big<C_::RW, C_::CPW, true>(x.n, C_::LD, x.S(), x.s.tau(), C);
+    } else apply_q_right<C_::R8, C_::CPS>(x.n, C_::LD, F, x.s.tau(), C);
 }
 template <int NMAX>
 DEVI void trsm_left_any(Ctx<NMAX>& x, const cplx* F, const cplx* rinv, const double* rs, cplx* C) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) trsm_left_upper_big<C_::RW, C_::CPW>(x.n, C_::LD, F, rinv, rs, C);
-    else trsm_left_upper<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, rs, C);
+    if constexpr (C_::GG) {
+        copy_col_major(x.n, C_::LD, x.S(), F);
+        trsm_left_upper_big<C_::RW, C_::CPW, true>(x.n, C_::LD, x.S(), rinv, rs, C);
+    } else trsm_left_upper<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, rs, C);
 }
 template <int NMAX>
 DEVI void trsm_right_any(Ctx<NMAX>& x, const cplx* F, const cplx* rinv, const double* cs, cplx* C) {
     using C_ = Cfg<NMAX>;
-    if constexpr (C_::GG) trsm_right_upperH_big<C_::RW, C_::CPW>(x.n, C_::LD, F, rinv, cs, C);
-    else trsm_right_upperH<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, cs, C);
+    if constexpr (C_::GG) {
+        copy_col_major(x.n, C_::LD, x.S(), F);
+        trsm_right_upperH_big<C_::RW, C_::CPW, true>(x.n, C_::LD, x.S(), rinv, cs, C);
+    } else trsm_right_upperH<C_::R8, C_::CPS>(x.n, C_::LD, F, rinv, cs, C);
 }
 template <int NMAX>
 DEVI void permute_rows_any(Ctx<NMAX>& x, cplx* C, bool forward) {
