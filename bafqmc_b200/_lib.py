@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libbafqmc_b200.so"
 
 OK = 0
 ERRORS = {-1: "BAFQMC_EARG", -2: "BAFQMC_ECUDA", -3: "BAFQMC_EUNSUPPORTED", -4: "BAFQMC_ESTATE",
-          -5: "BAFQMC_ENUMERIC"}
+          -5: "BAFQMC_ENUMERIC", -6: "BAFQMC_ETIMEOUT"}
 OBS_SCALARS = 32
 COUNTERS = 14
 POLE_SCALARS = 5
@@ -41,6 +41,7 @@ class Point(C.Structure):
 _P = C.c_void_p
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int32)
+_FP = C.POINTER(C.c_float)
 SIGNATURES = {
     "bafqmc_create": (C.c_int, [C.POINTER(Point), C.c_int, _IP, C.c_int, C.c_int, C.POINTER(_P)]),
     "bafqmc_create_tuned": (C.c_int, [C.POINTER(Point), C.c_int, _IP, C.c_int, C.c_int, _IP, C.POINTER(_P)]),
@@ -71,6 +72,20 @@ SIGNATURES = {
     "bafqmc_synchronize": (C.c_int, [_P]),
     "bafqmc_stream": (_P, [_P]),
     "bafqmc_sweep_noalloc": (C.c_int, [C.POINTER(Point), C.c_int, _P, _P, C.c_int, _P, _P]),
+    "bafqmc_net_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
+    "bafqmc_net_destroy": (None, [_P]),
+    "bafqmc_net_num_params": (C.c_longlong, [_P]),
+    "bafqmc_net_set_params": (C.c_int, [_P, _FP]),
+    "bafqmc_net_get_params": (C.c_int, [_P, _FP]),
+    "bafqmc_net_set_tensor_cores": (C.c_int, [_P, C.c_int]),
+    "bafqmc_net_forward": (C.c_int, [_P, C.c_int, _DP, _FP]),
+    "bafqmc_net_loss_grad": (C.c_int, [_P, C.c_int, _DP, _DP, _DP, _FP]),
+    "bafqmc_net_reserve_data": (C.c_int, [_P, C.c_int, C.c_int]),
+    "bafqmc_net_collect": (C.c_int, [_P, _P]),
+    "bafqmc_net_train": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, _DP]),
+    "bafqmc_net_status": (C.c_int, [_P, _IP]),
+    "bafqmc_net_set_wait_test": (C.c_int, [_P, C.c_int]),
+    "bafqmc_learned_move": (C.c_int, [_P, _P, _IP, _DP]),
 }
 
 _lib = None

@@ -13,6 +13,7 @@
 
 #include "../../include/bafqmc_b200.h"
 #include "kernels.h"
+#include "net.h"
 #include "sweep.cuh"
 
 using bq::ChainDev;
@@ -184,6 +185,8 @@ double rng_gaussian(int32_t& seed) {   // fields.f90:280-288
 }
 
 }  // namespace
+
+int bq::net_fail(int code, const std::string& msg) { return fail(code, msg); }
 
 struct bafqmc_handle {
     int device = 0;
@@ -375,6 +378,34 @@ void free_handle(bafqmc_handle* h) {
     delete h;
 }
 
+}  // namespace
+
+namespace {
+// the proposal state of the global moves, allocated on first use
+int ensure_proposal_state(bafqmc_handle* h) {
+    if (h->d_arena2) return BAFQMC_OK;
+    CK(cudaMalloc(&h->d_arena2, sizeof(double2) * h->arena_total));
+    CK(cudaMalloc(&h->d_phi2, sizeof(double) * h->phi_total));
+    CK(cudaMalloc(&h->d_sc2, sizeof(ChainScalars) * h->nchains));
+    CK(cudaMemset(h->d_sc2, 0, sizeof(ChainScalars) * h->nchains));
+    CK(cudaMalloc(&h->d_fn2, sizeof(double) * h->nchains));
+    CK(cudaMalloc(&h->d_acc, sizeof(int) * h->nchains));
+    return BAFQMC_OK;
+}
+// every chain of the handle is a number-conserving chain of the network's lattice
+int check_net_chains(const bafqmc_handle* h, const bafqmc_net* n) {
+    for (int c = 0; c < h->nchains; ++c) {
+        const PointHost& p = h->pts[h->chain_point[c]];
+        if (p.pairing)
+            return fail(BAFQMC_EUNSUPPORTED, "the learned proposer runs number-conserving chains only (chain " +
+                                                 std::to_string(c) + " is a Nambu chain)");
+        if (p.p.Lx != n->shape.Lx || p.p.Ly != n->shape.Ly || p.p.Ltrot != n->shape.L)
+            return fail(BAFQMC_EARG, "chain " + std::to_string(c) + " is not on the network's lattice (" +
+                                         std::to_string(n->shape.Lx) + "x" + std::to_string(n->shape.Ly) + ", Ltrot " +
+                                         std::to_string(n->shape.L) + ")");
+    }
+    return BAFQMC_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -717,24 +748,85 @@ int bafqmc_global_shift(bafqmc_handle* h, const double* shift, int* accepted) {
     if (!h || !shift) return fail(BAFQMC_EARG, "null argument");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     CK(cudaSetDevice(h->device));
-    if (!h->d_arena2) {
-        CK(cudaMalloc(&h->d_arena2, sizeof(double2) * h->arena_total));
-        CK(cudaMalloc(&h->d_phi2, sizeof(double) * h->phi_total));
-        CK(cudaMalloc(&h->d_sc2, sizeof(ChainScalars) * h->nchains));
-        CK(cudaMemset(h->d_sc2, 0, sizeof(ChainScalars) * h->nchains));
-        CK(cudaMalloc(&h->d_fn2, sizeof(double) * h->nchains));
-        CK(cudaMalloc(&h->d_acc, sizeof(int) * h->nchains));
-    }
+    int rc = ensure_proposal_state(h);
+    if (rc != BAFQMC_OK) return rc;
     const bq::KernelArgs ka = h->args(), kp = h->args2();
     CK(bq::launch_global_propose(ka, kp, shift, h->stream));
     for (int c = 0; c < bq::kNumClasses; ++c)
         CK(bq::launch_pre(c, kp, h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
     CK(bq::launch_field_norm(ka, h->d_tmp, h->stream));
     CK(bq::launch_field_norm(kp, h->d_fn2, h->stream));
-    CK(bq::launch_global_accept(ka, kp, h->d_tmp, h->d_fn2, h->d_acc, h->stream));
+    CK(bq::launch_global_accept(ka, kp, h->d_tmp, h->d_fn2, nullptr, h->d_acc, h->stream));
     if (accepted) {
         CK(cudaMemcpyAsync(accepted, h->d_acc, sizeof(int) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+    }
+    return BAFQMC_OK;
+}
+
+
+int bafqmc_net_collect(bafqmc_net* n, bafqmc_handle* h) {
+    NvtxRange nvtx_("bafqmc_net_collect");
+    if (!n || !h) return fail(BAFQMC_EARG, "null argument");
+    if (!h->have_fields) return fail(BAFQMC_ESTATE, "fields not initialised");
+    int rc = check_net_chains(h, n);
+    if (rc != BAFQMC_OK) return rc;
+    if (!n->d_data || n->data_chains != h->nchains)
+        return fail(BAFQMC_ESTATE, "bafqmc_net_reserve_data has not reserved a set of this handle's chain count");
+    if (n->data_used >= n->data_slots) return fail(BAFQMC_ESTATE, "the training set is full");
+    CK(cudaSetDevice(h->device));
+    cudaStream_t own = n->stream;
+    n->stream = h->stream;
+    const cudaError_t e = bq::launch_collect(n, h->args(), n->data_used);
+    n->stream = own;
+    CK(e);
+    n->data_used += 1;
+    return BAFQMC_OK;
+}
+
+int bafqmc_learned_move(bafqmc_handle* h, bafqmc_net* n, int* accepted, double* hastings) {
+    NvtxRange nvtx_("bafqmc_learned_move");
+    if (!h || !n) return fail(BAFQMC_EARG, "null argument");
+    if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
+    int rc = check_net_chains(h, n);
+    if (rc != BAFQMC_OK) return rc;
+    CK(cudaSetDevice(h->device));
+    if ((rc = ensure_proposal_state(h)) != BAFQMC_OK) return rc;
+    if ((rc = bq::net_ensure_cap(n, h->nchains)) != BAFQMC_OK) return rc;
+    if (n->move_cap < h->nchains) {
+        if (n->d_lqf) CK(cudaFree(n->d_lqf));
+        if (n->d_hastings) CK(cudaFree(n->d_hastings));
+        n->d_lqf = n->d_hastings = nullptr;
+        CK(cudaMalloc(&n->d_lqf, sizeof(double) * h->nchains));
+        CK(cudaMalloc(&n->d_hastings, sizeof(double) * h->nchains));
+        n->move_cap = h->nchains;
+    }
+    // the network's kernels run on the handle's stream for the move
+    cudaStream_t own = n->stream;
+    n->stream = h->stream;
+    const bq::KernelArgs ka = h->args(), kp = h->args2();
+    cudaError_t e = bq::launch_pack_chains(n, ka);
+    if (e == cudaSuccess) e = bq::net_forward(n, h->nchains);
+    if (e == cudaSuccess) e = bq::launch_learned_propose(n, ka, kp, n->d_lqf);
+    if (e == cudaSuccess) e = bq::launch_pack_chains(n, kp);
+    if (e == cudaSuccess) e = bq::net_forward(n, h->nchains);
+    if (e == cudaSuccess) e = bq::launch_learned_reverse(n, ka, kp, n->d_lqf, n->d_hastings);
+    n->stream = own;
+    CK(e);
+    for (int c = 0; c < bq::kNumClasses; ++c)
+        CK(bq::launch_pre(c, kp, h->d_cls[c], (int)h->cls_list[c].size(), h->stream));
+    CK(bq::launch_field_norm(ka, h->d_tmp, h->stream));
+    CK(bq::launch_field_norm(kp, h->d_fn2, h->stream));
+    CK(bq::launch_global_accept(ka, kp, h->d_tmp, h->d_fn2, n->d_hastings, h->d_acc, h->stream));
+    if (accepted) CK(cudaMemcpyAsync(accepted, h->d_acc, sizeof(int) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    if (hastings)
+        CK(cudaMemcpyAsync(hastings, n->d_hastings, sizeof(double) * h->nchains, cudaMemcpyDeviceToHost, h->stream));
+    if (accepted || hastings) {
+        int st = 0;
+        CK(cudaMemcpyAsync(&st, n->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (st) return fail(BAFQMC_ETIMEOUT, "a bounded wait of the tensor-core convolution expired (status " +
+                                                 std::to_string(st) + ")");
     }
     return BAFQMC_OK;
 }

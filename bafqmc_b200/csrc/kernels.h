@@ -43,8 +43,9 @@ cudaError_t launch_field_norm(const KernelArgs& ka, double* out, cudaStream_t st
 cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st);   // bad[chain]: non-finite field
 // global shift move: proposal into kp's state, then the exact decision (kp's pre run in between)
 cudaError_t launch_global_propose(const KernelArgs& ka, const KernelArgs& kp, const double* shift, cudaStream_t st);
+// hastings (optional): log q(phi|phi') - log q(phi'|phi) per chain of a non-symmetric proposal
 cudaError_t launch_global_accept(const KernelArgs& ka, const KernelArgs& kp, const double* fn, const double* fn2,
-                                 int* accepted, cudaStream_t st);
+                                 const double* hastings, int* accepted, cudaStream_t st);
 // block statistics over n = npts * obs_stride values: accumulate one bin, finish blocks, final mean / sem
 cudaError_t launch_stats_add(const double* pout, double* cur, double* blk, int n, int finish, int block_size,
                              cudaStream_t st);

@@ -1772,10 +1772,15 @@ __global__ void global_propose_kernel(KernelArgs ka, KernelArgs kp, double shift
 
 // Exact Metropolis-Hastings decision of a global move (global_update.f90:237-249:
 // accept if w'/w >= u, u the chain's next draw), with log w = -sum phi^2 / 2
-// - 2 log|det(I - B(beta,0))| from the two states' last factorisations at
-// tau = beta.  An accepted chain takes the proposal's fields and UDV arena.
+// - f log|det(I - B(beta,0))| from the two states' last factorisations at
+// tau = beta: f = 2 for a number-conserving chain (flavours b and c = conj(b)),
+// f = 1 for a Nambu chain (the 4Ns determinant to the power -1/2 is the
+// squared modulus of its {b, c^dagger} block's, to the power -1/2).
+// hastings (optional) adds log q(phi|phi') - log q(phi'|phi) of a
+// non-symmetric proposal; a non-finite exponent rejects.  An accepted chain
+// takes the proposal's fields and UDV arena.
 __global__ void global_accept_kernel(KernelArgs ka, KernelArgs kp, const double* fn, const double* fn2,
-                                     int* accepted) {
+                                     const double* hastings, int* accepted) {
     const int chain = blockIdx.x;
     if (chain >= ka.nchains) return;
     const ChainDev cd = ka.chains[chain];
@@ -1785,11 +1790,13 @@ __global__ void global_accept_kernel(KernelArgs ka, KernelArgs kp, const double*
     if (threadIdx.x == 0) {
         acc = 0;
         if (!(sc->status & 1)) {
-            const double lw = fn[chain] - 2.0 * sc->logdetM;
-            const double lw2 = fn2[chain] - 2.0 * kp.sc[chain].logdetM;
+            const double f = P.pairing ? 1.0 : 2.0;
+            const double lw = fn[chain] - f * sc->logdetM;
+            const double lw2 = fn2[chain] - f * kp.sc[chain].logdetM;
+            const double x = lw2 - lw + (hastings ? hastings[chain] : 0.0);
             const uint32_t seed = lcg_mul(kLcgA, sc->seed);
             sc->seed = seed;
-            acc = !(kp.sc[chain].status & 1) && exp(lw2 - lw) >= lcg_u(seed);
+            acc = !(kp.sc[chain].status & 1) && !isnan(x) && x < INFINITY && exp(x) >= lcg_u(seed);
             sc->glb_prop += 1.0;
             if (acc) {
                 sc->glb_acc += 1.0;
@@ -1912,8 +1919,8 @@ cudaError_t launch_global_propose(const KernelArgs& ka, const KernelArgs& kp, co
     return cudaGetLastError();
 }
 cudaError_t launch_global_accept(const KernelArgs& ka, const KernelArgs& kp, const double* fn, const double* fn2,
-                                 int* accepted, cudaStream_t st) {
-    global_accept_kernel<<<ka.nchains, 256, 0, st>>>(ka, kp, fn, fn2, accepted);
+                                 const double* hastings, int* accepted, cudaStream_t st) {
+    global_accept_kernel<<<ka.nchains, 256, 0, st>>>(ka, kp, fn, fn2, hastings, accepted);
     return cudaGetLastError();
 }
 cudaError_t launch_field_check(const KernelArgs& ka, int* bad, cudaStream_t st) {

@@ -187,6 +187,18 @@ class Ensemble:
         _lib.check(self.lib.bafqmc_global_shift(self.h, _dptr(sh), _iptr(acc)))
         return acc
 
+    def learned_move(self, net, want: bool = True):
+        """One learned global move per chain (bafqmc_learned_move) with the
+        network `net` (a bafqmc_b200.proposer.Proposer).  Returns (accepted,
+        hastings) per chain, or None without synchronising if want is False."""
+        if not want:
+            _lib.check(self.lib.bafqmc_learned_move(self.h, net.h, None, None))
+            return None
+        acc = np.zeros(self.nchains, dtype=np.int32)
+        hst = np.zeros(self.nchains, dtype=np.float64)
+        _lib.check(self.lib.bafqmc_learned_move(self.h, net.h, _iptr(acc), _dptr(hst)))
+        return acc, hst
+
     def stats_reset(self, block_size: int, max_blocks: int = 1024):
         """Start on-device block statistics of the per-bin point averages (bafqmc_stats_reset)."""
         _lib.check(self.lib.bafqmc_stats_reset(self.h, int(block_size), int(max_blocks)))

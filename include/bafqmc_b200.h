@@ -39,6 +39,7 @@ extern "C" {
 #define BAFQMC_EUNSUPPORTED (-3)/* size or sector not built in this library */
 #define BAFQMC_ESTATE (-4)      /* call out of order (e.g. sweep before pre) */
 #define BAFQMC_ENUMERIC (-5)    /* non-finite Green's function detected */
+#define BAFQMC_ETIMEOUT (-6)    /* a bounded device-side wait expired (the call's results are not valid) */
 
 /* Number of scalar observable slots per chain before the site densities. */
 #define BAFQMC_OBS_SCALARS 32
@@ -185,8 +186,80 @@ int bafqmc_pole_diagnostics(bafqmc_handle* h, double* z, int zstride, double* sc
  * w'/w >= u' for the chain's third draw u' (global_update.f90:237-249).  An
  * accepted chain continues from the proposal's fields and UDV factors.
  * accepted (optional, [nchains]) receives 0 or 1.  Quarantined chains are
- * skipped.  Requires a built G (bafqmc_pre or a sweep). */
+ * skipped.  Requires a built G (bafqmc_pre or a sweep).  The weight's
+ * determinant factor is |det(I - B)|^-2 for a number-conserving chain and
+ * |det(I - B_1)|^-1 for a Nambu chain (its 4Ns determinant to the power -1/2,
+ * src/pairing/src/localU.f90:33-113, is the squared modulus of the
+ * {b, c^dagger} block's). */
 int bafqmc_global_shift(bafqmc_handle* h, const double* shift, int* accepted);
+
+/* Learned global proposer.  The reference has none: its only global move is
+ * the dead global_update.f90 (accept rule global_update.f90:237-249, kept
+ * below with the Hastings term of a non-symmetric proposal).
+ *
+ * The network is a 4-layer periodic 3x3x3 convolution over the (imaginary
+ * time x site) field of one lattice (Lx x Ly sites, Ltrot slices): 2 -> width
+ * -> width -> width -> 4 channels, ReLU between layers, bf16 weights and
+ * activations with float32 accumulation.  Its output per field (t, site, aux)
+ * is a mean displacement m and a log scale lsig of a Gaussian proposal
+ * phi' = phi + m(phi) + exp(lsig(phi)) xi.  Parameters are one float32 vector
+ * (per layer W[27][cout][cin] then b[cout]; tap k = 3((b+1)3 + (c+1)) + (a+1)
+ * for offsets (a, b, c) in (t, y, x)), the layout of the CPU oracle
+ * oracle/proposer.py.  With width 64, Lx*Ly a multiple of 4 and Ltrot a
+ * multiple of 32, the 64-channel layers run on the tensor cores (tcgen05,
+ * operands staged by TMA); bafqmc_net_set_tensor_cores(n, 0) selects the
+ * CUDA-core kernels for the same layers (a cross-check).  A network is not
+ * thread-safe; it runs on its own stream, and on the ensemble's stream inside
+ * bafqmc_learned_move and bafqmc_net_collect. */
+typedef struct bafqmc_net bafqmc_net;
+int bafqmc_net_create(int Lx, int Ly, int Ltrot, int width, int device, bafqmc_net** out);
+void bafqmc_net_destroy(bafqmc_net* n);
+long long bafqmc_net_num_params(const bafqmc_net* n);
+/* set_params also resets the optimiser state */
+int bafqmc_net_set_params(bafqmc_net* n, const float* params);
+int bafqmc_net_get_params(bafqmc_net* n, float* params);
+int bafqmc_net_set_tensor_cores(bafqmc_net* n, int enable);
+/* Host buffers: phi [chains][Ltrot][Lx*Ly][2] doubles (the confin order, rounded
+ * to bf16 on input), out [chains][Ltrot][Lx*Ly][4] floats (m_0, m_1, lsig_0, lsig_1). */
+int bafqmc_net_forward(bafqmc_net* n, int chains, const double* phi, float* out);
+/* Training loss of pairs (phi[b], target[b]): the mean over fields of the
+ * Gaussian negative log-likelihood z^2/2 + lsig, z = (target - phi - m) e^{-lsig}
+ * (inputs stored as float32), and its gradient (grad: num_params floats). */
+int bafqmc_net_loss_grad(bafqmc_net* n, int chains, const double* phi, const double* target, double* loss,
+                         float* grad);
+/* Training set on the device: `slots` snapshots of the fields of a handle
+ * with `chains` chains; bafqmc_net_collect appends the handle's current
+ * fields as the next snapshot (call it after each sweep of the plain sampler). */
+int bafqmc_net_reserve_data(bafqmc_net* n, int chains, int slots);
+int bafqmc_net_collect(bafqmc_net* n, bafqmc_handle* h);
+/* `steps` Adam steps (lr; beta 0.9, 0.999) on batches of `batch` pairs, each a
+ * snapshot of one chain and the same chain `lag` snapshots later, drawn from
+ * the training set by a counter-based generator seeded with `seed`.
+ * losses (optional, [steps]) receives each batch's loss. */
+int bafqmc_net_train(bafqmc_net* n, int steps, int batch, int lag, double lr, unsigned long long seed,
+                     double* losses);
+/* Status word of the tensor-core kernels: 0, or bit 0 (a wait of the copy /
+ * MMA / epilogue pipeline expired and the kernel left its tiles) and bit 1
+ * (the final wait for the MMAs in flight expired before the tensor memory was
+ * released).  A call that sees a nonzero status returns BAFQMC_ETIMEOUT. */
+int bafqmc_net_status(bafqmc_net* n, int* status);
+/* Test hook of the bounded waits: with enable set, the tensor-core kernels
+ * issue no MMA and poll each wait only 4096 times, so every wait expires and
+ * the kernel takes its give-up path (nothing is left in flight, the tensor
+ * memory is released); enable = 0 restores normal operation.  Both clear the
+ * status word. */
+int bafqmc_net_set_wait_test(bafqmc_net* n, int enable);
+/* One learned move of every chain of h (number-conserving chains on the
+ * network's lattice): the network at phi gives the proposal phi' (xi from the
+ * chain's LCG, two draws per field in the field order, the Box-Muller cosine
+ * branch of fields.f90:280-288), the network at phi' gives
+ * hastings = log q(phi|phi') - log q(phi'|phi), phi' is rebuilt from scratch
+ * (bafqmc_pre's work, in the second per-chain state of bafqmc_global_shift),
+ * and the chain's next draw u accepts when
+ * exp(log w(phi') - log w(phi) + hastings) >= u.  accepted and hastings
+ * (optional, [nchains]) receive the decisions and Hastings terms; with either
+ * given the call synchronises.  Quarantined chains are skipped. */
+int bafqmc_learned_move(bafqmc_handle* h, bafqmc_net* n, int* accepted, double* hastings);
 
 /* Per chain, 14 doubles: acc_sum[2], therm_acc_sum[2], Xmaxm, Xmeanm,
  * status (bit 0: the chain's Green's function became non-finite, at a

@@ -1,0 +1,216 @@
+"""The learned proposer on the GPU against its CPU oracle (oracle/proposer.py).
+
+* Forward pass: the tensor-core convolution (64-channel layers) and the
+  CUDA-core kernels against the oracle's bf16-mirroring network, and against
+  each other.  Tolerance: relative Frobenius error 2e-3 and max-abs 1e-2 of
+  the output scale (bf16 activations: an accumulation-order difference can
+  flip one rounding of an activation by 2^-8 relative; measured 2e-4).
+* Gradient: the device's loss and parameter gradient against the oracle's
+  (relative error 1e-4 on the loss, 5e-3 on each layer's gradient; measured
+  1e-5 .. 1.6e-3).
+* Move: decisions, seeds and accepted fields against an oracle acceptance
+  that recomputes both weights from scratch in float64 and draws the same
+  Gaussians from the chain's LCG, with the device's network outputs (the
+  network itself is pinned by the forward test).
+* Bounded waits: with the wait test hook every wait of the tensor-core
+  kernel expires, the call returns BAFQMC_ETIMEOUT with the status set, and
+  the next normal call is exact again.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from bafqmc_b200.params import SolverParams
+from oracle import oracle as O
+from oracle import proposer as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from bafqmc_b200 import build
+    build.build()
+    from bafqmc_b200 import _lib, proposer, solver
+    return proposer, solver, _lib
+
+
+def _params(width=64, seed=1, lsig=None):
+    p = P.init_params(width, seed=seed)
+    layers = P.unpack(p, width)
+    rng = np.random.default_rng(seed + 100)
+    layers[3][0][...] *= 5.0
+    for _, b in layers:
+        b[...] = rng.normal(0, 0.05, size=b.shape)
+    if lsig is not None:   # small moves: mean displacement and log scale nearly constant
+        layers[3][0][...] *= 0.01
+        layers[3][1][0:2] = 0.0
+        layers[3][1][2:4] = lsig
+    return p
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("tc", [True, False])
+def test_forward_matches_oracle(mods, tc):
+    proposer, _, _ = mods
+    Lx, Ly, L = 4, 4, 32
+    params = _params()
+    phi = np.random.default_rng(3).normal(size=(3, L, Lx * Ly, 2))
+    with proposer.Proposer(Lx, Ly, L, params=params) as net:
+        net.set_tensor_cores(tc)
+        out = net.forward(phi)
+        assert net.status() == 0
+    ref = P.forward(params, phi, Lx, Ly, rounding=True)
+    scale = np.max(np.abs(ref))
+    print("rel", _rel(out, ref), "max", np.max(np.abs(out - ref)) / scale)
+    assert _rel(out, ref) <= 2e-3
+    assert np.max(np.abs(out - ref)) <= 1e-2 * scale
+
+
+def test_tensor_cores_agree_with_cuda_cores_at_6x6(mods):
+    proposer, _, _ = mods
+    Lx, Ly, L = 6, 6, 160
+    params = _params(seed=5)
+    phi = np.random.default_rng(4).normal(size=(2, L, Lx * Ly, 2))
+    with proposer.Proposer(Lx, Ly, L, params=params) as net:
+        a = net.forward(phi)
+        net.set_tensor_cores(False)
+        b = net.forward(phi)
+    assert _rel(a, b) <= 2e-3
+    ref = P.forward(params, phi[:1], Lx, Ly, rounding=True)
+    assert _rel(a[:1], ref) <= 2e-3
+
+
+def test_ragged_shape_runs_on_cuda_cores(mods):
+    """3x3 sites, 20 slices: no tensor-core tiling applies; the CUDA-core path serves it."""
+    proposer, _, _lib = mods
+    Lx, Ly, L = 3, 3, 20
+    params = _params(width=32, seed=2)
+    phi = np.random.default_rng(6).normal(size=(2, L, Lx * Ly, 2))
+    with proposer.Proposer(Lx, Ly, L, width=32, params=params) as net:
+        with pytest.raises(_lib.BafqmcError):
+            net.set_tensor_cores(True)
+        out = net.forward(phi)
+    ref = P.forward(params, phi, Lx, Ly, width=32, rounding=True)
+    assert _rel(out, ref) <= 2e-3
+
+
+@pytest.mark.parametrize("tc", [True, False])
+def test_gradient_matches_oracle(mods, tc):
+    proposer, _, _ = mods
+    Lx, Ly, L = 4, 4, 32
+    params = _params(seed=7)
+    rng = np.random.default_rng(8)
+    phi = rng.normal(size=(2, L, Lx * Ly, 2))
+    target = rng.normal(size=phi.shape)
+    with proposer.Proposer(Lx, Ly, L, params=params) as net:
+        net.set_tensor_cores(tc)
+        loss, grad = net.loss_grad(phi, target)
+    # the device stores the pair as float32
+    phi32, tg32 = phi.astype(np.float32).astype(np.float64), target.astype(np.float32).astype(np.float64)
+    rloss, rgrad = P.loss_and_grad(params, phi32, tg32, Lx, Ly, rounding=True)
+    assert abs(loss - rloss) <= 1e-4 * abs(rloss)
+    off = 0
+    for l, (ci, co) in enumerate(P.layer_shapes(64)):
+        n = 27 * co * ci + co
+        e = _rel(grad[off:off + n], rgrad[off:off + n])
+        print("layer", l, "grad rel err", e)
+        assert e <= 5e-3, l
+        off += n
+
+
+def _oracle_log_weight(op, seed, phi):
+    _, _, (ch,) = O.init_chains(op, confin=[(seed, phi)])
+    ch.pre()
+    return ch.pole_diagnostics()["log_weight"]
+
+
+def test_learned_move_decisions_match_oracle(mods):
+    proposer, solver, _ = mods
+    kw = dict(U1=1.0, U2=-0.5, mu=-5.0, Nlx=4, Nly=4, Ltrot=32, Beta=1.6, NlxTherm=4, NlyTherm=4, LtrotTherm=32,
+              Nwrap=8, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0)
+    op, sp = O.Params(**kw), SolverParams(**kw)
+    seeds0 = [31 + 7 * k for k in range(16)]
+    params = _params(seed=11, lsig=math.log(0.02))
+    _, _, chains = O.init_chains(op, seeds=seeds0)
+    with solver.Ensemble([sp], [0] * len(seeds0)) as ens, proposer.Proposer(4, 4, 32, params=params) as net:
+        ens.fields_from_seeds(seeds0)
+        ens.pre()
+        ens.sweep(1)
+        s1, phis1 = ens.get_state()
+        for k, ch in enumerate(chains):
+            ch.pre()
+            ch.sweep_bin()
+            assert int(s1[k]) == ch.seed
+            np.testing.assert_array_equal(phis1[k], ch.phi)
+        out = net.forward(np.stack(phis1))                 # the device network at phi
+        acc, hst = ens.learned_move(net)
+        s2, phis2 = ens.get_state()
+        props = []
+        for k, ch in enumerate(chains):
+            seed, prop, lqf = P.propose(ch.seed, ch.phi, out[k])
+            props.append((seed, prop, lqf))
+        outp = net.forward(np.stack([p for _, p, _ in props]))   # the device network at phi'
+    assert 0 < acc.sum() < len(seeds0), acc
+    for k, ch in enumerate(chains):
+        seed, prop, lqf = props[k]
+        h = P.log_q(prop, ch.phi, outp[k]) - lqf
+        assert abs(h - hst[k]) <= 1e-6 * max(1.0, abs(h)), (k, h, hst[k])
+        lw = _oracle_log_weight(op, ch.seed, ch.phi)
+        lw2 = _oracle_log_weight(op, seed, prop)
+        seed, decision = P.accept(seed, lw, lw2, float(hst[k]))
+        x = lw2 - lw + hst[k]
+        assert bool(acc[k]) == decision or abs(math.exp(x) - (seed / 2 ** 31)) < 1e-9, k
+        assert int(s2[k]) == seed, k
+        if acc[k]:
+            np.testing.assert_allclose(phis2[k], prop, rtol=0, atol=1e-12)
+        else:
+            np.testing.assert_array_equal(phis2[k], ch.phi)
+
+
+def test_bounded_waits_expire_safely(mods):
+    proposer, _, _lib = mods
+    Lx, Ly, L = 4, 4, 32
+    params = _params(seed=13)
+    phi = np.random.default_rng(9).normal(size=(2, L, Lx * Ly, 2))
+    with proposer.Proposer(Lx, Ly, L, params=params) as net:
+        good = net.forward(phi)
+        net.set_wait_test(True)
+        with pytest.raises(_lib.BafqmcError) as ei:
+            net.forward(phi)
+        assert ei.value.code == -6
+        assert net.status() & 1
+        net.set_wait_test(False)
+        assert net.status() == 0
+        again = net.forward(phi)
+    np.testing.assert_array_equal(again, good)
+
+
+def test_training_lowers_the_loss(mods):
+    """A few hundred Adam steps on pairs of the plain sampler's configurations
+    (4x4, L = 32, 64 chains x 24 sweeps, lag 4) lower the batch loss."""
+    proposer, solver, _ = mods
+    sp = SolverParams(U1=1.0, U2=-0.5, mu=-5.0, Nlx=4, Nly=4, Ltrot=32, Beta=1.6, NlxTherm=4, NlyTherm=4,
+                      LtrotTherm=32, Nwrap=8, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0)
+    nch = 64
+    with solver.Ensemble([sp], np.zeros(nch, dtype=np.int32)) as ens, proposer.Proposer(4, 4, 32, seed=3) as net:
+        ens.fields_from_seeds(100 + np.arange(nch))
+        ens.pre()
+        ens.sweep(5)
+        net.reserve(nch, 24)
+        for _ in range(24):
+            ens.sweep(1)
+            net.collect(ens)
+        losses = net.train(300, 16, 4, 1e-3, seed=5)
+        assert net.status() == 0
+    first, last = losses[:30].mean(), losses[-30:].mean()
+    print("loss", first, "->", last)
+    assert np.all(np.isfinite(losses))
+    assert last < first - 0.05
