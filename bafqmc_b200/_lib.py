@@ -17,7 +17,7 @@ OBS_SCALARS = 32
 COUNTERS = 14
 POLE_SCALARS = 5
 NUM_CLASSES = 7
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "wait_test": 2}
 
 
 class BafqmcError(RuntimeError):
@@ -85,6 +85,7 @@ SIGNATURES = {
     "bafqmc_net_train": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_ulonglong, _DP]),
     "bafqmc_net_status": (C.c_int, [_P, _IP]),
     "bafqmc_net_set_wait_test": (C.c_int, [_P, C.c_int]),
+    "bafqmc_net_time_layers": (C.c_int, [_P, C.c_int, C.c_int, _DP]),
     "bafqmc_learned_move": (C.c_int, [_P, _P, _IP, _DP]),
 }
 

@@ -3,6 +3,7 @@
 // device state of a batch of chains of the number-conserving and Nambu
 // pairing solvers.
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1058,9 +1059,10 @@ int bafqmc_autotune(const bafqmc_point* pts, int npts, int device, int trial_cha
 
 int bafqmc_set_precision(bafqmc_handle* h, int mode) {
     if (!h) return fail(BAFQMC_EARG, "null handle");
-    if (mode != BAFQMC_PRECISION_FP64 && mode != BAFQMC_PRECISION_MIXED)
-        return fail(BAFQMC_EARG, "precision must be BAFQMC_PRECISION_FP64 or BAFQMC_PRECISION_MIXED");
-    h->mixed = mode == BAFQMC_PRECISION_MIXED ? 1 : 0;
+    if (mode != BAFQMC_PRECISION_FP64 && mode != BAFQMC_PRECISION_MIXED && mode != BAFQMC_PRECISION_WAIT_TEST)
+        return fail(BAFQMC_EARG,
+                    "precision must be BAFQMC_PRECISION_FP64, BAFQMC_PRECISION_MIXED or BAFQMC_PRECISION_WAIT_TEST");
+    h->mixed = mode;
     return BAFQMC_OK;
 }
 
@@ -1109,6 +1111,32 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kNoAllocMaxDevices = 64;
 unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+cudaError_t g_noalloc_setup_err[kNoAllocMaxDevices] = {};
+
+// a^k mod 2^31 for the kernels' LCG skip-ahead, filled once (thread-safe static)
+const uint32_t* lcg_pow_table() {
+    static const std::vector<uint32_t> tab = [] {
+        std::vector<uint32_t> t(bq::kMaxPow);
+        unsigned long long v = 1;
+        for (int k = 0; k < bq::kMaxPow; ++k) {
+            t[k] = (uint32_t)v;
+            v = (v * 48828125ull) & 0x7fffffffull;
+        }
+        return t;
+    }();
+    return tab.data();
+}
+
+// Set-up of a device, once, with that device current: the scratch array's
+// device address and the LCG power table in constant memory.
+void noalloc_setup(int dev) {
+    void* base = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (e == cudaSuccess) e = bq::upload_pow_table(lcg_pow_table(), bq::kMaxPow);
+    g_noalloc_setup_err[dev] = e;
+    if (e == cudaSuccess) g_noalloc_base[dev] = static_cast<unsigned char*>(base);
+}
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
@@ -1136,12 +1164,15 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(BAFQMC_EARG, "bafqmc_sweep_noalloc: device index too large");
-    if (!g_noalloc_base[dev]) {   // once per device, with that device current
-        void* base = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_noalloc_base[dev] = static_cast<unsigned char*>(base);
-    }
+    std::call_once(g_noalloc_once[dev], noalloc_setup, dev);
+    if (g_noalloc_setup_err[dev] != cudaSuccess)
+        return cuda_fail(g_noalloc_setup_err[dev], "bafqmc_sweep_noalloc set-up (cudaGetSymbolAddress, LCG table)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(BAFQMC_ESTATE, "bafqmc_sweep_noalloc copies host-side set-up data and reads results back on "
+                                   "every call; it cannot run inside a stream capture");
     PointHost ph;
     int rc = setup_point(*pt, ph);
     if (rc != BAFQMC_OK) return rc;
@@ -1153,7 +1184,8 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     const size_t o_ch = align256(o_pt + sizeof(PointDev));
     const size_t o_sc = align256(o_ch + sizeof(ChainDev) * nchains);
     const size_t o_ix = align256(o_sc + sizeof(ChainScalars) * nchains);
-    const size_t o_mt = align256(o_ix + sizeof(int) * nchains);
+    const size_t o_bad = align256(o_ix + sizeof(int) * nchains);
+    const size_t o_mt = align256(o_bad + sizeof(int) * nchains);
     const size_t nn = (size_t)n * n;
     const size_t o_ob = align256(o_mt + sizeof(double2) * (2 * nn + ph.Lq));
     const size_t o_ar = align256(o_ob + sizeof(double) * (size_t)nchains * stride);
@@ -1167,7 +1199,6 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
         return fail(BAFQMC_EARG, msg);
     }
     unsigned char* base = g_noalloc_base[dev];
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // descriptors staged on the host, copied into the array in one transfer
     std::vector<unsigned char> stage(o_ob, 0);
     const PointDev d = point_dev(ph, reinterpret_cast<const double2*>(base + o_mt));
@@ -1184,15 +1215,6 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     std::memcpy(stage.data() + o_mt, ph.expP.a.data(), sizeof(double2) * nn);
     std::memcpy(stage.data() + o_mt + sizeof(double2) * nn, ph.expM.a.data(), sizeof(double2) * nn);
     std::memcpy(stage.data() + o_mt + 2 * sizeof(double2) * nn, ph.phaseR.data(), sizeof(double2) * ph.Lq);
-    static uint32_t apow[bq::kMaxPow];
-    if (apow[0] == 0) {
-        unsigned long long v = 1;
-        for (int k = 0; k < bq::kMaxPow; ++k) {
-            apow[k] = (uint32_t)v;
-            v = (v * 48828125ull) & 0x7fffffffull;
-        }
-    }
-    CK(bq::upload_pow_table(apow, bq::kMaxPow));
     CK(cudaMemcpyAsync(base, stage.data(), o_ob, cudaMemcpyHostToDevice, st));
     // the array keeps the previous call's contents: reset what is accumulated
     CK(cudaMemsetAsync(base + o_ob, 0, o_ar - o_ob, st));
@@ -1211,6 +1233,16 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     ka.timers = 0;
     ka.mixed = 0;
     const int* d_ix = reinterpret_cast<const int*>(base + o_ix);
+    // fields must be finite, as bafqmc_set_state requires
+    int* d_bad = reinterpret_cast<int*>(base + o_bad);
+    CK(bq::launch_field_check(ka, d_bad, st));
+    std::vector<int> bad(nchains);
+    CK(cudaMemcpyAsync(bad.data(), d_bad, sizeof(int) * nchains, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int c = 0; c < nchains; ++c)
+        if (bad[c])
+            return fail(BAFQMC_EARG, "bafqmc_sweep_noalloc: non-finite field value (NaN or Inf) in chain " +
+                                         std::to_string(c));
     CK(bq::launch_pre(cls, ka, d_ix, nchains, st));
     CK(bq::launch_bin_reset(ka, st));
     for (int s = 0; s < nsweep; ++s) CK(bq::launch_sweep(cls, ka, d_ix, nchains, st));
@@ -1218,5 +1250,11 @@ extern "C" int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t
     CK(cudaMemcpyAsync(chain_obs, ka.obs, sizeof(double) * (size_t)nchains * stride, cudaMemcpyDeviceToDevice, st));
     noalloc_seeds_out<<<(nchains + 127) / 128, 128, 0, st>>>(sc, seeds, nchains);
     CK(cudaGetLastError());
-    return BAFQMC_OK;
+    // quarantined chains (status bit 0: a non-finite Green's function)
+    std::vector<ChainScalars> scs(nchains);
+    CK(cudaMemcpyAsync(scs.data(), sc, sizeof(ChainScalars) * nchains, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int quarantined = 0;
+    for (int c = 0; c < nchains; ++c) quarantined += (scs[c].status & 1) ? 1 : 0;
+    return quarantined;
 }

@@ -7,7 +7,9 @@
 //
 // Network (the oracle's definition, oracle/proposer.py):
 //   x0 = bf16(phi) (2 channels), x_l = bf16(relu(b_l + conv(x_{l-1}, W_l))) for
-//   l = 1..3 (width channels), out = b_4 + conv(x_3, W_4) (m_0, m_1, lsig_0, lsig_1),
+//   l = 1..3 (width channels), out = b_4 + conv(x_3, W_4) (mu_0, mu_1, lsig_0, lsig_1:
+//   mean and log scale of the proposed field, whose displacement from phi is
+//   the Gaussian mu - phi + exp(lsig) xi),
 // with periodic neighbours in t, y and x, bf16 weights and float32 accumulation.
 //
 // Kernels here run on the CUDA cores and serve every layer shape; the
@@ -280,13 +282,14 @@ __global__ void bgrad_kernel(NetShape s, const __nv_bfloat16* g, int pout, int c
 }
 
 // Loss of the pairs (input config pairs[b], target config pairs[B + b]) of the
-// float32 set src, and the gradient of the output (bf16, plane-major, 2 planes).
+// float32 set src: the Gaussian NLL of the target under N(mu, exp(lsig)^2) from
+// the network at the input (in d_out), and the gradient of the output (bf16,
+// plane-major, 2 planes).
 __global__ void loss_kernel(NetShape s, const float* out, const float* src, const int* pairs, int B,
                             __nv_bfloat16* g4, double* loss, double inv_nf) {
     __shared__ double red[32];
     const int b = blockIdx.x;
     const long long cfg = (long long)s.L * s.Ns * 2;
-    const float* in = src + pairs[b] * cfg;
     const float* tg = src + pairs[B + b] * cfg;
     double v[1] = {0.0};
     for (int r = threadIdx.x; r < s.L * s.Ns; r += blockDim.x) {
@@ -296,7 +299,7 @@ __global__ void loss_kernel(NetShape s, const float* out, const float* src, cons
         for (int a = 0; a < 2; ++a) {
             const double m = o[a], ls = o[2 + a];
             const double e = exp(-ls);
-            const double z = ((double)tg[(long long)r * 2 + a] - (double)in[(long long)r * 2 + a] - m) * e;
+            const double z = ((double)tg[(long long)r * 2 + a] - m) * e;
             v[0] += 0.5 * z * z + ls;
             f[a] = (float)(-z * e * inv_nf);
             f[2 + a] = (float)((1.0 - z * z) * inv_nf);
@@ -369,9 +372,10 @@ __global__ void requant_bwd_kernel(NetShape s, const float* p, __nv_bfloat16* wt
 }
 
 // ---------------------------------------------------------------------------
-// The move.  Proposal phi' = phi + m + exp(lsig) xi with xi from the chain's
-// LCG (two draws per field in the field order, the Box-Muller cosine branch of
-// fields.f90:280-288); lqf = log q(phi'|phi) = sum(-xi^2/2 - lsig).
+// The move.  Proposal phi' = mu + exp(lsig) xi (mu, lsig: the network at phi)
+// with xi from the chain's LCG (two draws per field in the field order, the
+// Box-Muller cosine branch of fields.f90:280-288); lqf = log q(phi'|phi) =
+// sum(-xi^2/2 - lsig).
 __global__ void learned_propose_kernel(NetShape s, const float* out, KernelArgs ka, KernelArgs kp, double* lqf) {
     __shared__ double red[32];
     const int chain = blockIdx.x;
@@ -385,7 +389,6 @@ __global__ void learned_propose_kernel(NetShape s, const float* out, KernelArgs 
     const int nf = s.L * s.Ns * 2;
     const uint32_t step = lcg_pow(2ull * blockDim.x);
     uint32_t sd = lcg_mul(lcg_pow(2ull * threadIdx.x + 1ull), seed0);
-    const double* phi = ka.phi + cd.phi_off;
     double* prop = kp.phi + cd.phi_off;
     const float* o = out + (long long)chain * s.L * s.Ns * kNetOut;
     double v[1] = {0.0};
@@ -395,7 +398,7 @@ __global__ void learned_propose_kernel(NetShape s, const float* out, KernelArgs 
         const double xi = sqrt(-2.0 * log(u1)) * cos(2.0 * 3.14159265358979323846 * u2);
         const double m = o[(f >> 1) * kNetOut + (f & 1)];
         const double ls = o[(f >> 1) * kNetOut + 2 + (f & 1)];
-        prop[f] = phi[f] + m + exp(ls) * xi;
+        prop[f] = m + exp(ls) * xi;
         v[0] += -0.5 * xi * xi - ls;
         sd = lcg_mul(step, sd);
     }
@@ -408,6 +411,7 @@ __global__ void learned_propose_kernel(NetShape s, const float* out, KernelArgs 
 }
 
 // hastings = log q(phi|phi') - log q(phi'|phi), out = the network at phi'
+// (phi' enters log q(phi|phi') only through the network's output)
 __global__ void learned_reverse_kernel(NetShape s, const float* out, KernelArgs ka, KernelArgs kp, const double* lqf,
                                        double* hastings) {
     __shared__ double red[32];
@@ -419,13 +423,12 @@ __global__ void learned_reverse_kernel(NetShape s, const float* out, KernelArgs 
     }
     const int nf = s.L * s.Ns * 2;
     const double* phi = ka.phi + cd.phi_off;
-    const double* prop = kp.phi + cd.phi_off;
     const float* o = out + (long long)chain * s.L * s.Ns * kNetOut;
     double v[1] = {0.0};
     for (int f = threadIdx.x; f < nf; f += blockDim.x) {
         const double m = o[(f >> 1) * kNetOut + (f & 1)];
         const double ls = o[(f >> 1) * kNetOut + 2 + (f & 1)];
-        const double z = (phi[f] - prop[f] - m) * exp(-ls);
+        const double z = (phi[f] - m) * exp(-ls);
         v[0] += -0.5 * z * z - ls;
     }
     block_sum<1>(v, red);
@@ -482,7 +485,7 @@ cudaError_t launch_pack_data(bafqmc_net* n, const float* src, const int* idx, in
     return cudaGetLastError();
 }
 
-static ConvRefArgs conv_args(bafqmc_net* n, int l, int mode) {
+ConvRefArgs conv_args(bafqmc_net* n, int l, int mode) {
     const NetShape& s = n->shape;
     ConvRefArgs a{};
     a.s = s;
@@ -931,6 +934,39 @@ int bafqmc_net_set_wait_test(bafqmc_net* n, int enable) {
     n->wait_test = enable ? 1 : 0;
     NCK(cudaMemset(n->d_err, 0, sizeof(int)));   // a new test (or its end) starts from a clean status
     return BAFQMC_OK;
+}
+
+int bafqmc_net_time_layers(bafqmc_net* n, int chains, int reps, double* ms) {
+    if (!n || !ms || chains < 1 || reps < 1) return bq::net_fail(BAFQMC_EARG, "bad timing arguments");
+    NCK(cudaSetDevice(n->device));
+    int rc = bq::net_ensure_cap(n, chains);
+    if (rc != BAFQMC_OK) return rc;
+    const bq::NetShape& s = n->shape;
+    // inputs: whatever x0 holds (zeros or the last packed fields); the time does not depend on the values
+    cudaEvent_t ev[bq::kNetLayers + 1];
+    for (auto& e : ev) NCK(cudaEventCreate(&e));
+    double acc[bq::kNetLayers] = {};
+    for (int r = 0; r < reps + 1; ++r) {   // the first repetition warms up
+        NCK(cudaEventRecord(ev[0], n->stream));
+        for (int l = 0; l < bq::kNetLayers; ++l) {
+            cudaError_t e;
+            if (n->use_tc && bq::conv_tc_applies(s, l)) e = bq::launch_conv_tc(n, l, false, chains);
+            else if (l == bq::kNetLayers - 1) e = bq::run_conv_ref<1>(bq::conv_args(n, l, bq::CONV_OUT), chains, n->stream);
+            else e = bq::run_conv_ref<16>(bq::conv_args(n, l, bq::CONV_HIDDEN), chains, n->stream);
+            NCK(e);
+            NCK(cudaEventRecord(ev[l + 1], n->stream));
+        }
+        NCK(cudaEventSynchronize(ev[bq::kNetLayers]));
+        if (r == 0) continue;
+        for (int l = 0; l < bq::kNetLayers; ++l) {
+            float t = 0.f;
+            NCK(cudaEventElapsedTime(&t, ev[l], ev[l + 1]));
+            acc[l] += t;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int l = 0; l < bq::kNetLayers; ++l) ms[l] = acc[l] / reps;
+    return check_status(n);
 }
 
 int bafqmc_net_status(bafqmc_net* n, int* status) {

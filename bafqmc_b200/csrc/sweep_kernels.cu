@@ -147,6 +147,8 @@ struct Smem {
     DEVI uint32_t* tc_slot() const { return at<uint32_t>(oTcBar + 8); }
     DEVI uint32_t* tc_phase() const { return at<uint32_t>(oTcBar + 12); }
     DEVI int* tc_on() const { return at<int>(oTcBar + 16); }
+    DEVI uint32_t* tc_pending() const { return at<uint32_t>(oTcBar + 20); }   // 2 + parity of a group left in flight
+    DEVI int* tc_test() const { return at<int>(oTcBar + 24); }                // the wait-test mode of the products
     DEVI TcBufs tcb() const {
         return TcBufs{at<uint32_t>(oTc), at<uint32_t>(oTc + kTcABytes), at<uint32_t>(oTc + 2 * kTcABytes),
                       at<uint32_t>(oTc + 2 * kTcABytes + kTcBBytes), tc_mbar(), *tc_slot()};
@@ -307,12 +309,15 @@ DEVI void conj_transpose_any(Ctx<NMAX>& x, cplx* A) {
 // real.  With the mixed-precision option on, classes with tensor-core staging
 // run it as tc_product; a product that did not complete within its wait bound
 // leaves X unchanged, flags the chain (status bit 2) and the kernel continues
-// in FP64.
+// in FP64 (the tensor cores stay off for the rest of the launch, so the MMA
+// barrier's parity bookkeeping is not used again).
 template <int NMAX, bool RIGHT>
 DEVI void slice_mult(Ctx<NMAX>& x, cplx* X, const double* R) {
     if constexpr (Cfg<NMAX>::TCORE) {
         if (*x.s.tc_on()) {
-            if (tc_product(x.n, Cfg<NMAX>::LD, X, R, RIGHT, x.s.tcb(), x.s.tc_phase())) return;
+            if (tc_product(x.n, Cfg<NMAX>::LD, X, R, RIGHT, x.s.tcb(), x.s.tc_phase(), *x.s.tc_test() != 0,
+                           x.s.tc_pending()))
+                return;
             if (threadIdx.x == 0) {
                 *x.s.tc_on() = 0;
                 x.sc->status |= 4;
@@ -332,6 +337,8 @@ DEVI void tc_begin(Ctx<NMAX>& x, const KernelArgs& ka) {
         if (threadIdx.x == 0) {
             *x.s.tc_on() = ka.mixed ? 1 : 0;
             *x.s.tc_phase() = 0;
+            *x.s.tc_pending() = 0;
+            *x.s.tc_test() = ka.mixed == 2 ? 1 : 0;
         }
         if (ka.mixed) {
             if (threadIdx.x < 32) tmem_alloc(smem_u32(x.s.tc_slot()), kTcCols);
@@ -342,12 +349,21 @@ DEVI void tc_begin(Ctx<NMAX>& x, const KernelArgs& ka) {
         if (ka.mixed) tc_fence_after();
     }
 }
+// The tensor memory is released only after every MMA group the CTA issued has
+// completed: a group that a product gave up on gets one more bounded wait here;
+// if it still has not arrived the chain's status gets bit 3.
 template <int NMAX>
 DEVI void tc_end(Ctx<NMAX>& x, const KernelArgs& ka) {
     if constexpr (Cfg<NMAX>::TCORE) {
         if (ka.mixed) {
             tc_fence_before();
             __syncthreads();
+            const uint32_t pend = *x.s.tc_pending();
+            if (pend) {
+                const bool done = mbar_wait(smem_u32(x.s.tc_mbar()), pend - 2u);
+                if (threadIdx.x == 0 && !done) x.sc->status |= 8;
+                __syncthreads();
+            }
             tc_fence_after();
             if (threadIdx.x < 32) tmem_dealloc(*x.s.tc_slot(), kTcCols);
         }

@@ -74,9 +74,9 @@ DEVI void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// Waits for the completion of the phase with the given parity; false after kTcSpin polls.
-DEVI bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int it = 0; it < kTcSpin; ++it) {
+// Waits for the completion of the phase with the given parity; false after `spin` polls.
+DEVI bool mbar_wait(uint32_t mbar, uint32_t parity, int spin = kTcSpin) {
+    for (int it = 0; it < spin; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t"
@@ -137,8 +137,13 @@ struct TcBufs {
 // multiple of 128); returns with the CTA synchronised.  *phase (shared
 // memory) is the parity of the next completion of b.mbar.
 // Returns false if an MMA group did not complete within the poll bound (X is
-// then unchanged).
-DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const TcBufs& b, uint32_t* phase) {
+// then unchanged); a group that did not complete within a second bound either
+// is left in flight, and *pending (shared memory) receives 2 + its parity, so
+// that the caller waits for it before it releases the tensor memory.
+// wait_test: issue no MMA and poll 1024 times, so that the wait expires with
+// nothing in flight (the test of this give-up path).
+DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const TcBufs& b, uint32_t* phase,
+                     bool wait_test, uint32_t* pending) {
     cplx* C = X;
     const int tid = threadIdx.x, T = blockDim.x;
     const int nb = (n + 15) & ~15;            // MMA N
@@ -224,7 +229,7 @@ DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const 
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !wait_test) {
             tc_fence_after();
             for (int s = 0; s < kc / 8; ++s) {
 #pragma unroll
@@ -243,11 +248,14 @@ DEVI bool tc_product(int n, int ld, cplx* X, const double* R, bool right, const 
         }
         // every thread waits: the staging buffers are reused by the next chunk
         const uint32_t ph = *phase;
-        if (!mbar_wait(mb, ph)) ok = false;
+        if (!mbar_wait(mb, ph, wait_test ? 1024 : kTcSpin)) ok = false;
         const bool all = __syncthreads_and(ok ? 1 : 0) != 0;
         if (tid == 0) *phase = ph ^ 1u;
         if (!all) {   // give the group in flight one more bounded wait, then stop
-            mbar_wait(mb, ph);
+            if (!wait_test) {
+                const bool done = mbar_wait(mb, ph);
+                if (tid == 0 && !done) *pending = 2u + ph;
+            }
             ok = false;
             break;
         }

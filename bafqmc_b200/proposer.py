@@ -3,7 +3,8 @@
 its parameter files.
 
 The network maps the HS field phi[t][site][aux] of one chain to a Gaussian
-proposal phi' = phi + m(phi) + exp(lsig(phi)) xi (4-layer periodic 3x3x3
+proposal phi' = mu(phi) + exp(lsig(phi)) xi, i.e. a Gaussian displacement
+mu - phi + exp(lsig) xi from phi (4-layer periodic 3x3x3
 convolution over imaginary time and the lattice, 2 -> width -> width ->
 width -> 4 channels, bf16 weights, float32 accumulation).  Moves are
 accepted by the exact Metropolis-Hastings ratio under the true weight
@@ -30,12 +31,14 @@ def layer_shapes(width: int = 64):
 
 
 def init_params(width: int = 64, seed: int = 0) -> np.ndarray:
-    """He-uniform weights (bound sqrt(6 / (27 cin))), zero biases; the last
-    layer at a tenth of that bound, so an untrained network proposes small moves."""
+    """He-uniform weights (bound sqrt(6 / (27 cin))), zero biases, and a zero
+    last layer: the untrained network proposes the prior N(0, 1) for every
+    field independently of phi (mu = 0, lsig = 0), a move whose Hastings term
+    cancels the Gaussian part of the weight exactly."""
     rng = np.random.default_rng(seed)
     parts = []
     for l, (ci, co) in enumerate(layer_shapes(width)):
-        bound = math.sqrt(6.0 / (NTAP * ci)) * (0.1 if l == 3 else 1.0)
+        bound = math.sqrt(6.0 / (NTAP * ci)) * (0.0 if l == 3 else 1.0)
         parts.append(rng.uniform(-bound, bound, size=NTAP * co * ci).astype(np.float32))
         parts.append(np.zeros(co, dtype=np.float32))
     return np.concatenate(parts)
@@ -103,7 +106,7 @@ class Proposer:
 
     # ---- evaluation (host buffers)
     def forward(self, phi: np.ndarray) -> np.ndarray:
-        """phi [B, Ltrot, Ns, 2] -> [B, Ltrot, Ns, 4] (m_0, m_1, lsig_0, lsig_1)."""
+        """phi [B, Ltrot, Ns, 2] -> [B, Ltrot, Ns, 4] (mu_0, mu_1, lsig_0, lsig_1)."""
         x = np.ascontiguousarray(phi, dtype=np.float64)
         B = x.shape[0]
         assert x.shape == (B, self.Ltrot, self.Lx * self.Ly, 2)
@@ -119,6 +122,12 @@ class Proposer:
         grad = np.zeros(self.nparams, dtype=np.float32)
         _lib.check(self.lib.bafqmc_net_loss_grad(self.h, x.shape[0], _d(x), _d(t), _d(loss), _f(grad)))
         return float(loss[0]), grad
+
+    def time_layers(self, chains: int, reps: int = 5) -> np.ndarray:
+        """Milliseconds per launch of each forward layer for `chains` chains (CUDA events)."""
+        ms = np.zeros(4, dtype=np.float64)
+        _lib.check(self.lib.bafqmc_net_time_layers(self.h, int(chains), int(reps), _d(ms)))
+        return ms
 
     # ---- training on the plain sampler's configurations
     def reserve(self, chains: int, slots: int):

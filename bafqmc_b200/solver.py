@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _lib
 from .observables import FILE_ORDER, FILE_ORDER_PAIRING, OBS_SCALARS, decode
-from .params import NAUX, SolverParams, conf_transfer
+from .params import NAUX, ParamError, SolverParams, conf_transfer
 
 
 def _dptr(a: np.ndarray):
@@ -174,7 +174,8 @@ class Ensemble:
 
     def set_precision(self, mode: str):
         """"fp64" (default) or "mixed": slice products of chains with 72 < Ndim <= 144
-        on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision)."""
+        on the tensor cores in 3xTF32-compensated FP32 (bafqmc_set_precision);
+        "wait_test" is the test hook of the products' bounded wait."""
         _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
 
     def global_shift(self, shift) -> np.ndarray:
@@ -409,6 +410,10 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     run_dir = Path(run_dir)
     t0 = time.time()
     p = SolverParams.from_file(run_dir / "paramC_sets.txt", pairing=pairing)
+    if p.is_tau:
+        # dynamics.f90 (entered with is_tau, calc_basic.f90:56) is not part of this library
+        raise ParamError("is_tau = .true. asks for the time-displaced Green's functions (dynamics.f90), which this "
+                         "library does not compute; set is_tau = .false. (line 5 of paramC_sets.txt)")
     info = open(run_dir / "info.txt", "w")
     w = lambda label, v: info.write(f" {label:<47}:{_scalar(v)!r:>26}\n")
     if pairing:   # write_info (src/pairing/src/calc_basic.f90:140-180)

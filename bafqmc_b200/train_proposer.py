@@ -9,11 +9,15 @@ equilibrated for `equil` sweeps; the fields after each of the next `sweeps`
 sweeps are collected on the device (chains x sweeps configurations, 2x10^5
 at the defaults).  The network is then trained by Adam on pairs (phi, phi')
 of one chain `lag` sweeps apart: it learns a Gaussian transition
-phi -> phi + m(phi) + exp(lsig(phi)) xi that jumps as far as `lag` sweeps
-of the plain sampler.  Every step of training (forward, loss, gradient,
-optimiser) runs on the GPU in the library's own kernels.  Finally the
-trained network's moves are tried on the ensemble (each followed by a local
-sweep) and the acceptance is recorded with the parameters.
+phi -> mu(phi) + exp(lsig(phi)) xi that jumps as far as `lag` sweeps of the
+plain sampler.  Every step of training (forward, loss, gradient, optimiser)
+runs on the GPU in the library's own kernels.  The untrained network (zero
+last layer) is the prior's independence sampler; after every chunk of
+steps the network's moves are tried on the ensemble (`eval_moves` moves,
+each followed by a local sweep) and the parameters with the highest exact
+Metropolis-Hastings acceptance so far are kept (the untrained network
+included), since the acceptance, not the training loss, sets what a move
+is worth.
 """
 from __future__ import annotations
 
@@ -40,6 +44,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--width", type=int, default=64)
     ap.add_argument("--moves", type=int, default=20, help="trial moves after training")
+    ap.add_argument("--eval-moves", type=int, default=3, help="moves per acceptance check")
     ap.add_argument("--seed0", type=int, default=7000001)
     ap.add_argument("--out", type=str, default="")
     a = ap.parse_args(argv)
@@ -61,8 +66,20 @@ def main(argv=None):
     ens.synchronize()
     t1 = time.time()
     rec["seconds"]["sampling"] = t1 - t0
-    # Adam with a cosine decay of the learning rate, in chunks
+    def acceptance(k):
+        acc = []
+        for _ in range(k):
+            acc.append(ens.learned_move(net)[0].mean())
+            ens.sweep(1)
+        return float(np.mean(acc))
+
+    # Adam with a cosine decay of the learning rate, in chunks; the parameters
+    # with the best acceptance are kept
+    best_acc, best_params, best_step = acceptance(a.eval_moves), net.get_params(), 0
+    rec["acceptance_untrained"] = best_acc
+    print(f"step 0: acceptance {best_acc:.4f}", flush=True)
     losses = []
+    history = []
     chunk = 250
     done = 0
     while done < a.steps:
@@ -70,12 +87,19 @@ def main(argv=None):
         lr = a.lr * 0.5 * (1.0 + math.cos(math.pi * done / a.steps))
         losses.append(net.train(n, a.batch, a.lag, lr, seed=a.seed0 + done))
         done += n
-        print(f"step {done}: loss {losses[-1][-50:].mean():.5f} (lr {lr:.2e})", flush=True)
+        acc = acceptance(a.eval_moves)
+        history.append((done, float(losses[-1][-50:].mean()), acc))
+        print(f"step {done}: loss {losses[-1][-50:].mean():.5f} (lr {lr:.2e}) acceptance {acc:.4f}", flush=True)
+        if acc >= best_acc:
+            best_acc, best_params, best_step = acc, net.get_params(), done
+    net.set_params(best_params)
     losses = np.concatenate(losses)
     t2 = time.time()
     rec["seconds"]["training"] = t2 - t1
     rec["loss_first_100"] = float(losses[:100].mean())
     rec["loss_last_100"] = float(losses[-100:].mean())
+    rec["history"] = history
+    rec["kept_step"] = best_step
     # the trained moves on the ensemble, each followed by a local sweep
     acc = []
     hst = []

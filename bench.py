@@ -1,22 +1,37 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 BAFQMC sweep.
+"""Benchmark of the B200 BAFQMC sampler at 6x6, beta = 8.
 
-Workload: the batched plain method at 6x6, beta=8 -- number-conserving
-triangular lattice (Ns=36), t=1, U1=1, U2=-0.5, mu=-5, dtau=0.05 (160 slices),
-stabilisation every 10 slices, shiftLoc=1.5, N(0,1) fields from per-chain
-seeds, 4096 independent chains per GPU, FP64 throughout.
+Headline metric: effective samples per second per B200 of the learned
+sampler against the plain FP64 sweep, at equal error bars on rho, -E,
+Re S_SF(K) and Re S_DW(K).
 
-A step is one sweep (left + right traversal of imaginary time, one
-measurement bin) of every chain on the GPU.  value = effective samples/s =
-(chain-sweeps/s) / (2 tau_int), tau_int the largest of rho, -E, Re S_SF(K),
-Re S_DW(K) (calibrated by bafqmc_b200.calibrate_tau; same Markov chain for
-every implementation of this sampler, so the same tau applies to the CPU arm).
+* Plain arm: 4096 number-conserving chains, 6x6 triangular lattice (Ns = 36),
+  t = 1, U1 = 1, U2 = -0.5, mu = -5, beta = 8, dtau = 0.05 (L = 160), Nwrap = 10,
+  shiftLoc = 1.5, N(0,1) fields from per-chain seeds; a step is one sweep
+  (left + right traversal, one measurement bin) of every chain, FP64.
+* Learned arm (the line's value): the same point with 1024 chains; a step is
+  one learned global move (the bf16 convolutional proposer of
+  bafqmc_b200/data/proposer_6x6_beta8.npz, trained on the GPU on 2x10^5
+  configurations of the plain sampler, accepted by the exact
+  Metropolis-Hastings ratio) followed by one local sweep, FP64 sweeps.
+
+ESS/s = (chain-steps/s) / (2 tau_int), tau_int the largest over the four
+observables, calibrated per arm by bafqmc_b200.calibrate_tau (units: steps
+of that arm).  At equal error bars the time each arm needs is inversely
+proportional to its ESS/s, so ess_ratio = ESS/s(learned) / ESS/s(plain) is
+the equal-error speed-up, reported against the 10x target.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--gpus N > 1 without a torchrun environment launches N ranks itself (one
+process per GPU, chains sharded per rank, NCCL all-reduce of each bin
+record in the end-to-end leg); under torchrun the ranks come from the
+environment.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import math
 import os
@@ -34,7 +49,15 @@ sys.path.insert(0, str(ROOT))
 METRIC = "effective samples/sec per B200 at 6x6 β=8: learned+mixed vs plain FP64, equal error"
 UNIT = "effective samples/s"
 TAU_FILE = ROOT / "bafqmc_b200" / "data" / "tau_int_6x6_beta8.json"
+TAU_LEARNED_FILE = ROOT / "bafqmc_b200" / "data" / "tau_int_6x6_beta8_learned.json"
+NET_FILE = ROOT / "bafqmc_b200" / "data" / "proposer_6x6_beta8.npz"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+TARGET_RATIO = 10.0
+# kernel launches of one learned step: the move (input pack + 4 layers, twice;
+# proposal; Hastings term; pre of the proposal; two field norms; accept) and
+# the sweep's bin graph (reset, sweep, finish)
+LEARNED_STEP_LAUNCHES = 2 * 5 + 2 + 1 + 2 + 1 + 3
+PLAIN_STEP_LAUNCHES = 3
 
 
 def workload():
@@ -42,20 +65,20 @@ def workload():
     return workload_6x6_beta8()
 
 
-def tau_table():
-    if TAU_FILE.exists():
-        d = json.loads(TAU_FILE.read_text())
-        return d["tau_int"], f"{TAU_FILE.relative_to(ROOT)} ({d['chains']} chains x {d['sweeps']} sweeps)"
-    return None, "uncalibrated (tau_int = 0.5)"
+def tau_table(path: Path = TAU_FILE):
+    if path.exists():
+        d = json.loads(path.read_text())
+        return d["tau_int"], f"{path.relative_to(ROOT)} ({d['chains']} chains x {d['sweeps']} steps)"
+    return None, f"uncalibrated ({path.name} missing; tau_int = 0.5)"
 
 
-def ess_rate(chain_sweeps_per_s: float):
-    taus, src = tau_table()
+def ess_rate(steps_per_s: float, path: Path = TAU_FILE):
+    taus, src = tau_table(path)
     if not taus:
-        return chain_sweeps_per_s, {"tau_int": None, "tau_source": src}
+        return steps_per_s, {"tau_int": None, "tau_source": src}
     name = max(taus, key=lambda k: taus[k])
-    return chain_sweeps_per_s / (2.0 * taus[name]), {"tau_int_max": round(taus[name], 3), "tau_limiting": name,
-                                                     "tau_source": src}
+    return steps_per_s / (2.0 * taus[name]), {"tau_int_max": round(taus[name], 3), "tau_limiting": name,
+                                              "tau_source": src}
 
 
 def flops_per_chain_sweep(n: int, L: int, nwrap: int, naccept: float) -> float:
@@ -65,6 +88,18 @@ def flops_per_chain_sweep(n: int, L: int, nwrap: int, naccept: float) -> float:
     8 N^2 per accepted rank-1 update, and 2L/Nwrap stabilisations at (15 + 45) N^3
     (pivoted QR + ZUNGQR + ZTRMM, and stab_green), by LAPACK's complex flop counts."""
     return 2 * L * 12.0 * n ** 3 + 8.0 * n ** 2 * naccept + (2.0 * L / nwrap) * 60.0 * n ** 3
+
+
+def conv_flops(chains: int, L: int, ns: int, cin: int = 64, cout: int = 64) -> float:
+    """Algorithmic flops of one periodic 3x3x3 convolution launch: 2 x 27 cin cout per point."""
+    return 2.0 * 27 * cin * cout * chains * L * ns
+
+
+def measured_peaks() -> dict:
+    try:
+        return json.loads(PEAKS_FILE.read_text())
+    except (OSError, ValueError):
+        return {}
 
 
 class ClockSampler:
@@ -195,7 +230,9 @@ def run_reference(args, rank: int, world: int):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(walls)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded N(0,1) HS fields)",
-            "config": {"workload": "6x6 beta=8 batched plain FP64 sweep", "sample_per_step":
+            "config": {"workload": "6x6 beta=8 (U1=1, U2=-0.5, mu=-5, dtau=0.05, L=160, Nwrap=10, shiftLoc=1.5): "
+                                   "the reference's plain local sweep on the host cores (the reference has no "
+                                   "learned sampler)", "sample_per_step":
                        f"{cores} chains x {per} sweeps on {cores} host threads", "chain_sweeps_per_s": rate, **tau},
             "cpu_baseline": {"value": ess, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{cores} chains x {per} sweeps per step, oracle/csweep.cpp (C++ "
@@ -334,13 +371,254 @@ def run_12x12(args):
     ens.close()
 
 
+# ---------------------------------------------------------------------------
+# the two GPU arms of the headline
+def _timed_steps(ens, stream, step, steps, world, dev, sweep_events=False):
+    """Device time of `steps` calls of step() on the ensemble's stream (max over
+    ranks), bracketed by a barrier and synchronize on both sides; with
+    sweep_events, also the summed device time of the sweeps inside the steps."""
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sw = []
+    e0.record(stream)
+    for _ in range(steps):
+        step(sw if sweep_events else None)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    dev_s = e0.elapsed_time(e1) / 1e3
+    sweep_s = sum(a.elapsed_time(b) for a, b in sw) / 1e3 if sw else None
+    if world > 1:
+        t = torch.tensor([dev_s, sweep_s or 0.0], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, sweep_s = float(t[0]), (float(t[1]) if sweep_s is not None else None)
+    return dev_s, sweep_s
+
+
+def plain_arm(args, rank, world, dev):
+    """4096 chains per GPU of the plain FP64 sweep: device-timed chain-sweeps/s."""
+    import torch
+    from bafqmc_b200.solver import Ensemble
+    p = workload()
+    C = args.chains
+    ens = Ensemble([p], np.zeros(C, dtype=np.int32), device=dev.index)
+    ens.fields_from_seeds(20240601 + 7919 * (rank * C + np.arange(C)))
+    ens.pre()
+    for _ in range(max(args.warmup, 3)):
+        ens.sweep(1)
+    ens.synchronize()
+    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+    cnt0 = ens.counters()
+
+    def step(_):
+        ens.sweep(1)
+
+    dev_s, _ = _timed_steps(ens, stream, step, args.steps, world, dev)
+    cnt1 = ens.counters()
+    acc = (cnt1[:, 0:2] - cnt0[:, 0:2]).mean(0) / args.steps
+    ens.close()
+    rate = world * C * args.steps / dev_s
+    ess, tau = ess_rate(rate, TAU_FILE)
+    naccept = float(acc.sum()) * 2 * p.Ltrot * p.Ndim
+    return {"chains_per_gpu": C, "ms_per_step": 1e3 * dev_s / args.steps, "chain_sweeps_per_s": rate,
+            "ess_per_s": ess, "acceptance": acc.tolist(), **tau,
+            "sweep_flops_per_chain": flops_per_chain_sweep(p.Ndim, p.Ltrot, p.Nwrap, naccept)}
+
+
+def learned_arm(args, rank, world, dev):
+    """1024 chains per GPU of the learned sampler (one learned move, then one
+    local sweep, per step): device-timed chain-steps/s, the sweeps' share, the
+    move acceptance, the network layers' times and the end-to-end leg."""
+    import torch
+    from bafqmc_b200.proposer import Proposer
+    from bafqmc_b200.solver import Ensemble
+    p = workload()
+    C = args.learned_chains
+    net = Proposer.load(NET_FILE, device=dev.index)
+    ens = Ensemble([p], np.zeros(C, dtype=np.int32), device=dev.index)
+    ens.fields_from_seeds(31000007 + 7919 * (rank * C + np.arange(C)))
+    ens.pre()
+    ens.sweep(10)
+    for _ in range(max(args.warmup, 3)):
+        ens.learned_move(net, want=False)
+        ens.sweep(1)
+    ens.synchronize()
+    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+    cnt0 = ens.counters()
+
+    def step(sw):
+        ens.learned_move(net, want=False)
+        if sw is None:
+            ens.sweep(1)
+            return
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ens.sweep(1)
+        b.record(stream)
+        sw.append((a, b))
+
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    dev_s, sweep_s = _timed_steps(ens, stream, step, args.steps, world, dev, sweep_events=True)
+    clk = clocks.stop()
+    cnt1 = ens.counters()
+    acc = (cnt1[:, 0:2] - cnt0[:, 0:2]).mean(0) / args.steps
+    move_acc = float((cnt1[:, 9] - cnt0[:, 9]).mean() / args.steps)
+    naccept = float(acc.sum()) * 2 * p.Ltrot * p.Ndim
+    rate = world * C * args.steps / dev_s
+    ess, tau = ess_rate(rate, TAU_LEARNED_FILE)
+    out = {"chains_per_gpu": C, "ms_per_step": 1e3 * dev_s / args.steps, "chain_steps_per_s": rate,
+           "ess_per_s": ess, "acceptance": acc.tolist(), "move_acceptance": move_acc, **tau,
+           "sweep_ms_per_step": 1e3 * sweep_s / args.steps,
+           "sweep_flops_per_chain": flops_per_chain_sweep(p.Ndim, p.Ltrot, p.Nwrap, naccept), "clocks": clk,
+           "net_file": str(NET_FILE.relative_to(ROOT)),
+           "net_sha256_16": hashlib.sha256(NET_FILE.read_bytes()).hexdigest()[:16]}
+    # the network's layers, device-timed at the arm's chain count
+    ms = net.time_layers(C, reps=5)
+    out["layer_ms"] = ms.tolist()
+
+    # ---- end to end through the C ABI with host buffers: every step is one
+    # checkpointed step, as a reference run from confin.txt to confout.txt: the
+    # chains' seeds and fields go host -> device from pinned memory
+    # (bafqmc_set_state), bafqmc_pre rebuilds the UDV slots, one learned move and
+    # one sweep, and the bin records, seeds and fields come back device -> host.
+    from bafqmc_b200.multigpu import chain_average, torch_all_reduce
+    import torch.distributed as dist
+    reduce = torch_all_reduce(device=dev) if world > 1 else (lambda b: b)
+    nphi = int(ens.phi_offsets[-1])
+    h_seeds = torch.empty(C, dtype=torch.int32, pin_memory=True).numpy()
+    h_phi = torch.empty(nphi, dtype=torch.float64, pin_memory=True).numpy()
+    ens.get_state_flat(h_seeds, h_phi)
+    h2d = h_seeds.nbytes + h_phi.nbytes
+    d2h = 0
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ens.set_state_flat(h_seeds, h_phi)
+        ens.pre()
+        ens.learned_move(net, want=False)
+        ens.sweep(1)
+        pt = ens.point_obs_raw()
+        ch = ens.chain_obs_raw()
+        ens.get_state_flat(h_seeds, h_phi)
+        d2h = pt.nbytes + ch.nbytes + h_seeds.nbytes + h_phi.nbytes
+        chain_average(pt[0] * C, C, reduce)   # job-wide average (m_process_obs_equal's MPI_REDUCE)
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value, _ = ess_rate(world * C * args.steps / e2e_s, TAU_LEARNED_FILE)
+    out["e2e"] = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                  "step": "checkpointed step: set_state (pinned h2d) + pre + learned move + 1 sweep + bins and "
+                          "state d2h"}
+    ens.close()
+    net.close()
+    return out
+
+
+def run_headline(args, rank, world, local):
+    # the CPU baseline runs before any CUDA call
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_cores or (os.cpu_count() or 1))
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    plain = plain_arm(args, rank, world, dev)
+    learned = learned_arm(args, rank, world, dev)
+    peaks = measured_peaks()
+    if rank == 0:
+        fp64_peak = fp64_gemm_peak(dev)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    p = workload()
+    C = learned["chains_per_gpu"]
+    # dominant kernel: the FP64 sweep (timed inside the learned steps)
+    sweep_tflops = learned["sweep_flops_per_chain"] * C / (learned["sweep_ms_per_step"] / 1e3) / 1e12
+    traffic = None
+    tfile = ROOT / "profiles" / "sweep_kernel_6x6_beta8.md"
+    if tfile.exists():
+        import re
+        m = re.search(r"dram_bytes_per_launch_4096_chains:\s*(\d+)", tfile.read_text())
+        if m:   # per launch, scaled to this run's chain count
+            traffic = int(m.group(1)) * C // 4096
+    bf16_peak = peaks.get("bf16_tflops")
+    conv_ms = float(np.mean(learned["layer_ms"][1:3]))
+    conv_tflops = conv_flops(C, p.Ltrot, p.Lq) / (conv_ms / 1e3) / 1e12
+    ratio = learned["ess_per_s"] / plain["ess_per_s"]
+    line = {
+        "metric": METRIC, "value": learned["ess_per_s"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": learned["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 sweeps + bf16 network (f32 accumulate)",
+        "data": "synthetic (seeded N(0,1) HS fields)",
+        "config": {
+            "workload": "6x6 beta=8 learned sampler (U1=1, U2=-0.5, mu=-5, dtau=0.05, L=160, Nwrap=10, "
+                        "shiftLoc=1.5): one learned global move + one local sweep per step, 1024 chains per GPU",
+            "parallelism": f"chains x {world} GPU",
+            "precision": "sweeps, stabilisation, (I-B)^-1, ratios and acceptance FP64 (the 6x6 kernel class has no "
+                         "mixed slice-product path); proposer network bf16 with f32 accumulation on tcgen05",
+            "g_maxabs_err_vs_fp64": 0.0,
+            "l2": "working set 1.5 MB/chain x chains >> 126 MB L2 (no flush needed)",
+            "learned": {k: v for k, v in learned.items() if k not in ("e2e", "clocks")},
+            "plain": plain,
+            "ess_ratio_learned_vs_plain": ratio, "target_ratio": TARGET_RATIO,
+            "meets_target": bool(ratio >= TARGET_RATIO),
+            "equal_error": "time to a given SEM on all four observables is 2 tau_int / (chain-steps/s) per "
+                           "effective sample, so the ESS/s ratio is the equal-error speed-up",
+        },
+        "roofline": {"bound": "tensor", "pipe": "fp64",
+                     "limiter": "FP64 dependency latency and barriers (the sweep issues DFMA, no tensor instruction)",
+                     "kernel": "sweep_kernel<36,0>", "achieved": sweep_tflops, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": sweep_tflops / fp64_peak, "traffic": traffic,
+                     "traffic_source": "dram bytes of one launch from the ncu capture in "
+                                       "profiles/sweep_kernel_6x6_beta8.md, scaled to this chain count "
+                                       "(not measured in this run)",
+                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no "
+                                    "FP64 figure)"},
+        "roofline_network": {"bound": "tensor", "pipe": "bf16 tcgen05", "kernel": "conv_tc_kernel (64->64 layers)",
+                             "achieved": conv_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                             "frac": conv_tflops / bf16_peak if bf16_peak else None,
+                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), of measured"},
+        "clocks": learned["clocks"],
+        "e2e": learned["e2e"],
+        "gpu_launches": LEARNED_STEP_LAUNCHES * args.steps,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def _spawn_rank(local, args, world, port):
+    os.environ.update({"RANK": str(local), "LOCAL_RANK": str(local), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    os.environ.setdefault("NCCL_DEBUG", "INFO")
+    run_headline(args, local, world, local)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--chains", type=int, default=4096, help="chains per GPU")
+    ap.add_argument("--chains", type=int, default=4096, help="chains per GPU of the plain arm")
+    ap.add_argument("--learned-chains", type=int, default=1024, help="chains per GPU of the learned arm")
     ap.add_argument("--cpu-cores", type=int, default=0, help="cores for the CPU baseline (0 = all)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
@@ -355,143 +633,24 @@ def main():
     if args.workload == "ragged":
         run_ragged(args)
         return
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    env_world = os.environ.get("WORLD_SIZE")
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank, int(env_world or 1))
         return
-
-    # the CPU baseline runs before any CUDA call
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.cpu_cores or (os.cpu_count() or 1))
-
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-
-    from bafqmc_b200.solver import Ensemble
-    p = workload()
-    C = args.chains
-    ens = Ensemble([p], np.zeros(C, dtype=np.int32), device=local)
-    ens.fields_from_seeds(20240601 + 7919 * (rank * C + np.arange(C)))
-    ens.pre()
-    for _ in range(max(args.warmup, 3)):
-        ens.sweep(1)
-    ens.synchronize()
-    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # ---- device-timed region: K sweeps, inputs resident in HBM
-    cnt0 = ens.counters()
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        ens.sweep(1)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize(dev)
-    barrier()
-    clk = clocks.stop()
-    dev_s = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([dev_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s = float(t.item())
-    cnt1 = ens.counters()
-    chain_sweeps = world * C * args.steps / dev_s
-    value, tau = ess_rate(chain_sweeps)
-
-    # ---- end to end through the C ABI with host buffers: every step is one
-    # checkpointed bin, as a reference run from confin.txt to confout.txt: the
-    # chains' seeds and fields go host -> device from pinned memory
-    # (bafqmc_set_state), bafqmc_pre rebuilds the UDV slots, one sweep, and the
-    # bin records, seeds and fields come back device -> host.
-    from bafqmc_b200.multigpu import chain_average, torch_all_reduce
-    reduce = torch_all_reduce(device=dev) if world > 1 else (lambda b: b)
-    nphi = int(ens.phi_offsets[-1])
-    h_seeds = torch.empty(C, dtype=torch.int32, pin_memory=True).numpy()
-    h_phi = torch.empty(nphi, dtype=torch.float64, pin_memory=True).numpy()
-    ens.get_state_flat(h_seeds, h_phi)
-    h2d = h_seeds.nbytes + h_phi.nbytes
-    d2h = 0
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ens.set_state_flat(h_seeds, h_phi)
-        ens.pre()
-        ens.sweep(1)
-        pt = ens.point_obs_raw()
-        ch = ens.chain_obs_raw()
-        ens.get_state_flat(h_seeds, h_phi)
-        d2h = pt.nbytes + ch.nbytes + h_seeds.nbytes + h_phi.nbytes
-        # job-wide chain average across GPUs (m_process_obs_equal's MPI_REDUCE)
-        job_avg = chain_average(pt[0] * C, C, reduce)
-    torch.cuda.synchronize(dev)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value, _ = ess_rate(world * C * args.steps / e2e_s)
-
-    # ---- roofline: FP64 flops of the sweep kernel
-    acc = (cnt1[:, 0:2] - cnt0[:, 0:2]).mean(0) / args.steps     # acceptance per channel
-    naccept = float(acc.sum()) * 2 * p.Ltrot * p.Ndim
-    flops = flops_per_chain_sweep(p.Ndim, p.Ltrot, p.Nwrap, naccept) * C * args.steps
-    achieved = flops / dev_s / 1e12 if world == 1 else flops / dev_s / 1e12
-    if rank == 0:
-        peak = fp64_gemm_peak(dev)
-    if world > 1:
-        dist.barrier()
-    if rank != 0:
-        ens.close()
-        if world > 1:
-            dist.destroy_process_group()
+    if env_world is None and args.gpus > 1:
+        # no launcher: one process per GPU, spawned here
+        import torch.multiprocessing as mp
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        mp.spawn(_spawn_rank, args=(args, args.gpus, port), nprocs=args.gpus, join=True)
         return
-    traffic = None
-    tfile = ROOT / "profiles" / "sweep_kernel_6x6_beta8.md"
-    if tfile.exists():
-        import re
-        m = re.search(r"dram_bytes_per_launch_4096_chains:\s*(\d+)", tfile.read_text())
-        if m:   # per launch, scaled to this run's chain count
-            traffic = int(m.group(1)) * C // 4096
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) HS fields)",
-        "config": {"workload": "6x6 beta=8 batched plain FP64 sweep (U1=1, U2=-0.5, mu=-5, dtau=0.05, "
-                               "L=160, Nwrap=10, shiftLoc=1.5)",
-                   "chains_per_gpu": C, "chain_sweeps_per_s": chain_sweeps, "parallelism": f"chains x {world} GPU",
-                   "l2": "working set 1.4 MB/chain x chains >> 126 MB L2 (no flush needed)",
-                   "acceptance": acc.tolist(), **tau},
-        "roofline": {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"},
-        "clocks": clk,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "step": "checkpointed bin: set_state (pinned h2d) + pre + 1 sweep + bins and state d2h"},
-        "gpu_launches": 3 * args.steps,
-    }
-    if cpu is not None:
-        line["cpu_baseline"] = cpu
-    print(json.dumps(line), flush=True)
-    ens.close()
-    if world > 1:
-        dist.destroy_process_group()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(env_world or 1)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    run_headline(args, rank, world, local)
 
 
 if __name__ == "__main__":

@@ -201,8 +201,10 @@ int bafqmc_global_shift(bafqmc_handle* h, const double* shift, int* accepted);
  * time x site) field of one lattice (Lx x Ly sites, Ltrot slices): 2 -> width
  * -> width -> width -> 4 channels, ReLU between layers, bf16 weights and
  * activations with float32 accumulation.  Its output per field (t, site, aux)
- * is a mean displacement m and a log scale lsig of a Gaussian proposal
- * phi' = phi + m(phi) + exp(lsig(phi)) xi.  Parameters are one float32 vector
+ * is the mean mu and log scale lsig of a Gaussian proposal
+ * phi' = mu(phi) + exp(lsig(phi)) xi, whose displacement from phi is the
+ * Gaussian mu - phi + exp(lsig) xi (with a zero last layer: the prior N(0, 1),
+ * independently of phi).  Parameters are one float32 vector
  * (per layer W[27][cout][cin] then b[cout]; tap k = 3((b+1)3 + (c+1)) + (a+1)
  * for offsets (a, b, c) in (t, y, x)), the layout of the CPU oracle
  * oracle/proposer.py.  With width 64, Lx*Ly a multiple of 4 and Ltrot a
@@ -220,10 +222,10 @@ int bafqmc_net_set_params(bafqmc_net* n, const float* params);
 int bafqmc_net_get_params(bafqmc_net* n, float* params);
 int bafqmc_net_set_tensor_cores(bafqmc_net* n, int enable);
 /* Host buffers: phi [chains][Ltrot][Lx*Ly][2] doubles (the confin order, rounded
- * to bf16 on input), out [chains][Ltrot][Lx*Ly][4] floats (m_0, m_1, lsig_0, lsig_1). */
+ * to bf16 on input), out [chains][Ltrot][Lx*Ly][4] floats (mu_0, mu_1, lsig_0, lsig_1). */
 int bafqmc_net_forward(bafqmc_net* n, int chains, const double* phi, float* out);
 /* Training loss of pairs (phi[b], target[b]): the mean over fields of the
- * Gaussian negative log-likelihood z^2/2 + lsig, z = (target - phi - m) e^{-lsig}
+ * Gaussian negative log-likelihood z^2/2 + lsig, z = (target - mu) e^{-lsig}
  * (inputs stored as float32), and its gradient (grad: num_params floats). */
 int bafqmc_net_loss_grad(bafqmc_net* n, int chains, const double* phi, const double* target, double* loss,
                          float* grad);
@@ -243,6 +245,11 @@ int bafqmc_net_train(bafqmc_net* n, int steps, int batch, int lag, double lr, un
  * (the final wait for the MMAs in flight expired before the tensor memory was
  * released).  A call that sees a nonzero status returns BAFQMC_ETIMEOUT. */
 int bafqmc_net_status(bafqmc_net* n, int* status);
+/* Device time of each layer of the forward pass (ms[4], milliseconds per
+ * launch), averaged over `reps` passes of `chains` chains after one warm-up
+ * pass, timed with CUDA events on the network's stream.  A profiling aid: the
+ * inputs are whatever the network last held. */
+int bafqmc_net_time_layers(bafqmc_net* n, int chains, int reps, double* ms);
 /* Test hook of the bounded waits: with enable set, the tensor-core kernels
  * issue no MMA and poll each wait only 4096 times, so every wait expires and
  * the kernel takes its give-up path (nothing is left in flight, the tensor
@@ -266,7 +273,8 @@ int bafqmc_learned_move(bafqmc_handle* h, bafqmc_net* n, int* accepted, double* 
  * stabilisation or in bafqmc_pre: the chain is quarantined, i.e. later sweeps
  * skip it and bafqmc_bin_point_obs averages over the other chains, until its
  * state is set again; bit 2: a tensor-core product did not complete within
- * its wait bound and the chain continued in FP64), seed, nobs, accepted global moves, proposals[2], accepted[2] (AccCounter,
+ * its wait bound and the chain continued in FP64; bit 3: such a product's MMAs
+ * had still not completed when the sweep released its tensor memory), seed, nobs, accepted global moves, proposals[2], accepted[2] (AccCounter,
  * Prop%Xmaxm/Xmeanm; the last four are PhaseCounter%count_proposed and
  * %count_accepted over all bins, src/pairing/src/operator_Hubbard.f90:269-284.
  * The Nambu weight ratio is real and positive here, so PhaseCounter's phase
@@ -285,6 +293,11 @@ int bafqmc_counters(bafqmc_handle* h, double* out);
  * the next bafqmc_pre / bafqmc_sweep.  Default BAFQMC_PRECISION_FP64. */
 #define BAFQMC_PRECISION_FP64 0
 #define BAFQMC_PRECISION_MIXED 1
+/* Test hook of the products' bounded wait: as MIXED, but the products issue
+ * no MMA and poll their barrier 1024 times, so every chain's first product
+ * gives up (status bit 2, nothing left in flight) and the chain continues in
+ * FP64, bit-identical to a BAFQMC_PRECISION_FP64 run. */
+#define BAFQMC_PRECISION_WAIT_TEST 2
 int bafqmc_set_precision(bafqmc_handle* h, int mode);
 
 /* Per-phase SM cycle counters of the sweep kernel (the reference has only a
@@ -308,11 +321,20 @@ void* bafqmc_stream(bafqmc_handle* h);
  *   chain_obs [nchains][BAFQMC_OBS_SCALARS + Lx*Ly] doubles, device memory: the
  *             bin averages, laid out as bafqmc_bin_chain_obs for that point
  *   stream    cudaStream_t to run on (NULL = legacy default stream)
- * Sizes beyond the array return BAFQMC_EARG with the bytes needed.  The first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  Every call reuses the same array, so calls that
- * overlap on the GPU (other streams, other host threads) race and must not be
- * issued; the call clears the accumulators it reads. */
+ * Sizes beyond the array return BAFQMC_EARG with the bytes needed, and a
+ * NaN or infinite field value returns BAFQMC_EARG naming the chain (as
+ * bafqmc_set_state).  The first call on a device sets it up once (the array's
+ * device address and the LCG table in constant memory, a synchronous copy);
+ * make that first call before any stream capture.  Every call copies
+ * host-side set-up data to the array and reads the fields' check and the
+ * chains' status back, synchronising the stream twice, so a call made while
+ * the stream is capturing returns BAFQMC_ESTATE.  cudaDeviceReset between
+ * calls is not supported (the device address is looked up once).  Every call
+ * reuses the same array, so calls that overlap on the GPU (other streams,
+ * other host threads) race and must not be issued; the call clears the
+ * accumulators it reads.  Returns the number of quarantined chains (>= 0;
+ * their Green's function became non-finite and their chain_obs row is NaN)
+ * or a negative BAFQMC_E* code. */
 #define BAFQMC_NOALLOC_MAX_BYTES (64u << 20)
 int bafqmc_sweep_noalloc(const bafqmc_point* pt, int nchains, int32_t* seeds, double* phi, int nsweep,
                          double* chain_obs, void* stream);

@@ -19,22 +19,27 @@ y*Lx + x, periodic in t, y and x):
   x0 = bf16(phi)                                        (2 channels)
   pre_l[p][o] = b_l[o] + sum_{tap, i} W_l[tap][o][i] x_{l-1}[nbr(p, tap)][i]
   x_l = bf16(relu(pre_l))                               l = 1, 2, 3 (C channels)
-  out = pre_4                                           4 channels: m_0, m_1, lsig_0, lsig_1
+  out = pre_4                                           4 channels: mu_0, mu_1, lsig_0, lsig_1
 
 with taps (a, b, c) in {-1, 0, 1}^3, nbr((t, y, x), (a, b, c)) =
 ((t + a) mod L, (y + b) mod Ly, (x + c) mod Lx), and the tap index
 k = 3 * ((b + 1) * 3 + (c + 1)) + (a + 1).  Weights are bf16 values (the
 float32 master copy rounded), accumulation is float32 on the device.
 
-Proposal: phi' = phi + m(phi) + exp(lsig(phi)) * xi, xi ~ N(0, 1) per field,
-drawn from the chain's LCG by the reference's Box-Muller form (two draws per
-value, fields.f90:280-288) in the field order.  log q(phi'|phi) =
-sum(-xi^2 / 2 - lsig(phi)) (constants cancel in the ratio).
+Proposal: phi' = mu(phi) + exp(lsig(phi)) * xi, xi ~ N(0, 1) per field, i.e.
+the Gaussian displacement phi' - phi = (mu - phi) + exp(lsig) xi: the network
+emits the mean mu of the proposed field (a skip connection from the input),
+so a network whose last layer is zero proposes the prior N(0, 1)
+independently of phi, a move the Gaussian part of the weight accepts with
+ratio 1 exactly.  xi is drawn from the chain's LCG by the reference's
+Box-Muller form (two draws per value, fields.f90:280-288) in the field
+order.  log q(phi'|phi) = sum(-xi^2 / 2 - lsig(phi)) (constants cancel in
+the ratio).
 
 Training loss for a pair (phi, phi_target) (a configuration of the plain
 sampler and one `lag` sweeps later in the same chain):
-  L = mean over fields of [ z^2 / 2 + lsig ],  z = (phi_target - phi - m) exp(-lsig)
-(the Gaussian negative log-likelihood of the displacement), averaged over the
+  L = mean over fields of [ z^2 / 2 + lsig ],  z = (phi_target - mu) exp(-lsig)
+(the Gaussian negative log-likelihood of the transition), averaged over the
 batch.  Backward: gradients of the pre-activations are rounded to bf16 before
 they feed the transposed convolutions (the device stores them in bf16).
 """
@@ -87,13 +92,13 @@ def unpack(params: np.ndarray, width: int = 64):
     return out
 
 
-def init_params(width: int = 64, seed: int = 0) -> np.ndarray:
-    """He-uniform weights (scaled by 1/sqrt(27 cin)), zero biases; the last
-    layer starts at 1/10 of that scale so the first proposals are small moves."""
+def init_params(width: int = 64, seed: int = 0, last_scale: float = 0.0) -> np.ndarray:
+    """He-uniform weights (bound sqrt(6 / (27 cin))), zero biases; the last
+    layer scaled by last_scale (0: the prior's independence sampler)."""
     rng = np.random.default_rng(seed)
     parts = []
     for l, (ci, co) in enumerate(layer_shapes(width)):
-        bound = math.sqrt(6.0 / (NTAP * ci)) * (0.1 if l == 3 else 1.0)
+        bound = math.sqrt(6.0 / (NTAP * ci)) * (last_scale if l == 3 else 1.0)
         parts.append(rng.uniform(-bound, bound, size=NTAP * co * ci).astype(np.float32))
         parts.append(np.zeros(co, dtype=np.float32))
     return np.concatenate(parts)
@@ -151,7 +156,7 @@ def to_grid(phi: np.ndarray, Lx: int, Ly: int) -> np.ndarray:
 
 def forward(params: np.ndarray, phi: np.ndarray, Lx: int, Ly: int, width: int = 64, rounding: bool = True,
             keep: bool = False):
-    """Network output [B, L, Ns, 4] (m_0, m_1, lsig_0, lsig_1) for fields [B, L, Ns, 2].
+    """Network output [B, L, Ns, 4] (mu_0, mu_1, lsig_0, lsig_1) for fields [B, L, Ns, 2].
 
     rounding=True mirrors the device (bf16 weights and activations, float32
     outputs); rounding=False is the float64 network the finite-difference
@@ -176,7 +181,7 @@ def forward(params: np.ndarray, phi: np.ndarray, Lx: int, Ly: int, width: int = 
 
 def loss_and_grad(params: np.ndarray, phi: np.ndarray, target: np.ndarray, Lx: int, Ly: int, width: int = 64,
                   rounding: bool = True):
-    """Mean Gaussian NLL of (target - phi) under N(m, exp(lsig)^2) and its
+    """Mean Gaussian NLL of target under N(mu, exp(lsig)^2) and its
     gradient w.r.t. the flat parameter vector (same layout as params)."""
     layers = unpack(np.asarray(params, dtype=np.float32 if rounding else np.float64), width)
     out, acts = forward(params, phi, Lx, Ly, width, rounding, keep=True)
@@ -184,7 +189,7 @@ def loss_and_grad(params: np.ndarray, phi: np.ndarray, target: np.ndarray, Lx: i
     nf = B * L * ns * 2
     o = out.astype(np.float64)
     m, ls = o[..., 0:2], o[..., 2:4]
-    z = (np.asarray(target, np.float64) - np.asarray(phi, np.float64) - m) * np.exp(-ls)
+    z = (np.asarray(target, np.float64) - m) * np.exp(-ls)
     loss = float(np.sum(0.5 * z * z + ls) / nf)
     g = np.empty_like(o)
     g[..., 0:2] = -z * np.exp(-ls) / nf
@@ -221,20 +226,21 @@ def gaussians(seed: int, n: int) -> tuple[int, np.ndarray]:
 
 
 def log_q(phi_from: np.ndarray, phi_to: np.ndarray, out_from: np.ndarray) -> float:
-    """log q(phi_to | phi_from) up to the constant, from the network output at phi_from."""
+    """log q(phi_to | phi_from) up to the constant, from the network output at
+    phi_from (phi_from enters only through it)."""
     o = np.asarray(out_from, np.float64)
     m, ls = o[..., 0:2], o[..., 2:4]
-    z = (np.asarray(phi_to, np.float64) - np.asarray(phi_from, np.float64) - m) * np.exp(-ls)
+    z = (np.asarray(phi_to, np.float64) - m) * np.exp(-ls)
     return float(np.sum(-0.5 * z * z - ls))
 
 
 def propose(seed: int, phi: np.ndarray, out: np.ndarray):
-    """phi' = phi + m + exp(lsig) xi for one chain ([L, Ns, 2] arrays); returns
+    """phi' = mu + exp(lsig) xi for one chain ([L, Ns, 2] arrays); returns
     (seed after the draws, phi', log q(phi'|phi))."""
     seed, xi = gaussians(seed, phi.size)
     xi = xi.reshape(phi.shape)
     o = np.asarray(out, np.float64)
-    prop = np.asarray(phi, np.float64) + o[..., 0:2] + np.exp(o[..., 2:4]) * xi
+    prop = o[..., 0:2] + np.exp(o[..., 2:4]) * xi
     return seed, prop, float(np.sum(-0.5 * xi * xi - o[..., 2:4]))
 
 

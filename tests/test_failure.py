@@ -93,3 +93,17 @@ def test_rank_leaving_ends_the_next_bin_reduction_with_an_error():
     mp.start_processes(_rank, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     assert out[1] == "left"
     assert out[0].startswith("error"), out[0]
+
+
+def test_time_displaced_request_is_refused(tmp_path):
+    """is_tau = .true. (calc_basic.f90:56) asks for dynamics.f90's time-displaced
+    Green's functions, which this library does not compute: the run directory
+    refuses it before any device work, instead of ignoring the flag."""
+    from bafqmc_b200.params import ParamError
+    from bafqmc_b200.solver import run_directory
+    text = params().to_text().splitlines()
+    text[4] = ".true. 10"
+    (tmp_path / "paramC_sets.txt").write_text("\n".join(text) + "\n")
+    with pytest.raises(ParamError, match="is_tau"):
+        run_directory(tmp_path, nchains=1)
+    assert not (tmp_path / "info.txt").exists()

@@ -118,3 +118,30 @@ def test_9x9_near_band_edge_green_error_every_sweep(solver_mod):
     assert np.all(cnt[:, 6].astype(int) & 4 == 0), "a tensor-core product timed out"
     assert gmax > 0.2
     assert max(errs) < G_TOL, errs
+
+
+def test_expired_product_wait_falls_back_to_fp64_exactly(solver_mod):
+    """The give-up path of the products' bounded wait: in the wait-test mode
+    the products issue no MMA and poll 1024 times, so each chain's first
+    product times out, the chain records status bit 2 and continues in FP64.
+    Nothing is left in flight (bit 3 stays clear), and seeds, fields and G
+    are bit-identical to a plain FP64 run from the same start."""
+    p = point(9, 9, 20, 1.0, nwrap=5)
+    seeds0 = 515 + 17 * np.arange(4)
+    out = {}
+    for mode in ("fp64", "wait_test"):
+        with solver_mod.Ensemble([p], np.zeros(len(seeds0), dtype=np.int32)) as ens:
+            ens.set_precision(mode)
+            ens.fields_from_seeds(seeds0)
+            ens.pre()
+            ens.sweep(1)
+            s, phis = ens.get_state()
+            out[mode] = (s, phis, [ens.green(c) for c in range(len(seeds0))], ens.counters())
+    status = out["wait_test"][3][:, 6].astype(np.int64)
+    assert np.all(status & 4), status
+    assert not np.any(status & 8), status
+    assert not np.any(out["fp64"][3][:, 6].astype(np.int64) & 12)
+    np.testing.assert_array_equal(out["wait_test"][0], out["fp64"][0])
+    for c in range(len(seeds0)):
+        np.testing.assert_array_equal(out["wait_test"][1][c], out["fp64"][1][c])
+        np.testing.assert_array_equal(out["wait_test"][2][c], out["fp64"][2][c])

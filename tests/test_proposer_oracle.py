@@ -11,15 +11,28 @@ from oracle import proposer as P
 
 def _small(width=4, Lx=3, Ly=2, L=4, B=2, seed=0):
     rng = np.random.default_rng(seed)
-    params = P.init_params(width, seed=seed)
     # a last layer as large as the others, so every output depends on every layer
+    params = P.init_params(width, seed=seed, last_scale=1.0)
     layers = P.unpack(params, width)
-    layers[3][0][...] *= 10.0
     for _, b in layers:
         b[...] = rng.normal(0, 0.1, size=b.shape)
     phi = rng.normal(size=(B, L, Lx * Ly, 2))
     target = phi + rng.normal(scale=0.7, size=phi.shape)
     return params.astype(np.float64), phi, target, (Lx, Ly, width)
+
+
+def test_zero_last_layer_is_the_prior_independence_sampler():
+    """mu = 0, lsig = 0: q(phi'|phi) = N(0, 1) whatever phi, and the Gaussian
+    part of the weight cancels the Hastings term exactly."""
+    rng = np.random.default_rng(2)
+    params = P.init_params(8, seed=4)
+    phi = rng.normal(size=(1, 4, 6, 2))
+    out = P.forward(params, phi, 3, 2, width=8)
+    assert np.all(out == 0.0)
+    seed, prop, lqf = P.propose(99, phi[0], out[0])
+    lqr = P.log_q(prop, phi[0], out[0])
+    log_prior_ratio = -0.5 * np.sum(prop ** 2) + 0.5 * np.sum(phi[0] ** 2)
+    assert abs(log_prior_ratio + lqr - lqf) < 1e-9
 
 
 def test_tap_order():
@@ -93,7 +106,7 @@ def test_proposal_log_q_and_draws():
     for _ in range(2 * phi.size):
         s = (48828125 * s) % 2147483648
     assert s == seed
-    np.testing.assert_allclose(prop, phi + out[..., :2] + np.exp(out[..., 2:]) * xi.reshape(phi.shape))
+    np.testing.assert_allclose(prop, out[..., :2] + np.exp(out[..., 2:]) * xi.reshape(phi.shape))
     # the accept rule: exp(x) >= u with u the chain's next draw
     s3, acc = P.accept(seed, 0.0, -1.0, 0.5)
     u = s3 / 2147483648

@@ -94,3 +94,20 @@ def test_noalloc_rejects_sizes_beyond_the_array():
                                   torch.cuda.current_stream().cuda_stream)
     assert rc == -1
     assert b"scratch" in lib.bafqmc_last_error()
+
+
+def test_noalloc_rejects_non_finite_fields():
+    """A NaN field is refused as bafqmc_set_state refuses it, naming the chain."""
+    torch, lib = _setup()
+    from bafqmc_b200 import _lib
+    from bafqmc_b200.solver import point_struct
+    p = _point()
+    nchains, stride = 3, _lib.OBS_SCALARS + p.Lq
+    seeds = torch.tensor([11, 12, 13], dtype=torch.int32, device="cuda")
+    phi = torch.zeros(nchains * p.Ltrot * p.Lq * 2, dtype=torch.float64, device="cuda")
+    phi[p.Ltrot * p.Lq * 2 + 5] = float("nan")   # chain 1
+    obs = torch.zeros(nchains * stride, dtype=torch.float64, device="cuda")
+    rc = lib.bafqmc_sweep_noalloc(C.byref(point_struct(p)), nchains, seeds.data_ptr(), phi.data_ptr(), 1,
+                                  obs.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == -1
+    assert b"chain 1" in lib.bafqmc_last_error()
