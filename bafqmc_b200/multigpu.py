@@ -64,3 +64,28 @@ def gather_rows(local_rows: np.ndarray, group=None) -> np.ndarray:
     out = [torch.zeros_like(pad) for _ in range(world)]
     dist.all_gather(out, pad, group=group)
     return torch.cat([o[: int(k)] for o, k in zip(out, ns)]).numpy()
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def _rank_entry(rank, fn, world, port, args):
+    import os
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    fn(rank, world, *args)
+
+
+def launch_ranks(fn, world: int, *args) -> None:
+    """Run fn(rank, world, *args) in `world` spawned processes on this node, one
+    per GPU, with RANK / LOCAL_RANK / WORLD_SIZE / MASTER_ADDR (127.0.0.1) /
+    MASTER_PORT set as torchrun sets them, so that fn may call
+    torch.distributed.init_process_group() with the env:// defaults.  Raises if
+    any rank fails."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_rank_entry, args=(fn, world, free_port(), args), nprocs=world, join=True,
+                       start_method="spawn")

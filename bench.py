@@ -604,11 +604,10 @@ def run_headline(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def _spawn_rank(local, args, world, port):
-    os.environ.update({"RANK": str(local), "LOCAL_RANK": str(local), "WORLD_SIZE": str(world),
-                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
-    os.environ.setdefault("NCCL_DEBUG", "INFO")
-    run_headline(args, local, world, local)
+def _bench_rank(rank, world, args):
+    import os
+    os.environ.setdefault("NCCL_DEBUG", "INFO")   # NCCL's init log shows the ranks and transports
+    run_headline(args, rank, world, rank)
 
 
 def main():
@@ -639,13 +638,9 @@ def main():
         run_reference(args, rank, int(env_world or 1))
         return
     if env_world is None and args.gpus > 1:
-        # no launcher: one process per GPU, spawned here
-        import torch.multiprocessing as mp
-        import socket
-        with socket.socket() as so:
-            so.bind(("127.0.0.1", 0))
-            port = so.getsockname()[1]
-        mp.spawn(_spawn_rank, args=(args, args.gpus, port), nprocs=args.gpus, join=True)
+        # no launcher: one process per GPU, spawned here (chains sharded by rank)
+        from bafqmc_b200.multigpu import launch_ranks
+        launch_ranks(_bench_rank, args.gpus, args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(env_world or 1)

@@ -63,3 +63,36 @@ def test_two_rank_reduce_and_gather_match_single_process():
 def test_single_rank_average_is_plain_mean():
     x = np.arange(12.0).reshape(3, 4)
     np.testing.assert_allclose(chain_average(x.sum(axis=0), 3, lambda b: b), x.mean(axis=0))
+
+
+def _launched(rank, world, out):
+    import torch
+    import torch.distributed as dist
+    from bafqmc_b200.multigpu import chain_average, shard, torch_all_reduce
+    dist.init_process_group("gloo")   # env:// from the launcher, as bench.py's ranks do with NCCL
+    try:
+        assert dist.get_rank() == rank and dist.get_world_size() == world
+        assert int(os.environ["LOCAL_RANK"]) == rank and os.environ["MASTER_ADDR"] == "127.0.0.1"
+        nchains = 4099
+        start, count = shard(nchains, rank, world)
+        local = np.arange(start, start + count, dtype=np.float64)
+        t = torch.tensor([float(count)])
+        dist.all_reduce(t)
+        out[rank] = (start, count, float(t.item()), chain_average(np.array([local.sum()]), count, torch_all_reduce()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_launcher_spawns_ranks_like_torchrun():
+    """bench.py --gpus N without torchrun uses multigpu.launch_ranks: each spawned
+    rank sees the torchrun environment, takes its shard of the job's chains and
+    joins the per-bin reduction."""
+    from bafqmc_b200.multigpu import launch_ranks
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    launch_ranks(_launched, 3, out)
+    assert sorted(out.keys()) == [0, 1, 2]
+    assert sum(out[r][1] for r in range(3)) == 4099
+    for r in range(3):
+        assert out[r][2] == 4099.0
+        np.testing.assert_allclose(out[r][3], [np.arange(4099).mean()], rtol=1e-14)
