@@ -1,29 +1,35 @@
-// Periodic 3x3x3 convolution of the 64-channel layers on the tensor cores
+// Periodic 3x3x3 convolutions of the proposer network on the tensor cores
 // (tcgen05.mma kind::f16, bf16 operands, float32 accumulators in tensor
-// memory), as an implicit GEMM: M = 128 output points, N = 64 output
-// channels, K = 27 taps x 64 input channels.
+// memory), as an implicit GEMM: M = 128 output points, N = the layer's output
+// channels (64, or 16 for the 4-channel output layer), K = 27 taps x the input
+// channels (8 planes of 8, or 2 planes for the 2-channel input and the output
+// layer's gradient).
 //
 // Tile: 4 consecutive sites x 32 consecutive time slices of one chain (M row
 // m = 32 * segment + slice offset).  For each of the 9 spatial offsets (b, c)
 // a stage holds, per segment s and 8-slice group g, the 10 rows t0 + 8g - 1 ..
-// t0 + 8g + 8 of the neighbour site's column (all 8 channel planes): one TMA
-// box of 8 channels x 10 rows x 8 planes (1280 bytes, laid out [plane][row]
-// [16 bytes]), placed at (4s + g) * 1280.  The three time offsets a of the
-// stage are then the same boxes read at a row offset 1 + a: a core matrix
-// (8 rows x 16 bytes) starts at box + plane * 160 + (1 + a) * 16, so the A
-// operand of tap (a, b, c) is the no-swizzle K-major layout with leading
-// (K, next plane) offset 160 bytes and stride (M, next 8-row group) offset
-// 1280 bytes.  The stage's three taps of weights, [tap][plane][64 rows][8],
-// arrive by one bulk copy (24 KB; K offset 1024, N offset 128).
+// t0 + 8g + 8 of the neighbour site's column (all PIN channel planes): one TMA
+// box of 8 channels x 10 rows x PIN planes (PIN * 160 bytes, laid out
+// [plane][row][16 bytes]), placed at (4s + g) * pitch with the pitch rounded
+// up to 128 bytes.  The three time offsets a of the stage are then the same
+// boxes read at a row offset 1 + a: a core matrix (8 rows x 16 bytes) starts
+// at box + plane * 160 + (1 + a) * 16, so the A operand of tap (a, b, c) is
+// the no-swizzle K-major layout with leading (K, next plane) offset 160 bytes
+// and stride (M, next 8-row group) offset = the pitch.  The stage's three taps
+// of weights, [tap][plane][N rows][8], arrive by one bulk copy (K offset
+// N * 16, N offset 128).
 //
 // Warp roles: warp 0 issues the copies (and owns the tensor memory), warp 1
 // the MMAs, warps 2-5 the epilogue (warp w reads tensor-memory lanes
 // 32 (w % 4) .. 32 (w % 4) + 31, i.e. rows of its lane quarter).  Stages are a
-// ring of kConvStages with full / empty mbarriers; the accumulator is double
-// buffered (2 x 64 columns), so a tile's epilogue overlaps the next tile's
-// MMAs.  Every wait is bounded: on expiry the kernel records status 1 in
-// *err, the other roles leave their loops, copies and MMAs in flight are
-// drained with bounded waits, and the tensor memory is released.
+// ring with full / empty mbarriers; the accumulator is double buffered
+// (2 x N columns), so a tile's epilogue overlaps the next tile's MMAs.
+// Epilogues: bias + ReLU into 8 bf16 planes (hidden layers), bias into the
+// float32 output [chain][t][site][4] (last layer), or the ReLU mask of the
+// previous layer into 8 bf16 planes (gradient pass).  Every wait is bounded:
+// on expiry the kernel records status 1 in *err, the other roles leave their
+// loops, copies and MMAs in flight are drained with bounded waits, and the
+// tensor memory is released.
 #pragma once
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -33,13 +39,26 @@
 
 namespace bq {
 
-constexpr int kConvStages = 4;
-constexpr int kConvBox = 1280;                   // 8 channels x 10 rows x 8 planes x 2 bytes
-constexpr int kConvABytes = 16 * kConvBox;       // 4 segments x 4 row groups
-constexpr int kConvBBytes = 3 * 8 * 64 * 16;     // 3 taps x 8 planes x 64 rows x 16 bytes
-constexpr int kConvStageBytes = kConvABytes + kConvBBytes;
 constexpr int kConvThreads = 192;
 constexpr long long kConvSpin = 1LL << 22;
+enum ConvTcMode { CTC_HIDDEN = 0, CTC_OUT = 1, CTC_BWD = 2 };
+
+template <int PIN, int NOUT>
+struct ConvTcCfg {
+    static constexpr int kBoxBytes = PIN * 160;                      // 8 channels x 10 rows x PIN planes x 2 B
+    static constexpr int kPitch = (kBoxBytes + 127) / 128 * 128;     // TMA destinations 128-byte aligned
+    static constexpr int kA = 16 * kPitch;                           // 4 segments x 4 row groups
+    static constexpr int kTapB = PIN * NOUT * 16;                    // one tap's weights
+    static constexpr int kB = 3 * kTapB;
+    static constexpr int kStage = kA + kB;
+    static constexpr int kTx = 16 * kBoxBytes + kB;                   // bytes the copies of a stage deliver
+    static constexpr int kStages = (200 * 1024) / kStage < 8 ? (200 * 1024) / kStage : 8;
+    static constexpr int kCols = 2 * NOUT < 32 ? 32 : 2 * NOUT;      // tensor-memory columns (power of 2)
+    static constexpr size_t kSmem = (size_t)kStages * kStage + 1024;
+    static_assert(kStage % 128 == 0 && kStages >= 2, "stage layout");
+    static_assert(NOUT == 16 || NOUT == 64, "N of the MMA");
+    static_assert(PIN == 2 || PIN == 8, "input planes");
+};
 
 __host__ __device__ constexpr uint32_t tc_idesc_bf16(int M, int N) {
     // F32 accumulator (bits 4-5 = 1), A and B bf16 (bits 7-9, 10-12 = 1), K-major
@@ -49,11 +68,12 @@ __host__ __device__ constexpr uint32_t tc_idesc_bf16(int M, int N) {
 struct ConvTcArgs {
     NetShape s;
     int chains;
-    const __nv_bfloat16* wt;     // [27][8][64][8] operand layout of this layer / direction
+    const __nv_bfloat16* wt;     // [27][PIN][NOUT][8] operand layout of this layer / direction
     const float* bias;           // forward: per output channel
+    int nbias;                   // real output channels (bias entries)
     const __nv_bfloat16* mask;   // backward: the layer input (ReLU mask), 8 planes
-    __nv_bfloat16* out;          // 8 planes, plane-major with halos
-    int bwd;
+    __nv_bfloat16* out;          // hidden / backward: 8 planes, plane-major with halos
+    float* outf;                 // last layer: [chain][t][site][4]
     int* err;
     long long spin;   // poll bound of every wait
     int skip_mma;     // test hook: issue no MMA, so that the waits on them expire
@@ -123,11 +143,13 @@ DEVI int nbr_site(const NetShape& s, int site, int bc) {
 
 }  // namespace convtc
 
+template <int PIN, int NOUT, int MODE>
 __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_constant__ CUtensorMap amap, ConvTcArgs a) {
+    using C = ConvTcCfg<PIN, NOUT>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte aligned base for the stages
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-    __shared__ uint64_t full[kConvStages], empty[kConvStages], tfull[2], tempty[2], drain;
+    __shared__ uint64_t full[C::kStages], empty[C::kStages], tfull[2], tempty[2], drain;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
     __shared__ float sbias[64];
@@ -138,7 +160,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        for (int i = 0; i < kConvStages; ++i) {
+        for (int i = 0; i < C::kStages; ++i) {
             mbar_init(smem_u32(&full[i]), 1);
             mbar_init(smem_u32(&empty[i]), 1);
         }
@@ -148,8 +170,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
         }
         mbar_init(smem_u32(&drain), 1);
     }
-    if (threadIdx.x < 64) sbias[threadIdx.x] = (!a.bwd && a.bias) ? a.bias[threadIdx.x] : 0.f;
-    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), 128);
+    if (threadIdx.x < 64)
+        sbias[threadIdx.x] = (MODE != CTC_BWD && a.bias && (int)threadIdx.x < a.nbias) ? a.bias[threadIdx.x] : 0.f;
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), C::kCols);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -171,17 +194,17 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                         break;
                     }
                     const uint32_t fb = smem_u32(&full[stage]);
-                    convtc::arrive_expect_tx(fb, kConvStageBytes);
-                    const uint32_t sa = smem_u32(smem + (size_t)stage * kConvStageBytes);
+                    convtc::arrive_expect_tx(fb, C::kTx);
+                    const uint32_t sa = smem_u32(smem + (size_t)stage * C::kStage);
                     for (int seg = 0; seg < 4; ++seg) {
                         const int col = b * s.Ns + convtc::nbr_site(s, 4 * sg + seg, bc);
                         for (int g = 0; g < 4; ++g)
-                            convtc::tma_load_4d(sa + (uint32_t)((4 * seg + g) * kConvBox), &amap, 0, tt * 32 + 8 * g, 0,
-                                                col, fb);
+                            convtc::tma_load_4d(sa + (uint32_t)((4 * seg + g) * C::kPitch), &amap, 0, tt * 32 + 8 * g,
+                                                0, col, fb);
                     }
-                    convtc::bulk_load(sa + kConvABytes, a.wt + (size_t)bc * (kConvBBytes / 2), kConvBBytes, fb);
+                    convtc::bulk_load(sa + C::kA, a.wt + (size_t)bc * (C::kB / 2), C::kB, fb);
                     ++issued;
-                    if (++stage == kConvStages) {
+                    if (++stage == C::kStages) {
                         stage = 0;
                         phase ^= 1u;
                     }
@@ -190,9 +213,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
             // drain: every issued stage's copies complete before the block exits
             int st = stage;
             uint32_t ph = phase;
-            for (int k = 0; k < min(issued, kConvStages); ++k) {
+            for (int k = 0; k < min(issued, C::kStages); ++k) {
                 if (--st < 0) {
-                    st = kConvStages - 1;
+                    st = C::kStages - 1;
                     ph ^= 1u;
                 }
                 volatile int never = 0;
@@ -202,7 +225,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
     } else if (warp == 1) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = tc_idesc_bf16(128, 64);
+            const uint32_t idesc = tc_idesc_bf16(128, NOUT);
             int stage = 0;
             uint32_t phase = 0;
             int acc = 0;
@@ -213,7 +236,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(acc * 64);
+                const uint32_t d = tmem + (uint32_t)(acc * NOUT);
                 bool ok = true;
                 for (int bc = 0; bc < 9; ++bc) {
                     if (!convtc::wait_bounded(smem_u32(&full[stage]), phase, &abort_flag, a.spin)) {
@@ -222,16 +245,17 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t sa = smem_u32(smem + (size_t)stage * kConvStageBytes);
-                    const uint32_t sb = sa + kConvABytes;
+                    const uint32_t sa = smem_u32(smem + (size_t)stage * C::kStage);
+                    const uint32_t sb = sa + C::kA;
                     for (int ta = 0; ta < 3 && !a.skip_mma; ++ta)
-                        for (int kk = 0; kk < 4; ++kk) {
-                            const uint64_t ad = tc_sdesc(sa + (uint32_t)(2 * kk * 160 + ta * 16), 160, kConvBox);
-                            const uint64_t bd = tc_sdesc(sb + (uint32_t)(ta * 8192 + 2 * kk * 1024), 1024, 128);
+                        for (int kk = 0; kk < PIN / 2; ++kk) {
+                            const uint64_t ad = tc_sdesc(sa + (uint32_t)(2 * kk * 160 + ta * 16), 160, C::kPitch);
+                            const uint64_t bd =
+                                tc_sdesc(sb + (uint32_t)(ta * C::kTapB + 2 * kk * NOUT * 16), NOUT * 16, 128);
                             convtc::mma_bf16(d, ad, bd, idesc, (bc | ta | kk) ? 1u : 0u);
                         }
                     if (!a.skip_mma) tc_commit(smem_u32(&empty[stage]));
-                    if (++stage == kConvStages) {
+                    if (++stage == C::kStages) {
                         stage = 0;
                         phase ^= 1u;
                     }
@@ -264,15 +288,21 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                 break;
             }
             tc_fence_after();
-            float v[64];
-            {
+            const uint32_t taddr = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * NOUT);
+            float v[NOUT];
+            if constexpr (NOUT == 64) {
                 float h[32];
-                convtc::tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * 64), h);
+                convtc::tmem_ld32(taddr, h);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = h[j];
-                convtc::tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * 64 + 32), h);
+                convtc::tmem_ld32(taddr + 32, h);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[32 + j] = h[j];
+            } else {
+                uint32_t r[16];
+                tmem_ld16(taddr, r);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
             }
             tc_fence_before();
             __syncwarp();
@@ -282,38 +312,44 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                 acc_phase ^= 1u;
             }
             const int site = 4 * sg + seg, t = tt * 32 + toff;
-            const long long rowbase = ((long long)b * s.Ns + site) * 8;   // plane 0 of the column
-            for (int q = 0; q < 8; ++q) {
-                float f[8];
-                if (a.bwd) {
-                    const uint4 mv =
-                        *reinterpret_cast<const uint4*>(a.mask + ((rowbase + q) * (s.L + 2) + t + 1) * 8);
-                    const __nv_bfloat162* mh = reinterpret_cast<const __nv_bfloat162*>(&mv);
+            if constexpr (MODE == CTC_OUT) {
+                float4 o = make_float4(v[0] + sbias[0], v[1] + sbias[1], v[2] + sbias[2], v[3] + sbias[3]);
+                *reinterpret_cast<float4*>(a.outf + (((long long)b * s.L + t) * s.Ns + site) * kNetOut) = o;
+            } else {
+                const long long rowbase = ((long long)b * s.Ns + site) * 8;   // plane 0 of the column
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const float2 mm = __bfloat1622float2(mh[k]);
-                        f[2 * k] = mm.x > 0.f ? v[8 * q + 2 * k] : 0.f;
-                        f[2 * k + 1] = mm.y > 0.f ? v[8 * q + 2 * k + 1] : 0.f;
+                for (int q = 0; q < 8; ++q) {
+                    float f[8];
+                    if constexpr (MODE == CTC_BWD) {
+                        const uint4 mv =
+                            *reinterpret_cast<const uint4*>(a.mask + ((rowbase + q) * (s.L + 2) + t + 1) * 8);
+                        const __nv_bfloat162* mh = reinterpret_cast<const __nv_bfloat162*>(&mv);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const float2 mm = __bfloat1622float2(mh[k]);
+                            f[2 * k] = mm.x > 0.f ? v[8 * q + 2 * k] : 0.f;
+                            f[2 * k + 1] = mm.y > 0.f ? v[8 * q + 2 * k + 1] : 0.f;
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) f[k] = fmaxf(v[8 * q + k] + sbias[8 * q + k], 0.f);
                     }
-                } else {
+                    uint4 o;
+                    __nv_bfloat162* oh = reinterpret_cast<__nv_bfloat162*>(&o);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) f[k] = fmaxf(v[8 * q + k] + sbias[8 * q + k], 0.f);
+                    for (int k = 0; k < 4; ++k) oh[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+                    __nv_bfloat16* col = a.out + (rowbase + q) * (s.L + 2) * 8;
+                    *reinterpret_cast<uint4*>(col + (t + 1) * 8) = o;
+                    if (t == 0) *reinterpret_cast<uint4*>(col + (s.L + 1) * 8) = o;
+                    if (t == s.L - 1) *reinterpret_cast<uint4*>(col) = o;
                 }
-                uint4 o;
-                __nv_bfloat162* oh = reinterpret_cast<__nv_bfloat162*>(&o);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) oh[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
-                __nv_bfloat16* col = a.out + (rowbase + q) * (s.L + 2) * 8;
-                *reinterpret_cast<uint4*>(col + (t + 1) * 8) = o;
-                if (t == 0) *reinterpret_cast<uint4*>(col + (s.L + 1) * 8) = o;
-                if (t == s.L - 1) *reinterpret_cast<uint4*>(col) = o;
             }
         }
     }
     __syncthreads();
     if (threadIdx.x == 0 && abort_flag) atomicOr(a.err, 1);
     tc_fence_after();
-    if (warp == 0) tmem_dealloc(tmem, 128);
+    if (warp == 0) tmem_dealloc(tmem, C::kCols);
 }
 
 }  // namespace bq

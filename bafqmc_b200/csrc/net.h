@@ -82,7 +82,7 @@ struct bafqmc_net {
     int data_chains = 0, data_slots = 0, data_used = 0;
     int* d_pairs = nullptr;      // [2 * cap] (input, target) configuration indices of a training batch
     uint64_t train_counter = 0;
-    int use_tc = 1;              // 64-channel layers on the tensor cores
+    int use_tc = 1;              // convolutions on the tensor cores (where conv_tc_applies)
     int* d_err = nullptr;        // status of the tensor-core kernels (bounded waits that expired)
     int wait_test = 0;           // bafqmc_net_set_wait_test: MMAs skipped, short wait bound
     // proposal bookkeeping of the move: log q(phi'|phi) and the Hastings term per chain
@@ -118,7 +118,7 @@ cudaError_t launch_pairs(bafqmc_net* n, int B, uint64_t seed, int lag);
 cudaError_t launch_collect(bafqmc_net* n, const KernelArgs& ka, int slot);
 // tensor-core convolution of layer l (forward, or the gradient pass if bwd)
 cudaError_t launch_conv_tc(bafqmc_net* n, int l, bool bwd, int chains);
-bool conv_tc_applies(const NetShape& s, int l);
+bool conv_tc_applies(const NetShape& s, int l, bool bwd);
 
 // the move on an ensemble: propose from ka's fields into kp's (seed advanced in ka),
 // then, after the forward pass at the proposal, the Hastings term

@@ -12,9 +12,9 @@
 //   the Gaussian mu - phi + exp(lsig) xi),
 // with periodic neighbours in t, y and x, bf16 weights and float32 accumulation.
 //
-// Kernels here run on the CUDA cores and serve every layer shape; the
-// 64-channel layers of the forward and transposed passes also have a
-// tensor-core path (conv_tc.cuh).
+// Kernels here run on the CUDA cores and serve every layer shape; every layer
+// of the forward pass and of the input-gradient pass also has a tensor-core
+// path (conv_tc.cuh) for width 64, sites a multiple of 4 and L a multiple of 32.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -519,7 +519,7 @@ cudaError_t net_forward(bafqmc_net* n, int chains) {
     const NetShape& s = n->shape;
     for (int l = 0; l < kNetLayers && e == cudaSuccess; ++l) {
         const bool last = l == kNetLayers - 1;
-        if (n->use_tc && conv_tc_applies(s, l))
+        if (n->use_tc && conv_tc_applies(s, l, false))
             e = launch_conv_tc(n, l, false, chains);
         else if (last)
             e = run_conv_ref<1>(conv_args(n, l, CONV_OUT), chains, n->stream);
@@ -554,7 +554,7 @@ cudaError_t net_backward(bafqmc_net* n, int chains) {
                                                     per);
         e = cudaGetLastError();
         if (e != cudaSuccess || l == 0) break;
-        if (n->use_tc && conv_tc_applies(s, l))
+        if (n->use_tc && conv_tc_applies(s, l, true))
             e = launch_conv_tc(n, l, true, chains);
         else
             e = run_conv_ref<16>(conv_args(n, l, CONV_BWD), chains, n->stream);
@@ -629,8 +629,9 @@ cudaError_t launch_learned_reverse(bafqmc_net* n, const KernelArgs& ka, const Ke
 // tensor-core convolution: host side
 namespace bq {
 
-bool conv_tc_applies(const NetShape& s, int l) {
-    return s.cin[l] == 64 && s.cout[l] == 64 && s.Ns % 4 == 0 && s.L % 32 == 0;
+bool conv_tc_applies(const NetShape& s, int l, bool bwd) {
+    if (s.width != 64 || s.Ns % 4 != 0 || s.L % 32 != 0) return false;
+    return bwd ? l >= 1 : true;   // the first layer's input gradient is never needed
 }
 
 namespace {
@@ -650,19 +651,30 @@ int sm_count(int device) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v < 1) v = 148;
     return v;
 }
+
+template <int PIN, int NOUT, int MODE>
+cudaError_t run_conv_tc(bafqmc_net* n, const CUtensorMap& map, const ConvTcArgs& a, int grid) {
+    using C = ConvTcCfg<PIN, NOUT>;
+    cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<PIN, NOUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)C::kSmem);
+    if (e != cudaSuccess) return e;
+    conv_tc_kernel<PIN, NOUT, MODE><<<grid, kConvThreads, C::kSmem, n->stream>>>(map, a);
+    return cudaGetLastError();
+}
 }  // namespace
 
 cudaError_t launch_conv_tc(bafqmc_net* n, int l, bool bwd, int chains) {
     const NetShape& s = n->shape;
-    if (!conv_tc_applies(s, l)) return cudaErrorInvalidValue;
+    if (!conv_tc_applies(s, l, bwd)) return cudaErrorInvalidValue;
     const __nv_bfloat16* A = bwd ? n->d_gact[l] : n->d_act[l];
+    const int pin = bwd ? s.pout[l] : s.pin[l];   // planes of the A operand
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     // 4-D view of the plane-major tensor: (channel in plane, row tp, plane, site column)
     CUtensorMap map;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)(s.L + 2), 8, (cuuint64_t)chains * s.Ns};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)(s.L + 2) * 16, (cuuint64_t)8 * (s.L + 2) * 16};
-    const cuuint32_t box[4] = {8, 10, 8, 1};
+    const cuuint64_t dims[4] = {8, (cuuint64_t)(s.L + 2), (cuuint64_t)pin, (cuuint64_t)chains * s.Ns};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)(s.L + 2) * 16, (cuuint64_t)pin * (s.L + 2) * 16};
+    const cuuint32_t box[4] = {8, 10, (cuuint32_t)pin, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(A), dims, strides,
                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -673,19 +685,20 @@ cudaError_t launch_conv_tc(bafqmc_net* n, int l, bool bwd, int chains) {
     a.chains = chains;
     a.wt = n->d_wt + n->wt_off[2 * l + (bwd ? 1 : 0)];
     a.bias = bwd ? nullptr : n->d_params + s.boff[l];
+    a.nbias = s.cout[l];
     a.mask = bwd ? n->d_act[l] : nullptr;
-    a.out = bwd ? n->d_gact[l - 1] : n->d_act[l + 1];
-    a.bwd = bwd ? 1 : 0;
+    a.out = bwd ? n->d_gact[l - 1] : (l + 1 < kNetLayers ? n->d_act[l + 1] : nullptr);
+    a.outf = n->d_out;
     a.err = n->d_err;
     a.spin = n->wait_test ? (1LL << 12) : kConvSpin;
     a.skip_mma = n->wait_test;
     const int ntiles = chains * (s.Ns / 4) * (s.L / 32);
     const int grid = std::min(ntiles, sm_count(n->device));
-    const size_t smem = (size_t)kConvStages * kConvStageBytes + 1024;
-    cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    conv_tc_kernel<<<grid, kConvThreads, smem, n->stream>>>(map, a);
-    return cudaGetLastError();
+    if (!bwd && l == 0) return run_conv_tc<2, 64, CTC_HIDDEN>(n, map, a, grid);
+    if (!bwd && l == kNetLayers - 1) return run_conv_tc<8, 16, CTC_OUT>(n, map, a, grid);
+    if (!bwd) return run_conv_tc<8, 64, CTC_HIDDEN>(n, map, a, grid);
+    if (l == kNetLayers - 1) return run_conv_tc<2, 64, CTC_BWD>(n, map, a, grid);
+    return run_conv_tc<8, 64, CTC_BWD>(n, map, a, grid);
 }
 
 }  // namespace bq
@@ -798,7 +811,7 @@ int bafqmc_net_create(int Lx, int Ly, int Ltrot, int width, int device, bafqmc_n
         cudaMalloc(&n->d_loss, sizeof(double)) != cudaSuccess || cudaMalloc(&n->d_err, sizeof(int)) != cudaSuccess ||
         cudaMemset(n->d_err, 0, sizeof(int)) != cudaSuccess)
         return bail(bq::net_fail(BAFQMC_ECUDA, "cudaMalloc network state"));
-    n->use_tc = bq::conv_tc_applies(s, 1) ? 1 : 0;
+    n->use_tc = bq::conv_tc_applies(s, 1, false) ? 1 : 0;
     *out = n;
     return BAFQMC_OK;
 }
@@ -842,7 +855,7 @@ int bafqmc_net_get_params(bafqmc_net* n, float* params) {
 
 int bafqmc_net_set_tensor_cores(bafqmc_net* n, int enable) {
     if (!n) return bq::net_fail(BAFQMC_EARG, "null network");
-    if (enable && !bq::conv_tc_applies(n->shape, 1))
+    if (enable && !bq::conv_tc_applies(n->shape, 1, false))
         return bq::net_fail(BAFQMC_EUNSUPPORTED,
                             "the tensor-core convolution needs width 64, sites a multiple of 4 and Ltrot a multiple of 32");
     n->use_tc = enable ? 1 : 0;
@@ -950,7 +963,7 @@ int bafqmc_net_time_layers(bafqmc_net* n, int chains, int reps, double* ms) {
         NCK(cudaEventRecord(ev[0], n->stream));
         for (int l = 0; l < bq::kNetLayers; ++l) {
             cudaError_t e;
-            if (n->use_tc && bq::conv_tc_applies(s, l)) e = bq::launch_conv_tc(n, l, false, chains);
+            if (n->use_tc && bq::conv_tc_applies(s, l, false)) e = bq::launch_conv_tc(n, l, false, chains);
             else if (l == bq::kNetLayers - 1) e = bq::run_conv_ref<1>(bq::conv_args(n, l, bq::CONV_OUT), chains, n->stream);
             else e = bq::run_conv_ref<16>(bq::conv_args(n, l, bq::CONV_HIDDEN), chains, n->stream);
             NCK(e);
