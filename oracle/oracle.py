@@ -109,6 +109,10 @@ class Params:
     RT: float = 1.0
     RDelta: float = 0.0
     pairing: bool = False
+    # Nambu propagator by scipy.linalg.expm instead of the reference's ZGEEV form
+    # (an exact exponential, for separating the reference's propagator error from
+    # the device's at points where G amplifies it)
+    exact_expm: bool = False
 
     @property
     def Lq(self) -> int:
@@ -302,6 +306,15 @@ class OperatorKinetic:
             # Nambu matrix is not Hermitian, so ZGEEV, the inverse eigenvector matrix and
             # exp(-+dtau w) on the eigenvalues.
             H = ham_T_pairing(p, latt)
+            if p.exact_expm:
+                from scipy.linalg import expm
+                w = np.linalg.eigvals(H)
+                self.energy_min = float(np.min(w.real))
+                self.energy_max = float(np.max(w.real))
+                self.bandwidth = self.energy_max - self.energy_min
+                self.expT_P = expm(-p.Dtau * H)
+                self.expT_M = expm(p.Dtau * H)
+                return
             w, V = np.linalg.eig(H)
             Vinv, _ = inv_and_det(V)
             self.energy_min = float(np.min(w.real))

@@ -6,12 +6,23 @@ with Delta = 0.5 is inside it; mu = -4 with Delta = 1 sits on its boundary.
 6x6 Nambu chains at beta = 8 are the largest Nambu points of the grid
 (2Ns = 72, L = 160).
 
-* Inside the condition (and at the boundary for beta = 2, where the fields do
-  not reach the pole in one sweep), the usual bar holds: seeds, fields and
-  counters bit-exact, G and every estimator within 1e-10.
-* On the boundary at beta = 4 a chain walks towards the pole in one sweep:
-  the oracle's ||G||_2 grows from about 2 to about 5e6.  A perturbation of
-  relative size eps of I - B moves G by about eps ||G||_2 ||I - B|| ~
+At mu = -4 the oracle is run with an exact exponential of the Nambu kinetic
+matrix (scipy.linalg.expm) in place of the reference's ZGEEV form: on the
+boundary (Delta = 1) the Bogoliubov matrix is nearly defective (its
+eigenvalues carry imaginary parts of 3e-8 that should vanish), the
+eigenvector form of e^{-dtau H} is wrong by 1e-2, and after one sweep the
+reference-form G of a chain differs from the exact one by 100%
+(tests/test_oracle_pairing.py pins that).  The device builds e^{-dtau H} by
+scaling and squaring, which agrees with expm to 4e-16.
+
+* At mu = -4, beta = 2 seeds, fields and counters are bit-exact against the
+  exact-propagator oracle.  One of the two chains walks towards a pole within
+  its first sweep (||G||_2 up to 2e6), where the oracle's own G moves by up to
+  1.4e-8 when its propagators carry 1e-15 noise; G and the estimators are
+  held to max(1e-10, 10x that sensitivity), measured in the test.
+* On the boundary at beta = 4 a chain walks towards the pole in one sweep
+  with the exact propagator too: ||G||_2 grows from about 4 to about 2e8.
+  A perturbation of relative size eps of I - B moves G by about
   eps ||G||_2^2 relative to ||G||, so no two FP64 implementations agree to
   1e-10 there.  The test reports ||G||_2 and the first divergence, and checks
   G within 1e-13 ||G||_2^2 (relative to max|G|) while the decisions still
@@ -23,6 +34,12 @@ import pytest
 from test_gpu_pairing import _run_both, assert_green_close, oracle_block, pair_params
 
 from oracle import oracle as O
+
+
+def exact(op):
+    """The same oracle parameters with the exact Nambu propagator."""
+    import dataclasses
+    return dataclasses.replace(op, exact_expm=True)
 
 pytestmark = pytest.mark.gpu
 
@@ -37,12 +54,65 @@ def solver_mod():
     return solver
 
 
+def _perturbed(op, seed, rng):
+    """An oracle chain whose propagators carry 1e-15 relative noise: how far its
+    G moves is what any FP64 implementation of this chain can resolve."""
+    _, opT, (ch,) = O.init_chains(op, seeds=[seed])
+    opT.expT_P = opT.expT_P * (1 + 1e-15 * rng.standard_normal(opT.expT_P.shape))
+    opT.expT_M = opT.expT_M * (1 + 1e-15 * rng.standard_normal(opT.expT_M.shape))
+    return ch
+
+
 @pytest.mark.parametrize("delta", [0.5, 1.0])
 def test_nambu_mu_minus4_beta2(solver_mod, delta):
+    """mu = -4, beta = 2, two chains, two bins, against the exact-propagator oracle.
+    Seeds, fields and counters bit-exact.  Chain 7001 walks towards a pole in
+    its first sweep (||G||_2 reaches 6e4 .. 2e6), where the oracle's own G moves
+    by up to 1.4e-8 under 1e-15 propagator noise; G and the estimators must
+    agree within max(1e-10, 10x that measured sensitivity)."""
+    from test_gpu_pairing import ATOL, PAIR_KEYS
     op, sp = pair_params(delta, mu=-4.0, Nlx=3, Nly=3, Ltrot=40, Beta=2.0, Nwrap=10)
-    ora = _run_both([op], [sp], [0, 0], [7001, 7002], nbins=2)
-    for _, ch in ora:
-        print("delta", delta, "||G||_2", np.linalg.norm(ch.prop.Gr, 2))
+    op = exact(op)
+    seeds = [7001, 7002]
+    rng = np.random.default_rng(5)
+    ora = []
+    for s in seeds:
+        latt, _, (ch,) = O.init_chains(op, seeds=[s])
+        ora.append((latt, ch, _perturbed(op, s, rng)))
+    ens = solver_mod.Ensemble([sp], [0, 0])
+    ens.fields_from_seeds(seeds)
+    for _, ch, chp in ora:
+        ch.pre()
+        chp.pre()
+    ens.pre()
+    for b in range(-1, 2):
+        if b >= 0:
+            for _, ch, chp in ora:
+                ch.sweep_bin()
+                chp.sweep_bin()
+            ens.sweep(1)
+        s_g, phis_g = ens.get_state()
+        cobs = ens.chain_obs() if b >= 0 else None
+        for c, (latt, ch, chp) in enumerate(ora):
+            Go, Gp = oracle_block(ch.prop.Gr, 9), oracle_block(chp.prop.Gr, 9)
+            scale = np.max(np.abs(Go))
+            sens = float(np.max(np.abs(Gp - Go)) / scale)
+            tol = max(1e-10, 10.0 * sens)
+            err = float(np.max(np.abs(ens.green(c) - Go)) / scale)
+            print(f"delta {delta} bin {b} chain {c}: ||G||_2 {np.linalg.norm(ch.prop.Gr, 2):.2e}, oracle sensitivity "
+                  f"{sens:.2e}, device G error {err:.2e}")
+            assert err <= tol, (b, c, err, tol)
+            assert int(s_g[c]) == ch.seed
+            np.testing.assert_array_equal(phis_g[c], ch.phi)
+            if b >= 0:
+                ref = ch.obs.as_dict(latt)
+                for k in PAIR_KEYS:
+                    np.testing.assert_allclose(np.atleast_1d(cobs[c][k]), np.atleast_1d(ref[k]), rtol=tol, atol=ATOL,
+                                               err_msg=f"bin {b} chain {c} {k}")
+    cnt = ens.counters()
+    for c, (_, ch, _) in enumerate(ora):
+        np.testing.assert_allclose(cnt[c, 0:2], ch.acc_sum, rtol=0, atol=0)
+    ens.close()
 
 
 def test_nambu_6x6_beta8(solver_mod):
@@ -53,6 +123,7 @@ def test_nambu_6x6_beta8(solver_mod):
 
 def test_nambu_boundary_beta4_divergence_is_reported(solver_mod):
     op, sp = pair_params(1.0, mu=-4.0, Nlx=3, Nly=3, Ltrot=80, Beta=4.0, Nwrap=10)
+    op = exact(op)
     seeds = [4242, 4243]
     ens = solver_mod.Ensemble([sp], [0, 0])
     ens.fields_from_seeds(seeds)
@@ -82,13 +153,13 @@ def test_nambu_boundary_beta4_divergence_is_reported(solver_mod):
 
 
 def test_mixed_12x12_near_the_band_edge(solver_mod):
-    """Mixed-precision slice products at 12x12, beta = 10, with mu = -3.5, half a
-    unit above the band edge (-3): G departs from the identity by O(0.1) (at
+    """Mixed-precision slice products at 12x12, beta = 10, with mu = -3.1, a tenth
+    above the band edge (-3): G departs from the identity by up to 3e-2 (at
     mu = -5 it differs from I by ~1e-9 and the G error says nothing).  G of the
     mixed chains after pre and after a sweep against G recomputed in FP64 from
     the same fields: within 1e-6."""
     from bafqmc_b200.params import SolverParams
-    p = SolverParams(U1=1.0, U2=-0.5, mu=-3.5, Nlx=12, Nly=12, Ltrot=200, Beta=10.0, NlxTherm=12, NlyTherm=12,
+    p = SolverParams(U1=1.0, U2=-0.5, mu=-3.1, Nlx=12, Nly=12, Ltrot=200, Beta=10.0, NlxTherm=12, NlyTherm=12,
                      LtrotTherm=200, Nwrap=10, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0)
     seeds = 99001 + 13 * np.arange(4)
     with solver_mod.Ensemble([p], np.zeros(len(seeds), dtype=np.int32)) as ens:
@@ -110,5 +181,5 @@ def test_mixed_12x12_near_the_band_edge(solver_mod):
         status = ens.counters()[:, 6].astype(np.int64)
     print(f"max |G - I| = {max(dev):.3e}, mixed G error vs FP64 = {max(errs):.3e}")
     assert not np.any(status & 5), status
-    assert min(dev) > 1e-2   # a point where G is not the identity
+    assert min(dev) > 1e-3   # a point where G is not the identity
     assert max(errs) <= 1e-6

@@ -27,7 +27,7 @@ import numpy as np
 import pytest
 from scipy.linalg import expm
 
-from oracle.oracle import Lattice, Params, run
+from oracle.oracle import Lattice, OperatorKinetic, Params, ham_T_pairing, run
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -197,3 +197,23 @@ def test_green_after_moves_is_exact():
     off[blk1] = 0.0
     off[blk2] = 0.0
     assert np.max(np.abs(off)) < 1e-10 * scale
+
+
+def test_reference_propagator_fails_on_the_finite_trace_boundary():
+    """The reference forms the Nambu e^{-dtau H} from ZGEEV eigenvectors
+    (src/pairing/src/non_interact.f90:131-178).  Inside mu < -3t - |Delta| that
+    agrees with an exact exponential to ~1e-15; on the boundary (mu = -4,
+    Delta = 1) the matrix is nearly defective and the eigenvector form is off
+    by more than 1e-3, so a chain's G there depends on the propagator's
+    construction, not only on the model.  (The device builds e^{-dtau H} by
+    scaling and squaring, which agrees with scipy's expm at both points.)"""
+    errs = {}
+    for delta, mu in [(0.3, -5.0), (0.5, -4.0), (1.0, -4.0)]:
+        p = Params(U1=1.0, U2=-0.5, mu=mu, Nlx=3, Nly=3, Ltrot=40, Beta=2.0, NlxTherm=3, NlyTherm=3,
+                     LtrotTherm=40, Nwrap=10, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0, RDelta=delta,
+                     pairing=True)
+        latt = Lattice(p)
+        kin = OperatorKinetic(p, latt)
+        errs[(delta, mu)] = float(np.max(np.abs(kin.expT_P - expm(-p.Dtau * ham_T_pairing(p, latt)))))
+    assert errs[(0.3, -5.0)] < 1e-13 and errs[(0.5, -4.0)] < 1e-13
+    assert errs[(1.0, -4.0)] > 1e-3
