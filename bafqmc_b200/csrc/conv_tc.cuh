@@ -8,14 +8,16 @@
 // Tile: 4 consecutive sites x 32 consecutive time slices of one chain (M row
 // m = 32 * segment + slice offset).  For each of the 9 spatial offsets (b, c)
 // a stage holds, per segment s and 8-slice group g, the 10 rows t0 + 8g - 1 ..
-// t0 + 8g + 8 of the neighbour site's column (all PIN channel planes): one TMA
-// box of 8 channels x 10 rows x PIN planes (PIN * 160 bytes, laid out
-// [plane][row][16 bytes]), placed at (4s + g) * pitch with the pitch rounded
-// up to 128 bytes.  The three time offsets a of the stage are then the same
-// boxes read at a row offset 1 + a: a core matrix (8 rows x 16 bytes) starts
-// at box + plane * 160 + (1 + a) * 16, so the A operand of tap (a, b, c) is
-// the no-swizzle K-major layout with leading (K, next plane) offset 160 bytes
-// and stride (M, next 8-row group) offset = the pitch.  The stage's three taps
+// t0 + 8g + 8 of the neighbour site's column (all PIN channel planes), laid out
+// [plane][row][16 bytes] (PIN * 160 bytes) at (4s + g) * PIN * 160.  One TMA
+// copy brings a segment's four groups: the tensor map views the plane-major
+// tensor as 5-D (channel in plane, row in group [10], plane, group [stride 8
+// rows, overlapping the row dimension], site column), box 8 x 10 x PIN x 4 x 1.
+// The three time offsets a of the stage are then the same rows read at a row
+// offset 1 + a: a core matrix (8 rows x 16 bytes) starts at
+// group + plane * 160 + (1 + a) * 16, so the A operand of tap (a, b, c) is the
+// no-swizzle K-major layout with leading (K, next plane) offset 160 bytes and
+// stride (M, next 8-row group) offset PIN * 160 bytes.  The stage's three taps
 // of weights, [tap][plane][N rows][8], arrive by one bulk copy (K offset
 // N * 16, N offset 128).
 //
@@ -46,8 +48,9 @@ enum ConvTcMode { CTC_HIDDEN = 0, CTC_OUT = 1, CTC_BWD = 2 };
 template <int PIN, int NOUT>
 struct ConvTcCfg {
     static constexpr int kBoxBytes = PIN * 160;                      // 8 channels x 10 rows x PIN planes x 2 B
-    static constexpr int kPitch = (kBoxBytes + 127) / 128 * 128;     // TMA destinations 128-byte aligned
-    static constexpr int kA = 16 * kPitch;                           // 4 segments x 4 row groups
+    static constexpr int kPitch = kBoxBytes;                         // one 8-row group; M stride of the operand
+    static constexpr int kSeg = 4 * kPitch;                          // one TMA box: a segment's 4 row groups
+    static constexpr int kA = 4 * kSeg;                              // 4 segments
     static constexpr int kTapB = PIN * NOUT * 16;                    // one tap's weights
     static constexpr int kB = 3 * kTapB;
     static constexpr int kStage = kA + kB;
@@ -55,7 +58,7 @@ struct ConvTcCfg {
     static constexpr int kStages = (200 * 1024) / kStage < 8 ? (200 * 1024) / kStage : 8;
     static constexpr int kCols = 2 * NOUT < 32 ? 32 : 2 * NOUT;      // tensor-memory columns (power of 2)
     static constexpr size_t kSmem = (size_t)kStages * kStage + 1024;
-    static_assert(kStage % 128 == 0 && kStages >= 2, "stage layout");
+    static_assert(kStage % 128 == 0 && kSeg % 128 == 0 && kStages >= 2, "stage layout (TMA boxes 128-byte aligned)");
     static_assert(NOUT == 16 || NOUT == 64, "N of the MMA");
     static_assert(PIN == 2 || PIN == 8, "input planes");
 };
@@ -100,11 +103,11 @@ DEVI void arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
 }
 DEVI void arrive(uint32_t mbar) { asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory"); }
-DEVI void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, uint32_t mbar) {
+DEVI void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4, uint32_t mbar) {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];" ::"r"(dst),
-        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+        "[%7];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(mbar)
         : "memory");
 }
 DEVI void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
@@ -196,11 +199,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_c
                     const uint32_t fb = smem_u32(&full[stage]);
                     convtc::arrive_expect_tx(fb, C::kTx);
                     const uint32_t sa = smem_u32(smem + (size_t)stage * C::kStage);
-                    for (int seg = 0; seg < 4; ++seg) {
+                    for (int seg = 0; seg < 4; ++seg) {   // one box: the segment's 4 groups of 10 rows
                         const int col = b * s.Ns + convtc::nbr_site(s, 4 * sg + seg, bc);
-                        for (int g = 0; g < 4; ++g)
-                            convtc::tma_load_4d(sa + (uint32_t)((4 * seg + g) * C::kPitch), &amap, 0, tt * 32 + 8 * g,
-                                                0, col, fb);
+                        convtc::tma_load_5d(sa + (uint32_t)(seg * C::kSeg), &amap, 0, 0, 0, tt * 4, col, fb);
                     }
                     convtc::bulk_load(sa + C::kA, a.wt + (size_t)bc * (C::kB / 2), C::kB, fb);
                     ++issued;

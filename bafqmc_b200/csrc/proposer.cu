@@ -670,13 +670,14 @@ cudaError_t launch_conv_tc(bafqmc_net* n, int l, bool bwd, int chains) {
     const int pin = bwd ? s.pout[l] : s.pin[l];   // planes of the A operand
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
-    // 4-D view of the plane-major tensor: (channel in plane, row tp, plane, site column)
+    // 5-D view of the plane-major tensor: (channel in plane, row in an 8-row group
+    // [10: the group and its two halo rows], plane, group [stride 8 rows], site column)
     CUtensorMap map;
-    const cuuint64_t dims[4] = {8, (cuuint64_t)(s.L + 2), (cuuint64_t)pin, (cuuint64_t)chains * s.Ns};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)(s.L + 2) * 16, (cuuint64_t)pin * (s.L + 2) * 16};
-    const cuuint32_t box[4] = {8, 10, (cuuint32_t)pin, 1};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(A), dims, strides,
+    const cuuint64_t dims[5] = {8, 10, (cuuint64_t)pin, (cuuint64_t)(s.L / 8), (cuuint64_t)chains * s.Ns};
+    const cuuint64_t strides[4] = {16, (cuuint64_t)(s.L + 2) * 16, 8 * 16, (cuuint64_t)pin * (s.L + 2) * 16};
+    const cuuint32_t box[5] = {8, 10, (cuuint32_t)pin, 4, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(A), dims, strides,
                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;

@@ -586,6 +586,74 @@ def stab_green(prop: Propagator, nt: int, ltrot: int, want_logdet: bool = False)
     return gr
 
 
+@dataclass
+class PropGreen:
+    """The time-displaced Green's functions (process_matrix.f90:17-24, 62-84):
+    Gr00 = G(0,0), Grtt = G(tau,tau), Grt0 = G(tau,0), Gr0t = G(0,tau), and the
+    drift maxima / sums of Wrap_tau (index 0: Gr0t, 1: Grt0, 2: Grtt, the order
+    Wrap_tau fills them, stabilization.f90:384-398)."""
+    n: int
+
+    def __post_init__(self):
+        self.Xmaxm = [0.0, 0.0, 0.0]
+        self.Xmeanm = [0.0, 0.0, 0.0]
+
+    def reset(self, gr: np.ndarray):
+        """Propgr_reset (process_matrix.f90:75-84)."""
+        self.Gr00 = gr.copy()
+        self.Grtt = gr.copy()
+        self.Grt0 = gr.copy()
+        self.Gr0t = -(np.eye(self.n, dtype=complex) - gr)
+
+
+def udv_unpivoted(a: np.ndarray):
+    """MyMats udv (src/common/mymats.f90:79-117): A = U diag(D) V by ZGEQRF without
+    pivoting, D = |diag R|, V = R / D row-wise, U from ZUNGQR."""
+    n = a.shape[0]
+    qr, tau, _, info = lapack.zgeqrf(np.asfortranarray(a), lwork=max(1, 64 * n))
+    if info != 0:
+        raise RuntimeError(f"zgeqrf info={info}")
+    d = np.abs(np.diag(qr)).astype(complex)
+    v = np.triu(qr) / d[:, None]
+    return _ungqr(qr, tau), d, v
+
+
+def stab_green_big(prop: Propagator, fermion_sign: bool = False):
+    """stabilization.f90:192-254: the 2N x 2N inverse whose blocks are G(0,0),
+    G(0,tau), G(tau,0), G(tau,tau), from the right factors of B(tau,0) and the left
+    factors of B(beta,tau).  Returns (Gr00, Gr0t, Grt0, Grtt).
+
+    The middle matrix is diag(VUL, UUR)^-1 K diag(VUR, UUL)^-1 with
+    K = [[I, s B(beta,tau)], [-B(tau,0), I]], whose inverse has top-left block
+    (I - s B(beta,0))^-1.  The reference puts +DUL in the top-right block
+    (stabilization.f90:206-209), i.e. s = -1, the fermion sign: its G(0,0) block
+    is (I + B)^-1, not the bosonic G = (I - B)^-1 of stab_green.  The default
+    here is the bosonic s = +1, consistent with the slice-by-slice propagation;
+    fermion_sign=True reproduces the reference's matrix."""
+    n = prop.n
+    inv = np.linalg.inv   # ZGETRF + ZGETRI (MyMats inv)
+    inv_ulur = inv(prop.UUL @ prop.UUR)
+    inv_vrvl = inv(prop.VUR @ prop.VUL)
+    big = np.zeros((2 * n, 2 * n), dtype=complex)
+    big[:n, :n] = inv_vrvl
+    big[n:, n:] = inv_ulur
+    for r in range(n):
+        big[r, r + n] = prop.DUL[r] if fermion_sign else -prop.DUL[r]
+        big[r + n, r] = -prop.DUR[r]
+    bu, bd, bv = udv_unpivoted(big)
+    left = np.zeros((2 * n, 2 * n), dtype=complex)
+    left[:n, :n] = inv(prop.VUR)
+    left[n:, n:] = inv(prop.UUL)
+    left = left @ inv(bv)
+    right = np.zeros((2 * n, 2 * n), dtype=complex)
+    right[:n, :n] = inv(prop.VUL)
+    right[n:, n:] = inv(prop.UUR)
+    right = inv(bu) @ right
+    left = left / bd[None, :]
+    tot = left @ right
+    return tot[:n, :n], tot[:n, n:], tot[n:, :n], tot[n:, n:]
+
+
 def compare_mat(a: np.ndarray, b: np.ndarray) -> float:
     """stabilization.f90:256-266 (L1 distance)."""
     return float(np.sum(np.abs(a - b)))
@@ -1074,6 +1142,51 @@ class Chain:
             self._drift(gr)
         wr.UR[st] = pr.UUR; wr.VR[st] = pr.VUR; wr.DR[st] = pr.DUR
 
+    # ---- time-displaced Green's functions (dynamics.f90:38-58, multiply.f90:48-97,
+    # Wrap_tau stabilization.f90:368-404), number-conserving chains
+    def tau_sweep_R(self, u2_slot_bug: bool = False, fermion_sign: bool = False, on_slice=None):
+        """Dyn_reset + Dyn_sweep_R at the start of a right traversal: G(tau,0),
+        G(0,tau) and G(tau,tau) propagated slice by slice from G(0,0), recomputed by
+        stab_green_big every Nwrap slices, the drifts recorded in self.pg.
+        The reference passes the U1 field slot to the U2 operator
+        (dynamics.f90:52); u2_slot_bug=True reproduces that, False uses the U2 slot.
+        fermion_sign=True uses the reference's stab_green_big matrix (see there).
+        on_slice(nt, pg) is called after each slice's stabilisation (a test hook)."""
+        import copy
+        p, o = self.p, self.opT
+        prop = copy.deepcopy(self.prop)          # Dyn_reset: Prop_d = Prop
+        if not hasattr(self, "pg"):
+            self.pg = PropGreen(p.Ndim)
+        pg = self.pg
+        pg.reset(self.prop.Gr)
+        for nt in range(1, p.Ltrot + 1):
+            for nf in (0, 1):
+                if not self.op[nf].active:
+                    continue
+                slot = 0 if (u2_slot_bug and nf == 1) else nf
+                ep = np.array([self._expalpha(nf, self.phi[nt - 1, ii, slot], 1) for ii in range(p.Ndim)])
+                em = np.array([self._expalpha(nf, self.phi[nt - 1, ii, slot], -1) for ii in range(p.Ndim)])
+                pg.Grt0 = ep[:, None] * pg.Grt0
+                pg.Gr0t = pg.Gr0t * em[None, :]
+                pg.Grtt = ep[:, None] * pg.Grtt * em[None, :]
+                prop.UUR = ep[:, None] * prop.UUR
+            pg.Grt0 = o.expT_P @ pg.Grt0
+            pg.Gr0t = pg.Gr0t @ o.expT_M
+            pg.Grtt = (o.expT_P @ pg.Grtt) @ o.expT_M
+            prop.UUR = o.expT_P @ prop.UUR
+            if nt % p.Nwrap == 0:
+                st = nt // p.Nwrap
+                prop.UUL = self.wr.UL[st].copy(); prop.VUL = self.wr.VL[st].copy(); prop.DUL = self.wr.DL[st].copy()
+                stab_UR(prop)
+                g00, g0t, gt0, gtt = stab_green_big(prop, fermion_sign)
+                for k, (new, old) in enumerate(((g0t, pg.Gr0t), (gt0, pg.Grt0), (gtt, pg.Grtt))):
+                    dif = compare_mat(new, old)
+                    pg.Xmaxm[k] = max(pg.Xmaxm[k], dif)
+                    pg.Xmeanm[k] += dif
+                pg.Gr00, pg.Gr0t, pg.Grt0, pg.Grtt = g00, g0t, gt0, gtt
+            if on_slice is not None:
+                on_slice(nt, pg)
+
     # ---- sweep schedule (local_sweep.f90:80-161)
     def pre(self):
         p, pr = self.p, self.prop
@@ -1103,8 +1216,10 @@ class Chain:
                 self.prop_L(0, nt - 1)
         self.wrap_L(0)
 
-    def sweep_R(self):
+    def sweep_R(self, tau: bool = False):
         p = self.p
+        if tau:   # Local_sweep_R's toggle (local_sweep.f90:119-123)
+            self.tau_sweep_R()
         self.wrap_R(0)
         for nt in range(1, p.Ltrot + 1):
             if self.op[0].active:
@@ -1116,8 +1231,9 @@ class Chain:
                 self.wrap_R(nt)
             self.measure()
 
-    def sweep_bin(self):
-        """Local_sweep%sweep with is_beta=.true. (local_sweep.f90:136-161)."""
+    def sweep_bin(self, tau: bool = False):
+        """Local_sweep%sweep with is_beta=.true. (local_sweep.f90:136-161); tau runs
+        the time-displaced pass at the start of each right traversal."""
         for o in self.op:
             o.reset()
             o.phase.reset()
@@ -1125,7 +1241,7 @@ class Chain:
         self.nobs = 0
         for _ in range(self.p.Nsweep):
             self.sweep_L()
-            self.sweep_R()
+            self.sweep_R(tau)
         self.obs.ave(self.nobs)
         for nf in (0, 1):
             if self.op[nf].active:
