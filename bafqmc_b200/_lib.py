@@ -64,6 +64,9 @@ SIGNATURES = {
     "bafqmc_log_weight": (C.c_int, [_P, _DP]),
     "bafqmc_pole_diagnostics": (C.c_int, [_P, _DP, C.c_int, _DP]),
     "bafqmc_set_precision": (C.c_int, [_P, C.c_int]),
+    "bafqmc_set_time_displaced": (C.c_int, [_P, C.c_int, C.c_int]),
+    "bafqmc_time_displaced_stats": (C.c_int, [_P, _DP, C.c_int]),
+    "bafqmc_time_displaced_probe": (C.c_int, [_P, C.c_int, _DP]),
     "bafqmc_stats_reset": (C.c_int, [_P, C.c_int, C.c_int]),
     "bafqmc_global_shift": (C.c_int, [_P, _DP, _IP]),
     "bafqmc_stats": (C.c_int, [_P, _DP, _DP, _IP]),

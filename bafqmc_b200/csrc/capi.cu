@@ -229,7 +229,14 @@ struct bafqmc_handle {
     int stats_block = 0, stats_max = 0, stats_in_block = 0, stats_blocks = 0;
     double* d_stats = nullptr;   // [npts*stride] x (current block sum, mean, sem, then stats_max block means)
     cudaGraphExec_t bin_graph = nullptr;
-    int graph_nsweep = 0, graph_timers = 0, graph_mixed = 0;
+    int graph_nsweep = 0, graph_timers = 0, graph_mixed = 0, graph_tau = 0, graph_probe = 0;
+    // time-displaced pass (bafqmc_set_time_displaced): the chains it runs, one
+    // matrix region per CTA, per-chain drift statistics, the optional probe
+    int tau_on = 0, tau_probe_nt = 0, tau_grid = 0;
+    int* d_tau_idx = nullptr;
+    double2* d_tau_ws = nullptr;
+    double* d_tau_stats = nullptr;
+    double2* d_tau_probe = nullptr;
 
     bq::KernelArgs args() const {
         bq::KernelArgs ka;
@@ -243,6 +250,12 @@ struct bafqmc_handle {
         ka.sc = d_sc;
         ka.timers = timers;
         ka.mixed = mixed;
+        if (tau_on) {
+            ka.tau_ws = d_tau_ws;
+            ka.tau_stats = d_tau_stats;
+            ka.tau_probe = tau_probe_nt > 0 ? d_tau_probe : nullptr;
+            ka.tau_probe_nt = tau_probe_nt;
+        }
         return ka;
     }
     bq::KernelArgs args2() const {   // the proposal state of the global moves
@@ -369,7 +382,8 @@ void free_handle(bafqmc_handle* h) {
     cudaSetDevice(h->device);
     void* ptrs[] = {h->d_pts, h->d_chains, h->d_mats, h->d_arena, h->d_phi, h->d_obs, h->d_sc,
                     h->d_pstart, h->d_plist, h->d_pout, h->d_tmp, h->d_pole, h->d_pole_mat, h->d_stats,
-                    h->d_arena2, h->d_phi2, h->d_sc2, h->d_fn2, h->d_acc};
+                    h->d_arena2, h->d_phi2, h->d_sc2, h->d_fn2, h->d_acc, h->d_tau_idx, h->d_tau_ws,
+                    h->d_tau_stats, h->d_tau_probe};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int c = 0; c < bq::kNumClasses; ++c)
@@ -690,13 +704,27 @@ int bafqmc_pre(bafqmc_handle* h) {
 
 namespace {
 // The launches of one bin: accumulator reset, nsweep persistent sweep launches
-// per kernel class, bin averages.
+// per kernel class, bin averages.  With the time-displaced pass on, each sweep
+// is a left-traversal launch, the pass, and a right-traversal launch
+// (Local_sweep_R's toggle, local_sweep.f90:119-123).
 cudaError_t record_bin(bafqmc_handle* h, int nsweep) {
     const bq::KernelArgs ka = h->args();
+    bq::KernelArgs kl = ka, kr = ka;
+    kl.traverse = 1;
+    kr.traverse = 2;
     cudaError_t e = bq::launch_bin_reset(ka, h->stream);
-    for (int s = 0; s < nsweep && e == cudaSuccess; ++s)
-        for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
-            e = bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
+    for (int s = 0; s < nsweep && e == cudaSuccess; ++s) {
+        if (h->tau_on) {
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, kl, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
+            if (e == cudaSuccess) e = bq::launch_tau(ka, h->d_tau_idx, h->nchains, h->tau_grid, h->stream);
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, kr, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
+        } else {
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
+        }
+    }
     if (e == cudaSuccess) e = bq::launch_bin_finish(ka, h->stream);
     return e;
 }
@@ -707,7 +735,8 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
     if (!h || nsweep < 1) return fail(BAFQMC_EARG, "bad sweep arguments");
     if (!h->pre_done) return fail(BAFQMC_ESTATE, "bafqmc_pre has not run");
     CK(cudaSetDevice(h->device));
-    if (!h->bin_graph || h->graph_nsweep != nsweep || h->graph_timers != h->timers || h->graph_mixed != h->mixed) {
+    if (!h->bin_graph || h->graph_nsweep != nsweep || h->graph_timers != h->timers || h->graph_mixed != h->mixed ||
+        h->graph_tau != h->tau_on || h->graph_probe != h->tau_probe_nt) {
         if (h->bin_graph) {
             CK(cudaGraphExecDestroy(h->bin_graph));
             h->bin_graph = nullptr;
@@ -729,6 +758,8 @@ int bafqmc_sweep(bafqmc_handle* h, int nsweep) {
         h->graph_nsweep = nsweep;
         h->graph_timers = h->timers;
         h->graph_mixed = h->mixed;
+        h->graph_tau = h->tau_on;
+        h->graph_probe = h->tau_probe_nt;
     }
     CK(cudaGraphLaunch(h->bin_graph, h->stream));
     h->bin_done = true;
@@ -1063,6 +1094,69 @@ int bafqmc_set_precision(bafqmc_handle* h, int mode) {
         return fail(BAFQMC_EARG,
                     "precision must be BAFQMC_PRECISION_FP64, BAFQMC_PRECISION_MIXED or BAFQMC_PRECISION_WAIT_TEST");
     h->mixed = mode;
+    return BAFQMC_OK;
+}
+
+int bafqmc_set_time_displaced(bafqmc_handle* h, int enable, int probe_nt) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    if (!enable) {
+        h->tau_on = 0;
+        h->tau_probe_nt = 0;
+        return BAFQMC_OK;
+    }
+    for (int c = 0; c < h->nchains; ++c) {
+        const PointHost& p = h->pts[h->chain_point[c]];
+        if (p.pairing)
+            return fail(BAFQMC_EUNSUPPORTED, "the time-displaced pass runs number-conserving chains only (chain " +
+                                                 std::to_string(c) + " is a Nambu chain)");
+        if (p.N > bq::kTauMaxN)
+            return fail(BAFQMC_EUNSUPPORTED, "the time-displaced pass needs N <= " + std::to_string(bq::kTauMaxN) +
+                                                 " (chain " + std::to_string(c) + " has N = " + std::to_string(p.N) + ")");
+        if (probe_nt < 0 || probe_nt > p.p.Ltrot)
+            return fail(BAFQMC_EARG, "probe slice outside 0..Ltrot");
+    }
+    CK(cudaSetDevice(h->device));
+    if (!h->d_tau_idx) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        h->tau_grid = std::max(1, std::min(sms, h->nchains));
+        std::vector<int> idx(h->nchains);
+        for (int c = 0; c < h->nchains; ++c) idx[c] = c;
+        CK(cudaMalloc(&h->d_tau_idx, sizeof(int) * h->nchains));
+        CK(cudaMemcpy(h->d_tau_idx, idx.data(), sizeof(int) * h->nchains, cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&h->d_tau_ws, sizeof(double2) * bq::tau_region_elems() * h->tau_grid));
+        CK(cudaMalloc(&h->d_tau_stats, sizeof(double) * bq::kTauStats * h->nchains));
+        CK(cudaMemset(h->d_tau_stats, 0, sizeof(double) * bq::kTauStats * h->nchains));
+    }
+    if (probe_nt > 0 && !h->d_tau_probe) {
+        CK(cudaMalloc(&h->d_tau_probe, sizeof(double2) * bq::kTauProbeElems * h->nchains));
+        CK(cudaMemset(h->d_tau_probe, 0, sizeof(double2) * bq::kTauProbeElems * h->nchains));
+    }
+    h->tau_on = 1;
+    h->tau_probe_nt = probe_nt;
+    return BAFQMC_OK;
+}
+
+int bafqmc_time_displaced_stats(bafqmc_handle* h, double* out, int reset) {
+    if (!h) return fail(BAFQMC_EARG, "null handle");
+    if (!h->d_tau_stats) return fail(BAFQMC_ESTATE, "the time-displaced pass has not been enabled");
+    CK(cudaSetDevice(h->device));
+    if (out)
+        CK(cudaMemcpyAsync(out, h->d_tau_stats, sizeof(double) * bq::kTauStats * h->nchains, cudaMemcpyDeviceToHost,
+                           h->stream));
+    if (reset) CK(cudaMemsetAsync(h->d_tau_stats, 0, sizeof(double) * bq::kTauStats * h->nchains, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return BAFQMC_OK;
+}
+
+int bafqmc_time_displaced_probe(bafqmc_handle* h, int chain, double* out) {
+    if (!h || !out || chain < 0 || chain >= h->nchains) return fail(BAFQMC_EARG, "bad probe arguments");
+    if (!h->d_tau_probe) return fail(BAFQMC_ESTATE, "no probe slice has been set");
+    const int n = h->pts[h->chain_point[chain]].N;
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(out, h->d_tau_probe + (size_t)chain * bq::kTauProbeElems, sizeof(double2) * 4 * n * n,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return BAFQMC_OK;
 }
 

@@ -21,7 +21,25 @@ struct KernelArgs {
     ChainScalars* sc;
     int timers;   // nonzero: accumulate per-phase SM cycles into ChainScalars::cyc
     int mixed;    // nonzero: slice products of the N <= 144 class on the tensor cores (3xTF32)
+    int traverse = 0;   // sweep_kernel: 0 both traversals, 1 the left one only, 2 the right one only
+    // time-displaced pass (tau_kernel): per-CTA matrix regions, per-chain drift
+    // statistics (kTauStats doubles), optional probe of the four functions at slice
+    // tau_probe_nt (kTauProbeElems complex values per chain)
+    double2* tau_ws = nullptr;
+    double* tau_stats = nullptr;
+    double2* tau_probe = nullptr;
+    int tau_probe_nt = 0;
 };
+
+// time-displaced pass of number-conserving chains with N <= kTauMaxN (2N x 2N
+// inverse in the N <= 144 routines).  Per chain: drift max of G(0,tau),
+// G(tau,0), G(tau,tau), their sums, passes run, non-finite recomputations.
+constexpr int kTauMaxN = 72;
+constexpr int kTauStats = 8;
+constexpr long long kTauProbeElems = 4LL * kTauMaxN * kTauMaxN;   // G(0,0), G(0,tau), G(tau,0), G(tau,tau)
+long long tau_region_elems();   // complex values of one CTA's matrix region
+// grid: CTAs (one per SM); each walks chains idx[k], k = blockIdx.x (mod grid)
+cudaError_t launch_tau(const KernelArgs& ka, const int* idx, int count, int grid, cudaStream_t st);
 
 // kernel classes of the fused sweep: size (N <= 16, N <= 36, N <= 72) + 3 * sector
 // (0 number-conserving, 1 Nambu), and class 6: number-conserving N <= 144

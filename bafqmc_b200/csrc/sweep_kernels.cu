@@ -1489,24 +1489,28 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
     __syncthreads();
     load_expT(x);
     lap(3);
-    // ---- left traversal
-    for (int nt = L; nt >= 1; --nt) {
-        if (nt % x.P().Nwrap == 0) {
-            wrap_L(x, nt);
-            lap(3);
+    // ---- left traversal (skipped by a right-only launch, which continues from
+    // the G, U_L and counters a left-only launch left in the arena)
+    if (ka.traverse != 2) {
+        for (int nt = L; nt >= 1; --nt) {
+            if (nt % x.P().Nwrap == 0) {
+                wrap_L(x, nt);
+                lap(3);
+            }
+            measure_any<NMAX, PAIR>(x);
+            lap(2);
+            slice_products<NMAX, true>(x);
+            lap(1);
+            if (x.P().active[1]) prop_any<NMAX, PAIR, true>(x, 1, nt - 1);
+            if (x.P().active[0]) prop_any<NMAX, PAIR, true>(x, 0, nt - 1);
+            lap(0);
         }
-        measure_any<NMAX, PAIR>(x);
-        lap(2);
-        slice_products<NMAX, true>(x);
-        lap(1);
-        if (x.P().active[1]) prop_any<NMAX, PAIR, true>(x, 1, nt - 1);
-        if (x.P().active[0]) prop_any<NMAX, PAIR, true>(x, 0, nt - 1);
-        lap(0);
+        wrap_L(x, 0);
+        sstore(n, Cfg<NMAX>::LD, x.A().ULc, x.U());
+        __syncthreads();
     }
-    wrap_L(x, 0);
-    sstore(n, Cfg<NMAX>::LD, x.A().ULc, x.U());
-    __syncthreads();
     // ---- right traversal
+    if (ka.traverse != 1) {
     sload(n, Cfg<NMAX>::LD, x.U(), x.A().URc);
     __syncthreads();
     wrap_R(x, 0);
@@ -1525,6 +1529,7 @@ __global__ void __launch_bounds__(Cfg<NMAX>::THREADS, Cfg<NMAX>::MINB) sweep_ker
         lap(2);
     }
     sstore(n, Cfg<NMAX>::LD, x.A().URc, x.U());
+    }
     sstore(n, Cfg<NMAX>::LD, x.A().G, x.G());
     flush_obs(x, ka.obs + (long)chain * ka.obs_stride);
     if (threadIdx.x == 0) {
@@ -1859,6 +1864,234 @@ __global__ void field_norm_kernel(KernelArgs ka, double* out) {
     for (long long k = threadIdx.x; k < tot; k += blockDim.x) v[0] += phi[k] * phi[k];
     block_sum<1>(v, red);
     if (threadIdx.x == 0) out[chain] = -0.5 * v[0];
+}
+
+// ---------------------------------------------------------------------------
+// Time-displaced Green's functions (Dyn_reset + Dyn_sweep_R, dynamics.f90:38-58;
+// propgrU_R / propgrT_R, multiply.f90:48-97; Wrap_tau and stab_green_big,
+// stabilization.f90:192-254, 368-404) of a number-conserving chain with
+// N <= 72, run between its left and right traversals (Local_sweep_R's toggle,
+// local_sweep.f90:119-123).  From G(0,0) and the left factors the left
+// traversal stored, G(tau,0) = B(tau,0) G, G(0,tau) = -(I - G) B(tau,0)^-1 and
+// G(tau,tau) = B(tau,0) G B(tau,0)^-1 are propagated slice by slice, and every
+// Nwrap slices recomputed from the stabilised factors as blocks of
+//   diag(V_R^-1, U_L^H) [[(V_R V_L)^-1, -D_L], [-D_R, (U_L U_R)^H]]^-1 diag(V_L^-1, U_R^H),
+// the inverse of [[I, -B(beta,tau)], [-B(tau,0), I]]; the L1 distance between
+// the propagated and the recomputed matrices is the drift Wrap_tau records.
+// Two departures from the reference, both deliberate: the U2 operator uses the
+// U2 field (dynamics.f90:52 passes the U1 field), and the 2N x 2N matrix has
+// the bosonic -D_L (stabilization.f90:206-209 has +D_L, whose inverse is the
+// fermionic (I + B)^-1 in its G(0,0) block).  The chain's own state is not
+// touched: the pass works on copies in its own region of global memory, with
+// the routines of the N <= 144 class (2N <= 144 rows).
+namespace taud {
+constexpr int LD = Cfg<144>::LD;
+constexpr long long MAT = 144LL * LD;   // complex values per matrix slot
+// slots of a chain's region; 0..4 are the N <= 144 context's W1, W2, G, U, S
+// (G holds G(0,0) of the pass, U the propagated right factor U_R)
+enum { GT0 = 5, G0T = 6, GTT = 7, VR = 8, BIG = 9, X = 10, VRI = 11, VLI = 12, UL = 13, VEC = 14, EP = 15, EM = 16, SLOTS = 17 };
+constexpr long long REGION = SLOTS * MAT;
+DEVI cplx* slot(const Ctx<144>& x, int k) { return x.wg + k * MAT; }
+}  // namespace taud
+
+long long tau_region_elems() { return taud::REGION; }
+
+// C <- A^-1 C for the x.n x x.n matrix A, which is destroyed: pivoted QR,
+// Q^H C, R^-1 D^-1, the row permutation back.
+COLD void tau_solve(Ctx<144>& x, cplx* A, cplx* C) {
+    qrp_any(x, A);
+    apply_qh_left_any(x, A, C);
+    cplx* rinv = reinterpret_cast<cplx*>(x.s.vn1());
+    double* dinv = x.s.u2();
+    diag_inverse(x.n, taud::LD, A, x.s.d(), rinv, dinv);
+    trsm_left_any(x, A, rinv, dinv, C);
+    permute_rows_any(x, C, false);
+}
+
+DEVI void tau_copy(int n, cplx* dst, const cplx* src) {   // both with leading dimension taud::LD
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        dst[r * taud::LD + c] = src[r * taud::LD + c];
+    }
+    __syncthreads();
+}
+
+// L1 distance of two n x n matrices (compare_mat, stabilization.f90:256-266),
+// valid in thread 0
+DEVI double tau_l1(Ctx<144>& x, int n, const cplx* a, const cplx* b) {
+    double v[1] = {0.0};
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        const cplx d = csub(a[r * taud::LD + c], b[r * taud::LD + c]);
+        v[0] += sqrt(d.x * d.x + d.y * d.y);
+    }
+    block_sum<1>(v, x.s.red());
+    return v[0];
+}
+
+// slice nt (1-based, propgrU_R then propgrT_R, multiply.f90:48-97): the HS
+// factors of both channels, then e^{-dtau K} from the left and e^{+dtau K} from
+// the right (real, in the EP and EM slots)
+COLD void tau_slice(Ctx<144>& x, int nt) {
+    constexpr int LD = taud::LD;
+    const int n = x.n;
+    const PointDev& P = x.P();
+    cplx *T0 = taud::slot(x, taud::GT0), *T1 = taud::slot(x, taud::G0T), *T2 = taud::slot(x, taud::GTT);
+    cplx* U = x.U();
+    cplx *ep = x.s.ean(), *em = x.s.ebn();
+    for (int ch = 0; ch < 2; ++ch) {
+        if (!P.active[ch]) continue;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            hs_factors(P.alpha_re[ch], P.alpha_im[ch], x.phi[((long)(nt - 1) * n + i) * 2 + ch], ep[i], em[i]);
+        __syncthreads();
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+            const int r = e / n, c = e - r * n;
+            T0[r * LD + c] = cmul(ep[r], T0[r * LD + c]);
+            T1[r * LD + c] = cmul(T1[r * LD + c], em[c]);
+            T2[r * LD + c] = cmul(cmul(ep[r], T2[r * LD + c]), em[c]);
+            U[r * LD + c] = cmul(ep[r], U[r * LD + c]);
+        }
+        __syncthreads();
+    }
+    const double *kp = reinterpret_cast<const double*>(taud::slot(x, taud::EP)),
+                 *km = reinterpret_cast<const double*>(taud::slot(x, taud::EM));
+    gemm_real_any<144, false>(x, T0, kp, T0);
+    gemm_real_any<144, true>(x, T1, T1, km);
+    gemm_real_any<144, false>(x, T2, kp, T2);
+    gemm_real_any<144, true>(x, T2, T2, km);
+    gemm_real_any<144, false>(x, U, kp, U);
+}
+
+// Wrap_tau at slice nt (stabilization.f90:368-404): stab_UR of the propagated
+// right factors, the 2N x 2N inverse, the drifts of G(0,tau), G(tau,0),
+// G(tau,tau) against the propagated ones (thread 0 accumulates them in dr:
+// max[3], sum[3], non-finite count), then the replacement.
+COLD void tau_wrap(Ctx<144>& x, const Arena& A, int nt, double* dr) {
+    using namespace taud;
+    const int n = x.n, st = nt / x.P().Nwrap;
+    cplx *W1 = x.W1(), *W2 = x.W2(), *U = x.U();
+    cplx *M = slot(x, BIG), *Xi = slot(x, X), *VRi = slot(x, VRI), *VLi = slot(x, VLI), *ULs = slot(x, UL);
+    stab_UR(x);                      // U = U_R, A.DRc = D_R, A.VRc and W2 = V_R
+    tau_copy(n, M, W2);
+    set_identity(n, LD, VRi);
+    __syncthreads();
+    tau_solve(x, M, VRi);            // V_R^-1
+    sload(n, LD, M, A.VLs(st));
+    set_identity(n, LD, VLi);
+    __syncthreads();
+    tau_solve(x, M, VLi);            // V_L^-1
+    sload(n, LD, ULs, A.ULs(st));
+    for (int e = threadIdx.x; e < 4 * n * n; e += blockDim.x) {
+        const int r = e / (2 * n), c = e - r * (2 * n);
+        M[r * LD + c] = cmk(0.0, 0.0);
+    }
+    __syncthreads();
+    gemm_any(x, M, op_n(VLi, LD), op_n(VRi, LD));               // (V_R V_L)^-1
+    gemm_any(x, M + n * LD + n, op_c(U, LD), op_c(ULs, LD));    // (U_L U_R)^H
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const cplx dl = A.DLs(st)[i], drv = A.DRc[i];
+        M[i * LD + n + i] = cmk(-dl.x, -dl.y);
+        M[(n + i) * LD + i] = cmk(-drv.x, -drv.y);
+    }
+    x.n = 2 * n;
+    set_identity(2 * n, LD, Xi);
+    __syncthreads();
+    tau_solve(x, M, Xi);
+    x.n = n;
+    // G(0,0) = V_R^-1 X00 V_L^-1
+    gemm_any(x, W1, op_n(VRi, LD), op_n(Xi, LD));
+    gemm_any(x, x.G(), op_n(W1, LD), op_n(VLi, LD));
+    // index 0: G(0,tau) = V_R^-1 X01 U_R^H; 1: G(tau,0) = U_L^H X10 V_L^-1; 2: G(tau,tau) = U_L^H X11 U_R^H
+    cplx* dst[3] = {slot(x, G0T), slot(x, GT0), slot(x, GTT)};
+    const MatOp left[3] = {op_n(VRi, LD), op_c(ULs, LD), op_c(ULs, LD)};
+    const cplx* blk[3] = {Xi + n, Xi + n * LD, Xi + n * LD + n};
+    const MatOp right[3] = {op_c(U, LD), op_n(VLi, LD), op_c(U, LD)};
+    for (int k = 0; k < 3; ++k) {
+        gemm_any(x, W1, left[k], op_n(blk[k], LD));
+        gemm_any(x, W2, op_n(W1, LD), right[k]);
+        const double dif = tau_l1(x, n, W2, dst[k]);
+        if (threadIdx.x == 0) {
+            if (dif == dif && dif <= 1.0e300) {
+                if (dif > dr[k]) dr[k] = dif;
+                dr[3 + k] += dif;
+            } else {
+                dr[6] += 1.0;
+            }
+        }
+        tau_copy(n, dst[k], W2);
+    }
+}
+
+// Dyn_reset + Dyn_sweep_R of one chain (dynamics.f90:37-57): copies of G and of
+// the right factors, L slices, a wrap every Nwrap slices; the arena's D_R and
+// V_R (which stab_UR updates) are put back at the end.
+COLD void tau_pass(Ctx<144>& x, const KernelArgs& ka, int chain) {
+    using namespace taud;
+    const int n = x.n, L = x.P().L;
+    const Arena A = x.A();
+    cplx *G = x.G(), *T0 = slot(x, GT0), *T1 = slot(x, G0T), *T2 = slot(x, GTT);
+    cplx *sv = slot(x, VEC), *svr = slot(x, VR);
+    gcopy(sv, A.DRc, n);
+    gcopy(svr, A.VRc, n * n);
+    sload_real(n, LD, reinterpret_cast<double*>(slot(x, EP)), x.P().expP);
+    sload_real(n, LD, reinterpret_cast<double*>(slot(x, EM)), x.P().expM);
+    sload(n, LD, G, A.G);
+    sload(n, LD, x.U(), A.URc);
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        const cplx g = G[r * LD + c];
+        T0[r * LD + c] = g;
+        T2[r * LD + c] = g;
+        T1[r * LD + c] = cmk(g.x - (r == c ? 1.0 : 0.0), g.y);   // -(I - G)
+    }
+    __syncthreads();
+    double dr[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int nt = 1; nt <= L; ++nt) {
+        tau_slice(x, nt);
+        if (nt % x.P().Nwrap == 0) tau_wrap(x, A, nt, dr);
+        if (nt == ka.tau_probe_nt && ka.tau_probe) {
+            cplx* pr = ka.tau_probe + (long long)chain * kTauProbeElems;
+            const cplx* src[4] = {G, T1, T0, T2};   // G(0,0), G(0,tau), G(tau,0), G(tau,tau)
+            for (int k = 0; k < 4; ++k) sstore(n, LD, pr + (long long)k * n * n, src[k]);
+        }
+    }
+    gcopy(A.DRc, sv, n);
+    gcopy(A.VRc, svr, n * n);
+    if (threadIdx.x == 0) {
+        double* o = ka.tau_stats + (long long)chain * kTauStats;
+        for (int k = 0; k < 3; ++k) {
+            o[k] = fmax(o[k], dr[k]);
+            o[3 + k] += dr[3 + k];
+        }
+        o[6] += 1.0;
+        o[7] += dr[6];
+    }
+    __syncthreads();
+}
+
+// One CTA per SM walks its share of the listed chains; its matrix region of
+// tau_region_elems() complex values is indexed by blockIdx.x.
+__global__ void __launch_bounds__(Cfg<144>::THREADS, 1) tau_kernel(KernelArgs ka, const int* idx, int count) {
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        const int chain = idx[k];
+        Ctx<144> x;
+        const bool ok = setup_ctx(x, ka, chain) && x.n <= kTauMaxN && !(x.sc->status & 1);
+        if (ok) {
+            x.wg = ka.tau_ws + (long long)blockIdx.x * taud::REGION;
+            tau_pass(x, ka, chain);
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_tau(const KernelArgs& ka, const int* idx, int count, int grid, cudaStream_t st) {
+    if (count <= 0) return cudaSuccess;
+    const size_t sm = Smem<144>::bytes();
+    const cudaError_t e = cudaFuncSetAttribute(tau_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    tau_kernel<<<grid < count ? grid : count, Cfg<144>::THREADS, sm, st>>>(ka, idx, count);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -178,6 +178,27 @@ class Ensemble:
         "wait_test" is the test hook of the products' bounded wait."""
         _lib.check(self.lib.bafqmc_set_precision(self.h, _lib.PRECISION[mode]))
 
+    def set_time_displaced(self, enable: bool = True, probe_nt: int = 0):
+        """Run the time-displaced pass (Dyn_sweep_R, dynamics.f90:44-57) in every
+        following sweep, between the left and right traversals; probe_nt in
+        1..Ltrot keeps the four functions of that slice (bafqmc_set_time_displaced)."""
+        _lib.check(self.lib.bafqmc_set_time_displaced(self.h, 1 if enable else 0, int(probe_nt)))
+
+    def time_displaced_stats(self, reset: bool = False) -> np.ndarray:
+        """[nchains, 8]: drift max of G(0,tau), G(tau,0), G(tau,tau), their sums,
+        passes run, non-finite recomputations (bafqmc_time_displaced_stats)."""
+        out = np.zeros((self.nchains, 8), dtype=np.float64)
+        _lib.check(self.lib.bafqmc_time_displaced_stats(self.h, _dptr(out), 1 if reset else 0))
+        return out
+
+    def time_displaced_probe(self, chain: int):
+        """(G(0,0), G(0,tau), G(tau,0), G(tau,tau)) of the chain at the probe slice."""
+        n = self.dims[self.chain_point[chain]][0]
+        out = np.zeros((4, n, n, 2), dtype=np.float64)
+        _lib.check(self.lib.bafqmc_time_displaced_probe(self.h, int(chain), _dptr(out)))
+        z = out[..., 0] + 1j * out[..., 1]
+        return z[0], z[1], z[2], z[3]
+
     def global_shift(self, shift) -> np.ndarray:
         """One global shift move per chain (bafqmc_global_shift): every field of
         channel ns shifted by (u - 1/2)|shift[ns]|, accepted by the exact weight
@@ -410,10 +431,11 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     run_dir = Path(run_dir)
     t0 = time.time()
     p = SolverParams.from_file(run_dir / "paramC_sets.txt", pairing=pairing)
-    if p.is_tau:
-        # dynamics.f90 (entered with is_tau, calc_basic.f90:56) is not part of this library
-        raise ParamError("is_tau = .true. asks for the time-displaced Green's functions (dynamics.f90), which this "
-                         "library does not compute; set is_tau = .false. (line 5 of paramC_sets.txt)")
+    if p.is_tau and (pairing or p.Ndim > 72):
+        # the time-displaced pass (dynamics.f90) is built for number-conserving chains with Ndim <= 72
+        raise ParamError("is_tau = .true. (line 5 of paramC_sets.txt) is supported for number-conserving runs with "
+                         f"Ndim <= 72 only (this run: {'Nambu' if pairing else 'Ndim = %d' % p.Ndim}); "
+                         "set is_tau = .false.")
     info = open(run_dir / "info.txt", "w")
     w = lambda label, v: info.write(f" {label:<47}:{_scalar(v)!r:>26}\n")
     if pairing:   # write_info (src/pairing/src/calc_basic.f90:140-180)
@@ -458,7 +480,11 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
         info.write(" Skipping Bosonic warm-up\n")
     ens.pre()
     seen = set()
+    istau = False
     for nbc in range(p.Nbin):
+        if nbc + 1 > p.Nthermal and p.is_tau and not istau:   # main.f90:49-50
+            istau = True
+            ens.set_time_displaced(True)
         ens.sweep(p.Nsweep)
         for c in ens.quarantined():
             if c not in seen:   # the reference has no counterpart: it would carry the NaN on
@@ -480,6 +506,16 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
                 if nprop > 0:
                     w(f"Phase_{name}_branch_pi_fraction", 0.0)
                 w(f"Phase_{name}_local_proposals", nprop)
+    if istau:
+        # Dyn_control_print (dynamics.f90:59-82): the sums are divided by chains * Nbin * Nst * Nsweep
+        # whatever Nthermal is, and the labels are those the reference prints: its
+        # Xmaxm(1..3) hold the drifts of G(0,tau), G(tau,0), G(tau,tau) in that order
+        # (stabilization.f90:384-398) while the lines name them GRtt, GRt0, GR0t.
+        ts = ens.time_displaced_stats()
+        norm = nchains * p.Nbin * p.Nst * p.Nsweep
+        for k, label in enumerate(("GRtt", "GRt0", "GR0t")):
+            w(f"Max diff {label}", float(ts[:, k].max()))
+            w(f"Mean diff {label}", float(ts[:, 3 + k].sum() / norm))
     quarantined = ens.quarantined()
     if quarantined:
         info.write(" non-finite Green's function, chains quarantined: "

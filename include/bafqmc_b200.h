@@ -300,6 +300,30 @@ int bafqmc_counters(bafqmc_handle* h, double* out);
 #define BAFQMC_PRECISION_WAIT_TEST 2
 int bafqmc_set_precision(bafqmc_handle* h, int mode);
 
+/* Time-displaced Green's functions, the is_tau option (calc_basic.f90:36,56;
+ * main.f90:50 enables it after Nthermal bins).  With enable set, each sweep of
+ * bafqmc_sweep runs Dyn_reset + Dyn_sweep_R (dynamics.f90:37-57) between its
+ * left and right traversals (local_sweep.f90:119-123): from G(0,0) the pass
+ * propagates G(tau,0), G(0,tau) and G(tau,tau) slice by slice and every Nwrap
+ * slices recomputes them from the stabilised factors (Wrap_tau,
+ * stabilization.f90:368-404), recording the L1 drift of each.  The Markov chain
+ * is unchanged (the pass works on copies).  Number-conserving chains with
+ * N <= 72 only (BAFQMC_EUNSUPPORTED otherwise).  The U2 operator uses the U2
+ * field and the 2N x 2N matrix the bosonic sign; dynamics.f90:52 passes the U1
+ * field to the U2 operator and stabilization.f90:206-209 use the fermion sign,
+ * both of which this library does not reproduce.
+ * probe_nt in 1..Ltrot keeps the four functions of slice probe_nt of the last
+ * pass for bafqmc_time_displaced_probe; 0 keeps none. */
+int bafqmc_set_time_displaced(bafqmc_handle* h, int enable, int probe_nt);
+/* out (optional): [nchains][8] = drift max of G(0,tau), G(tau,0), G(tau,tau)
+ * (Wrap_tau's Xmaxm(1..3)), drift sums of the same (Xmeanm before the
+ * division), passes run, non-finite recomputations; reset zeroes them after
+ * the copy. */
+int bafqmc_time_displaced_stats(bafqmc_handle* h, double* out, int reset);
+/* out: 4 row-major N x N complex matrices (interleaved re, im) of the chain:
+ * G(0,0), G(0,tau), G(tau,0), G(tau,tau) at the probe slice of the last pass. */
+int bafqmc_time_displaced_probe(bafqmc_handle* h, int chain, double* out);
+
 /* Per-phase SM cycle counters of the sweep kernel (the reference has only a
  * total wall time, main.f90:26-27,67-71).  enable switches counting for the
  * following sweeps; out (optional) receives [nchains][4] accumulated cycles:

@@ -95,13 +95,16 @@ def test_rank_leaving_ends_the_next_bin_reduction_with_an_error():
     assert out[0].startswith("error"), out[0]
 
 
-def test_time_displaced_request_is_refused(tmp_path):
-    """is_tau = .true. (calc_basic.f90:56) asks for dynamics.f90's time-displaced
-    Green's functions, which this library does not compute: the run directory
-    refuses it before any device work, instead of ignoring the flag."""
+def test_time_displaced_request_outside_its_range_is_refused(tmp_path):
+    """is_tau = .true. (calc_basic.f90:56) runs the time-displaced pass of
+    dynamics.f90, built here for number-conserving chains with Ndim <= 72: a
+    12x12 run (Ndim 144) is refused before any device work, instead of
+    ignoring the flag."""
+    import dataclasses
     from bafqmc_b200.params import ParamError
     from bafqmc_b200.solver import run_directory
-    text = params().to_text().splitlines()
+    p = dataclasses.replace(params(), Nlx=12, Nly=12, NlxTherm=12, NlyTherm=12)
+    text = p.to_text().splitlines()
     text[4] = ".true. 10"
     (tmp_path / "paramC_sets.txt").write_text("\n".join(text) + "\n")
     with pytest.raises(ParamError, match="is_tau"):
