@@ -469,69 +469,199 @@ DEVI bool metro_ratio(cplx d, double rg, double u, cplx gjj, cplx& coef) {
     return accept;
 }
 
-// The deferred rank-KB pass of prop_channel on one TR x TC tile at (r0, c0):
-// the block's rank-1 terms (coefficients, rows and columns staged in shared
-// memory) on the tile's elements outside the block's rows and columns.
-template <int NMAX>
-DEVI void rank_block_tile(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb, int r0, int c0) {
-    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
+// prop_channel visits the sites of a channel in blocks of KB.  Per block:
+//  1. lead_block: one warp makes the block's Metropolis decisions in visiting
+//     order on the block's kb x kb submatrix of G, held in registers, applying
+//     each accepted rank-1 term to the submatrix (no barrier per site);
+//  2. block_vectors: the full update vectors of the block from the recorded
+//     coefficients and block values;
+//  3. rank_tile / rank_rows: G += sum_m X_m Y_m^T on every element.
+// The rank-1 term of a site i (localU.f90:56-71, ZGERU) is
+// G <- G + coef G(:,i) (e_i - G(i,:))^T.  For any diagonal E it satisfies
+// F_i(E G E^-1) = E F_i(G) E^-1, and coef depends only on G(i,i), which E
+// leaves unchanged, so the wraps of the sites (row i by e^{a phi_i}, column i
+// by e^{-a phi_i} before the decision in the right traversal, with the old
+// field; row i by e^{-a phi_i} and column i by e^{a phi_i} after it in the left
+// traversal, with the final field) commute with the updates and are applied
+// once, as one diagonal similarity, in the last block's rank pass.
+
+static_assert(Cfg<16>::KB * Cfg<16>::KB <= 16 && Cfg<36>::KB * Cfg<36>::KB <= 16 && Cfg<72>::KB * Cfg<72>::KB <= 16 &&
+                  Cfg<144>::KB * Cfg<144>::KB <= 16,
+              "the block records (tau, delta2, the vn1 | vn2 snapshot) hold KB x KB values in NMAX >= 16 entries, "
+              "and the lead warp one element per lane");
+
+// the channel's deferred wrap: factor of row r and of column c
+template <int NMAX, bool LEFT>
+DEVI cplx wrap_row(const Smem<NMAX>& s, int r) {
+    if constexpr (LEFT) return s.accf()[r] ? s.ebn()[r] : s.ebo()[r];
+    else return s.eao()[r];
+}
+template <int NMAX, bool LEFT>
+DEVI cplx wrap_col(const Smem<NMAX>& s, int c) {
+    if constexpr (LEFT) return s.accf()[c] ? s.ean()[c] : s.eao()[c];
+    else return s.ebo()[c];
+}
+
+// Step 1, by the lead warp (the site strip's first warp).  Lane l < KB*KB holds
+// the element (l / KB, l % KB) of the block's kb x kb submatrix of the current
+// G; the decisions run in visiting order, every lane computing the same
+// Metropolis ratio from the diagonal element it receives by shuffle.  Records
+// per visited slot m: coef (coef()), X_m on the later block sites (xb = tau(),
+// [m][a], a > m) and Y_m on them (yb = delta2(), [m][b], b > m), where
+// X_m = coef G_{m-1}(:, i_m) and Y_m = e_{i_m} - G_{m-1}(i_m, :)^T.  Only the
+// trailing submatrix (sites after m) is updated: nothing later reads the
+// rest.  A rejected site has coef = 0, so its update adds exact zeros.
+
+// the submatrix at block start k0 into the QR norm vectors (vn1 | vn2, free
+// during local updates); the lead warp reads it back after the barrier, when
+// the rank pass may already be writing G
+template <int NMAX, bool LEFT>
+DEVI void block_snapshot(const Smem<NMAX>& s, const cplx* G, int n, int k0, int kb) {
+    constexpr int KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
+    const int lane = threadIdx.x & 31;
+    if (lane < KB * KB) {
+        const int a = lane / KB, b = lane % KB;
+        const int sa = LEFT ? n - 1 - (k0 + min(a, kb - 1)) : k0 + min(a, kb - 1);
+        const int sb = LEFT ? n - 1 - (k0 + min(b, kb - 1)) : k0 + min(b, kb - 1);
+        reinterpret_cast<cplx*>(s.vn1())[lane] = (a < kb && b < kb) ? G[sa * LD + sb] : cmk(0.0, 0.0);
+    }
+}
+
+DEVI cplx shfl_c(cplx v, int src) {
+    return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// The snapshot, the previous block's kbp rank terms (in the order and with the
+// operations of the rank pass, so the lanes hold exactly the G the pass
+// writes there), then the decisions.  Returns the accepted count.
+template <int NMAX, bool LEFT>
+COLD long long lead_block(Ctx<NMAX> x, int n, int k0, int kb, int kbp) {
+    constexpr int KB = Cfg<NMAX>::KB;
     const auto& s = x.s;
-    cplx g[TR][TC];
-    bool own[TR][TC];
+    const int lane = threadIdx.x & 31;
+    const bool own = lane < KB * KB;
+    const int a = own ? lane / KB : KB - 1, b = lane % KB;
+    cplx* xb = s.tau();
+    cplx* yb = s.delta2();
+    cplx g = reinterpret_cast<const cplx*>(s.vn1())[a * KB + b];
+    if (kbp > 0 && a < kb && b < kb) {
+        const int sa = LEFT ? n - 1 - (k0 + a) : k0 + a, sb = LEFT ? n - 1 - (k0 + b) : k0 + b;
 #pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-        for (int b = 0; b < TC; ++b) {
-            const int r = r0 + a, c = c0 + b;
-            own[a][b] = r < n && c < n && (unsigned)(r - slo) >= (unsigned)kb &&
-                        (unsigned)(c - slo) >= (unsigned)kb;
-            g[a][b] = G[min(r, n - 1) * LD + min(c, n - 1)];
+        for (int m = 0; m < KB; ++m) {
+            if (m >= kbp) break;
+            g = cfma(s.col(m)[sa], s.row(m)[sb], g);
         }
+    }
+    long long nacc = 0;
 #pragma unroll
     for (int m = 0; m < KB; ++m) {
         if (m >= kb) break;
-        const cplx cf = s.coef()[m];
+        const int i = LEFT ? n - 1 - (k0 + m) : k0 + m;
+        const cplx gmm = shfl_c(g, m * KB + m);
+        const cplx gam = shfl_c(g, a * KB + m);
+        const cplx gmb = shfl_c(g, m * KB + b);
+        cplx coef;
+        const bool accept = metro_ratio(s.delta()[i], s.rg()[i], s.u2()[i], gmm, coef);
+        const cplx xv = cmul(coef, gam);
+        const cplx yv = cmk(-gmb.x, -gmb.y);
+        if (a > m && b > m) g = cfma(xv, yv, g);
+        if (own && b == m && a > m) xb[m * KB + a] = xv;
+        if (own && a == m && b > m) yb[m * KB + b] = yv;
+        if (lane == 0) {
+            s.accf()[i] = accept ? 1 : 0;
+            s.coef()[m] = coef;
+        }
+        nacc += accept ? 1 : 0;
+    }
+    return nacc;
+}
+
+// Step 2.  X_k(r) = coef_k (G(r, i_k) + sum_{j<k} X_j(r) Y_j(i_k)) into col(k),
+// Y_k(c) = delta(c, i_k) - (G(i_k, c) + sum_{j<k} X_j(i_k) Y_j(c)) into row(k);
+// threads 0..n-1 build the X rows, n..2n-1 the Y columns.
+template <int NMAX, bool LEFT>
+DEVI void block_vectors(const Ctx<NMAX>& x, const cplx* G, int n, int k0, int kb) {
+    constexpr int KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
+    const auto& s = x.s;
+    const cplx* xb = s.tau();
+    const cplx* yb = s.delta2();
+    for (int t = threadIdx.x; t < 2 * n; t += blockDim.x) {
+        const bool isx = t < n;
+        const int v = isx ? t : t - n;
+        cplx acc[KB];
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            if (k >= kb) break;
+            const int ik = LEFT ? n - 1 - (k0 + k) : k0 + k;
+            cplx a = isx ? G[v * LD + ik] : G[ik * LD + v];
+#pragma unroll
+            for (int j = 0; j < k; ++j) a = isx ? cfma(acc[j], yb[j * KB + k], a) : cfma(xb[j * KB + k], acc[j], a);
+            if (isx) {
+                acc[k] = cmul(s.coef()[k], a);
+                s.col(k)[v] = acc[k];
+            } else {
+                acc[k] = cmk((v == ik ? 1.0 : 0.0) - a.x, -a.y);
+                s.row(k)[v] = acc[k];
+            }
+        }
+    }
+}
+
+// Step 3 on one TR x TC tile at (r0, c0): G(r,c) += sum_m X_m(r) Y_m(c), then
+// (WRAP, the channel's last block) the deferred wrap.  Rejected slots have
+// X_m = 0 and add exact zeros; coef() is not read (the lead thread is already
+// writing the next block's coefficients).
+template <int NMAX, bool LEFT, bool WRAP>
+DEVI void rank_tile(const Ctx<NMAX>& x, cplx* G, int n, int kb, int r0, int c0) {
+    constexpr int TR = Cfg<NMAX>::TR, TC = Cfg<NMAX>::TC, KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD;
+    const auto& s = x.s;
+    cplx g[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) g[a][b] = G[min(r0 + a, n - 1) * LD + min(c0 + b, n - 1)];
+#pragma unroll
+    for (int m = 0; m < KB; ++m) {
+        if (m >= kb) break;
         cplx cr[TR], y[TC];
 #pragma unroll
-        for (int a = 0; a < TR; ++a) cr[a] = cmul(cf, s.col(m)[min(r0 + a, n - 1)]);
+        for (int a = 0; a < TR; ++a) cr[a] = s.col(m)[min(r0 + a, n - 1)];
 #pragma unroll
-        for (int b = 0; b < TC; ++b) {
-            const cplx yv = s.row(m)[min(c0 + b, n - 1)];
-            y[b] = cmk(-yv.x, -yv.y);
-        }
+        for (int b = 0; b < TC; ++b) y[b] = s.row(m)[min(c0 + b, n - 1)];
 #pragma unroll
         for (int a = 0; a < TR; ++a)
 #pragma unroll
             for (int b = 0; b < TC; ++b) g[a][b] = cfma(cr[a], y[b], g[a][b]);
     }
+    if constexpr (WRAP) {
+        cplx fb[TC];
+#pragma unroll
+        for (int b = 0; b < TC; ++b) fb[b] = wrap_col<NMAX, LEFT>(s, min(c0 + b, n - 1));
+#pragma unroll
+        for (int a = 0; a < TR; ++a) {
+            const cplx fa = wrap_row<NMAX, LEFT>(s, min(r0 + a, n - 1));
+#pragma unroll
+            for (int b = 0; b < TC; ++b) g[a][b] = cmul(cmul(g[a][b], fa), fb[b]);
+        }
+    }
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
         for (int b = 0; b < TC; ++b)
-            if (own[a][b]) G[(r0 + a) * LD + c0 + b] = g[a][b];
+            if (r0 + a < n && c0 + b < n) G[(r0 + a) * LD + c0 + b] = g[a][b];
 }
 
-// The deferred rank-KB pass of prop_channel for the classes whose G lives in
-// HBM/L2.  Items are (32-column chunk, PR-row block): a warp's load or store of
-// one row of an item is a coalesced 512-byte segment, where TR x TC tiles of
-// adjacent threads touched a dozen cache lines per load.  (Loading a warp's
-// next item before computing the current one measured slower.)  The block
-// columns are first scaled by their coefficients in place (the strip no longer
-// reads them), with the arithmetic of rank_block_tile, so every element takes
-// the same operations in the same order.
-template <int NMAX>
-DEVI void rank_pass_rows(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb) {
+// Step 3 for the classes whose G lives in HBM/L2.  Items are (32-column chunk,
+// PR-row block): a warp's load or store of one row of an item is a coalesced
+// 512-byte segment.  Warp w (of nw, the lead's warp excluded) takes items
+// w, w + nw, ...
+template <int NMAX, bool LEFT, bool WRAP>
+DEVI void rank_rows(const Ctx<NMAX>& x, cplx* G, int n, int kb, int w, int nw) {
     constexpr int KB = Cfg<NMAX>::KB, LD = Cfg<NMAX>::LD, PR = 9;
-    auto& s = x.s;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kb * n; e += blockDim.x) {
-        const int m = e / n, r = e - m * n;
-        s.col(m)[r] = cmul(s.coef()[m], s.col(m)[r]);
-    }
-    __syncthreads();
-    const int lane = tid & 31, nw = blockDim.x >> 5;
+    const auto& s = x.s;
+    const int lane = threadIdx.x & 31;
     const int nch = (n + 31) >> 5, items = nch * ((n + PR - 1) / PR);
-    for (int it = tid >> 5; it < items; it += nw) {
+    for (int it = w; it < items; it += nw) {
         const int c = (it % nch) * 32 + lane, rb = (it / nch) * PR;
         if (c >= n) continue;
         cplx g[PR];
@@ -540,18 +670,19 @@ DEVI void rank_pass_rows(const Ctx<NMAX>& x, cplx* G, int n, int slo, int kb) {
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
             if (m >= kb) break;
-            const cplx yv = s.row(m)[c];
-            const cplx y = cmk(-yv.x, -yv.y);
+            const cplx y = s.row(m)[c];
             const cplx* cr = s.col(m);
 #pragma unroll
             for (int a = 0; a < PR; ++a) g[a] = cfma(cr[min(rb + a, n - 1)], y, g[a]);
         }
-        const bool cok = (unsigned)(c - slo) >= (unsigned)kb;
+        if constexpr (WRAP) {
+            const cplx fb = wrap_col<NMAX, LEFT>(s, c);
 #pragma unroll
-        for (int a = 0; a < PR; ++a) {
-            const int r = rb + a;
-            if (cok && r < n && (unsigned)(r - slo) >= (unsigned)kb) G[r * LD + c] = g[a];
+            for (int a = 0; a < PR; ++a) g[a] = cmul(cmul(g[a], wrap_row<NMAX, LEFT>(s, min(rb + a, n - 1))), fb);
         }
+#pragma unroll
+        for (int a = 0; a < PR; ++a)
+            if (rb + a < n) G[(rb + a) * LD + c] = g[a];
     }
 }
 
@@ -590,129 +721,45 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     }
     __syncthreads();
 
-    const int ncg = (n + TC - 1) / TC, nrg = (n + TR - 1) / TR;
-    const bool act = tid < ncg * nrg;
-    const int r0 = act ? (tid / ncg) * TR : 0, c0 = act ? (tid % ncg) * TC : 0;
-
-    // The block's sites run on the first two warps (named barrier 1) with the
-    // block's rows and columns in registers: thread t holds column t of the block
-    // rows (ra) and row t of the block columns (ca, for t outside the block).
-    // Registers are kept in visiting order (slot q = q-th site of the block), and
-    // the site loop is unrolled, so every register index is a constant.  A site
-    // costs one barrier: threads stage the site's row and column, load every
-    // operand of the site into registers, make the same Metropolis decision
-    // and update their own registers.
-    // The rank-1 term is ZGERU's x(i) alpha y(j): grouped x(i) (alpha y(j)) on
-    // the block rows and (x(i) alpha) y(j) on the block columns.
-    constexpr int NB = Cfg<NMAX>::NB;
-    long long nacc = 0;   // accepted proposals, counted by thread 0
+    // Blocks of KB sites in visiting order.  The lead warp (the site strip's first
+    // warp) decides block b + 1 while the other warps run block b's rank pass: it
+    // copies block b + 1's submatrix during block b's vector step (G is not
+    // written then) and adds block b's terms itself, exactly as the pass does.  The last block's pass applies the channel's deferred wrap.
+    constexpr int NT = Cfg<NMAX>::THREADS;
+    const bool lead = tid == 32 * x.sw0;
+    const int warp = tid >> 5;
+    const bool lwarp = warp == x.sw0;
+    const int rt = tid - (warp > x.sw0 ? 32 : 0);   // rank-pass thread index (lead warp excluded)
+    const int ncg = (n + TC - 1) / TC, ntiles = ncg * ((n + TR - 1) / TR);
+    long long nacc = 0;   // accepted proposals, counted by the lead
+    if (lwarp) {
+        block_snapshot<NMAX, LEFT>(s, G, n, 0, min(KB, n));
+        __syncwarp();
+        const long long c = lead_block<NMAX, LEFT>(x, n, 0, min(KB, n), 0);
+        if (lead) nacc += c;
+    }
+    __syncthreads();
     for (int k0 = 0; k0 < n; k0 += KB) {
-        const int kb = min(KB, n - k0);
-        const int slo = LEFT ? n - k0 - kb : k0;   // block sites are slo .. slo+kb-1
-        const int t = tid - 32 * x.sw0;
-        if ((unsigned)t < (unsigned)NB) {
-            const bool tv = t < n;
-            const bool tin = (unsigned)(t - slo) < (unsigned)kb;
-            // site of slot q
-#define SITE(q) (LEFT ? n - 1 - (k0 + (q)) : k0 + (q))
-            cplx ra[KB], ca[KB];
-#pragma unroll
-            for (int q = 0; q < KB; ++q) {
-                const int sq = SITE(q);
-                ra[q] = (tv && q < kb) ? G[sq * LD + t] : cmk(0.0, 0.0);
-                ca[q] = (tv && q < kb && !tin) ? G[t * LD + sq] : cmk(0.0, 0.0);
-            }
-#pragma unroll
-            for (int m = 0; m < KB; ++m) {
-                if (m < kb) {
-                    const int i = SITE(m);
-                    const bool ti = (t == i);
-                    cplx* xr = s.col(m);
-                    cplx* yr = s.row(m);
-                    const cplx ea = s.eao()[i], eb = s.ebo()[i];
-                    if (!LEFT) {   // right sweep: wrap site i first (row i by ea, then column i by eb)
-                        ra[m] = cmul(ra[m], ea);
-                        if (ti) {
-#pragma unroll
-                            for (int q = 0; q < KB; ++q) ra[q] = cmul(ra[q], eb);
-                        }
-                        if (!tin) ca[m] = cmul(ca[m], eb);
-                    }
-                    // stage: y(t) = G(i,t); x(t) = G(t,i) outside the block; thread i stages x inside it
-                    const cplx yt = ra[m], xt = ca[m];
-                    if (tv) {
-                        yr[t] = yt;
-                        if (!tin) xr[t] = xt;
-                        if (ti) {
-#pragma unroll
-                            for (int q = 0; q < KB; ++q)
-                                if (q < kb) xr[SITE(q)] = ra[q];
-                        }
-                    }
-                    asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");
-                    // every operand of this site in registers before any arithmetic
-                    const cplx yii = yr[i];
-                    const cplx dl = s.delta()[i];
-                    const double rgv = s.rg()[i], uv = s.u2()[i];
-                    cplx xq[KB], yq[KB];
-#pragma unroll
-                    for (int q = 0; q < KB; ++q) {
-                        xq[q] = (q < kb) ? xr[SITE(q)] : cmk(0.0, 0.0);
-                        yq[q] = (q < kb) ? yr[SITE(q)] : cmk(0.0, 0.0);
-                    }
-                    cplx ean = ea, ebn = eb;
-                    if (LEFT) {
-                        ean = s.ean()[i];
-                        ebn = s.ebn()[i];
-                    }
-                    cplx coef;
-                    const bool accept = metro_ratio(dl, rgv, uv, yii, coef);
-                    if (accept && tv) {
-                        // block rows, column t: temp = coef * (delta(t,i) - y(t))
-                        const cplx cy = cmul(coef, cmk((ti ? 1.0 : 0.0) - yt.x, -yt.y));
-#pragma unroll
-                        for (int q = 0; q < KB; ++q)
-                            if (q < kb) ra[q] = cfma(xq[q], cy, ra[q]);
-                        // row t, block columns: (x(t) coef) (delta(c,i) - y(c))
-                        if (!tin) {
-                            const cplx xc = cmul(xt, coef);
-#pragma unroll
-                            for (int q = 0; q < KB; ++q)
-                                if (q < kb) ca[q] = cfma(xc, cmk(((q == m) ? 1.0 : 0.0) - yq[q].x, -yq[q].y), ca[q]);
-                        }
-                    }
-                    if (LEFT) {   // left sweep: wrap site i with its final field (column i, then row i)
-                        const cplx eaf = accept ? ean : ea;
-                        const cplx ebf = accept ? ebn : eb;
-                        if (ti) {
-#pragma unroll
-                            for (int q = 0; q < KB; ++q) ra[q] = cmul(ra[q], eaf);
-                        }
-                        if (!tin) ca[m] = cmul(ca[m], eaf);
-                        ra[m] = cmul(ra[m], ebf);
-                    }
-                    // the coefficient for the deferred pass, the flag for the field write-back
-                    if (t == 0) {
-                        s.accf()[i] = accept ? 1 : 0;
-                        s.coef()[m] = coef;
-                        nacc += accept ? 1 : 0;
-                    }
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < KB; ++q) {
-                const int sq = SITE(q);
-                if (tv && q < kb) G[sq * LD + t] = ra[q];
-                if (tv && q < kb && !tin) G[t * LD + sq] = ca[q];
-            }
-#undef SITE
-        }
+        const int kb = min(KB, n - k0), k1 = k0 + KB, kb1 = min(KB, n - k1);
+        const bool more = k1 < n;
+        block_vectors<NMAX, LEFT>(x, G, n, k0, kb);
+        if (lwarp && more) block_snapshot<NMAX, LEFT>(s, G, n, k1, kb1);
         __syncthreads();
-        // the block's rank-1 terms on the elements outside its rows and columns
-        if constexpr (Cfg<NMAX>::GG) {
-            rank_pass_rows<NMAX>(x, G, n, slo, kb);
-        } else if (act) {
-            rank_block_tile<NMAX>(x, G, n, slo, kb, r0, c0);
+        if (lwarp) {
+            if (more) {
+                const long long c = lead_block<NMAX, LEFT>(x, n, k1, kb1, kb);
+                if (lead) nacc += c;
+            }
+        } else if constexpr (Cfg<NMAX>::GG) {
+            const int w = warp - (warp > x.sw0 ? 1 : 0), nw = NT / 32 - 1;
+            if (more) rank_rows<NMAX, LEFT, false>(x, G, n, kb, w, nw);
+            else rank_rows<NMAX, LEFT, true>(x, G, n, kb, w, nw);
+        } else {
+            for (int tt = rt; tt < ntiles; tt += NT - 32) {
+                const int r0 = (tt / ncg) * TR, c0 = (tt % ncg) * TC;
+                if (more) rank_tile<NMAX, LEFT, false>(x, G, n, kb, r0, c0);
+                else rank_tile<NMAX, LEFT, true>(x, G, n, kb, r0, c0);
+            }
         }
         __syncthreads();
     }

@@ -481,6 +481,7 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     ens.pre()
     seen = set()
     istau = False
+    tau_record = {}
     for nbc in range(p.Nbin):
         if nbc + 1 > p.Nthermal and p.is_tau and not istau:   # main.f90:49-50
             istau = True
@@ -512,6 +513,8 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
         # Xmaxm(1..3) hold the drifts of G(0,tau), G(tau,0), G(tau,tau) in that order
         # (stabilization.f90:384-398) while the lines name them GRtt, GRt0, GR0t.
         ts = ens.time_displaced_stats()
+        tau_record = {"tau_passes": int(ts[:, 6].sum()), "tau_drift_max": [float(ts[:, k].max()) for k in range(3)],
+                      "tau_nonfinite": int(ts[:, 7].sum())}
         norm = nchains * p.Nbin * p.Nst * p.Nsweep
         for k, label in enumerate(("GRtt", "GRt0", "GR0t")):
             w(f"Max diff {label}", float(ts[:, k].max()))
@@ -531,7 +534,7 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
         "chain_sweeps_per_s": nchains * p.Nbin * p.Nsweep / elapsed,
         "acceptance": [float(cnt[:, ch].sum() / (nchains * p.Nbin)) for ch in (0, 1)],
         "drift_max": float(cnt[:, 4].max()), "quarantined_chains": quarantined,
-        "status": [int(v) for v in cnt[:, 6]],
+        "status": [int(v) for v in cnt[:, 6]], **tau_record,
     }
     (run_dir / "run_record.json").write_text(json.dumps(record, indent=1) + "\n")
     seeds, phis = ens.get_state()

@@ -97,3 +97,34 @@ def test_binary_checkpoint_round_trip_and_resume(solver_mod, tmp_path):
         solver_mod.run_directory(d, nchains=2, log=lambda *a: None)
         runs[name] = ((d / "density_total").read_text(), (d / "confout.txt").read_text())
     assert runs["txt"] == runs["npz"]
+
+
+def test_time_displaced_run_directory(solver_mod, tmp_path):
+    """is_tau = .true. with Nthermal = 1 over 3 bins (main.f90:49-50): the pass
+    runs in bins 2 and 3 only, info.txt gets Dyn_control_print's six lines
+    (dynamics.f90:74-79) after the acceptance lines, and the Markov chain (the
+    checkpoint) is that of the same run without the pass, bit for bit."""
+    import json
+    import dataclasses
+    out = {}
+    for tau in (False, True):
+        d = tmp_path / ("tau" if tau else "plain")
+        d.mkdir()
+        p = dataclasses.replace(point(nbin=3), is_tau=tau, Nthermal=1)
+        (d / "paramC_sets.txt").write_text(p.to_text())
+        (d / "confin.txt").write_text("0\n")
+        (d / "seeds.txt").write_text("41\n42\n")
+        solver_mod.run_directory(d, nchains=2, log=lambda *a: None)
+        out[tau] = d
+    assert (out[False] / "confout.txt").read_text() == (out[True] / "confout.txt").read_text()
+    lines = (out[True] / "info.txt").read_text().splitlines()
+    labels = [ln.split(":")[0].strip() for ln in lines]
+    want = ["Max diff GRtt", "Mean diff GRtt", "Max diff GRt0", "Mean diff GRt0", "Max diff GR0t", "Mean diff GR0t"]
+    i = labels.index("Max diff GRtt")
+    assert labels[i:i + 6] == want
+    assert labels[i - 1] == "Accept_U2_shift" and labels[i + 6] == "Max diff Matrix"
+    vals = [float(lines[i + k].split(":")[1]) for k in range(6)]
+    assert all(0 < v < 1e-8 for v in vals), vals
+    assert "Max diff GRtt" not in (out[False] / "info.txt").read_text()
+    rec = json.loads((out[True] / "run_record.json").read_text())
+    assert rec["tau_passes"] == 2 * 2 and rec["tau_nonfinite"] == 0
