@@ -619,7 +619,11 @@ def run_headline(args, rank, world, local):
                          "than the FP64 N<=36 class the arms use (mixed_at_6x6); proposer network bf16 with f32 "
                          "accumulation on tcgen05",
             "g_maxabs_err_vs_fp64": 0.0,
-            "mixed_at_6x6": dict(mixed, ms_per_chain_sweep_fp64_class_used=plain["ms_per_step"] / plain["chains_per_gpu"]),
+            "mixed_at_6x6": dict(
+                mixed, ms_per_chain_sweep_fp64_class_used=plain["ms_per_step"] / plain["chains_per_gpu"],
+                # the plain sampler's ESS/s on one GPU with the mixed products (148 chains fill the class's one
+                # CTA per SM), at the plain chain's tau_int
+                ess_per_s_plain_sampler_mixed=(1e3 / mixed["ms_per_chain_sweep_mixed"]) / (2.0 * plain["tau_int_max"])),
             "l2": "working set 1.5 MB/chain x chains >> 126 MB L2 (no flush needed)",
             "learned": {k: v for k, v in learned.items() if k not in ("e2e", "clocks")},
             "plain": plain,

@@ -145,3 +145,24 @@ def test_expired_product_wait_falls_back_to_fp64_exactly(solver_mod):
     for c in range(len(seeds0)):
         np.testing.assert_array_equal(out["wait_test"][1][c], out["fp64"][1][c])
         np.testing.assert_array_equal(out["wait_test"][2][c], out["fp64"][2][c])
+
+
+def test_6x6_beta8_in_the_tensor_core_class(solver_mod):
+    """The 6x6, beta = 8 point (L = 160) run in the N <= 144 class, the one with
+    the tensor-core slice products, at mu = -3.1 (G departs from I by 8e-2):
+    G after bafqmc_pre and after two mixed sweeps against FP64 from the same
+    fields.  (The bench's mixed_at_6x6 line times the same configuration.)"""
+    p = point(6, 6, 160, 8.0, mu=-3.1)
+    seeds = [21, 22, 23, 24]
+    with solver_mod.Ensemble([p], np.zeros(len(seeds), dtype=np.int32), classes=[6]) as ens:
+        ens.set_precision("mixed")
+        ens.fields_from_seeds(seeds)
+        ens.pre()
+        errs = [max_green_error(solver_mod, ens, p)]
+        for _ in range(2):
+            ens.sweep(1)
+            errs.append(max_green_error(solver_mod, ens, p))
+        status = ens.counters()[:, 6].astype(np.int64)
+    print("6x6 mixed G error vs FP64:", errs)
+    assert not np.any(status & 5), status
+    assert max(errs) <= G_TOL
