@@ -1932,44 +1932,51 @@ __global__ void field_norm_kernel(KernelArgs ka, double* out) {
 // touched: the pass works on copies in its own region of global memory, with
 // the routines of the N <= 144 class (2N <= 144 rows).
 namespace taud {
-constexpr int LD = Cfg<144>::LD;
-constexpr long long MAT = 144LL * LD;   // complex values per matrix slot
-// slots of a chain's region; 0..4 are the N <= 144 context's W1, W2, G, U, S
+// The pass of an N <= 36 chain runs in the N <= 72 class's context (2N <= 72;
+// G and U in shared memory, register-resident factorisations), that of a
+// 36 < N <= 72 chain in the N <= 144 class's.  Matrices of the region have the
+// class's leading dimension.
+template <int NMAX> constexpr int LD = Cfg<NMAX>::LD;
+template <int NMAX> constexpr long long MAT = (long long)NMAX * Cfg<NMAX>::LD;   // complex values per slot
+// slots of a CTA's region; 0..4 are the class context's W1, W2 (and, N <= 144, G, U, S)
 // (G holds G(0,0) of the pass, U the propagated right factor U_R)
 enum { GT0 = 5, G0T = 6, GTT = 7, VR = 8, BIG = 9, X = 10, VRI = 11, VLI = 12, UL = 13, VEC = 14, EP = 15, EM = 16, SLOTS = 17 };
-constexpr long long REGION = SLOTS * MAT;
-DEVI cplx* slot(const Ctx<144>& x, int k) { return x.wg + k * MAT; }
+constexpr long long REGION = SLOTS * MAT<144>;   // the larger class's region serves both
+template <int NMAX> DEVI cplx* slot(const Ctx<NMAX>& x, int k) { return x.wg + k * MAT<NMAX>; }
 }  // namespace taud
 
 long long tau_region_elems() { return taud::REGION; }
 
 // C <- A^-1 C for the x.n x x.n matrix A, which is destroyed: pivoted QR,
 // Q^H C, R^-1 D^-1, the row permutation back.
-COLD void tau_solve(Ctx<144>& x, cplx* A, cplx* C) {
+template <int NMAX>
+COLD void tau_solve(Ctx<NMAX>& x, cplx* A, cplx* C) {
     qrp_any(x, A);
     apply_qh_left_any(x, A, C);
     cplx* rinv = reinterpret_cast<cplx*>(x.s.vn1());
     double* dinv = x.s.u2();
-    diag_inverse(x.n, taud::LD, A, x.s.d(), rinv, dinv);
+    diag_inverse(x.n, taud::LD<NMAX>, A, x.s.d(), rinv, dinv);
     trsm_left_any(x, A, rinv, dinv, C);
     permute_rows_any(x, C, false);
 }
 
-DEVI void tau_copy(int n, cplx* dst, const cplx* src) {   // both with leading dimension taud::LD
+template <int NMAX>
+DEVI void tau_copy(int n, cplx* dst, const cplx* src) {   // both with the class's leading dimension
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - r * n;
-        dst[r * taud::LD + c] = src[r * taud::LD + c];
+        dst[r * taud::LD<NMAX> + c] = src[r * taud::LD<NMAX> + c];
     }
     __syncthreads();
 }
 
 // L1 distance of two n x n matrices (compare_mat, stabilization.f90:256-266),
 // valid in thread 0
-DEVI double tau_l1(Ctx<144>& x, int n, const cplx* a, const cplx* b) {
+template <int NMAX>
+DEVI double tau_l1(Ctx<NMAX>& x, int n, const cplx* a, const cplx* b) {
     double v[1] = {0.0};
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int r = e / n, c = e - r * n;
-        const cplx d = csub(a[r * taud::LD + c], b[r * taud::LD + c]);
+        const cplx d = csub(a[r * taud::LD<NMAX> + c], b[r * taud::LD<NMAX> + c]);
         v[0] += sqrt(d.x * d.x + d.y * d.y);
     }
     block_sum<1>(v, x.s.red());
@@ -1979,8 +1986,9 @@ DEVI double tau_l1(Ctx<144>& x, int n, const cplx* a, const cplx* b) {
 // slice nt (1-based, propgrU_R then propgrT_R, multiply.f90:48-97): the HS
 // factors of both channels, then e^{-dtau K} from the left and e^{+dtau K} from
 // the right (real, in the EP and EM slots)
-COLD void tau_slice(Ctx<144>& x, int nt) {
-    constexpr int LD = taud::LD;
+template <int NMAX>
+COLD void tau_slice(Ctx<NMAX>& x, int nt) {
+    constexpr int LD = taud::LD<NMAX>;
     const int n = x.n;
     const PointDev& P = x.P();
     cplx *T0 = taud::slot(x, taud::GT0), *T1 = taud::slot(x, taud::G0T), *T2 = taud::slot(x, taud::GTT);
@@ -2002,24 +2010,26 @@ COLD void tau_slice(Ctx<144>& x, int nt) {
     }
     const double *kp = reinterpret_cast<const double*>(taud::slot(x, taud::EP)),
                  *km = reinterpret_cast<const double*>(taud::slot(x, taud::EM));
-    gemm_real_any<144, false>(x, T0, kp, T0);
-    gemm_real_any<144, true>(x, T1, T1, km);
-    gemm_real_any<144, false>(x, T2, kp, T2);
-    gemm_real_any<144, true>(x, T2, T2, km);
-    gemm_real_any<144, false>(x, U, kp, U);
+    gemm_real_any<NMAX, false>(x, T0, kp, T0);
+    gemm_real_any<NMAX, true>(x, T1, T1, km);
+    gemm_real_any<NMAX, false>(x, T2, kp, T2);
+    gemm_real_any<NMAX, true>(x, T2, T2, km);
+    gemm_real_any<NMAX, false>(x, U, kp, U);
 }
 
 // Wrap_tau at slice nt (stabilization.f90:368-404): stab_UR of the propagated
 // right factors, the 2N x 2N inverse, the drifts of G(0,tau), G(tau,0),
 // G(tau,tau) against the propagated ones (thread 0 accumulates them in dr:
 // max[3], sum[3], non-finite count), then the replacement.
-COLD void tau_wrap(Ctx<144>& x, const Arena& A, int nt, double* dr) {
+template <int NMAX>
+COLD void tau_wrap(Ctx<NMAX>& x, const Arena& A, int nt, double* dr) {
     using namespace taud;
+    constexpr int LD = taud::LD<NMAX>;
     const int n = x.n, st = nt / x.P().Nwrap;
     cplx *W1 = x.W1(), *W2 = x.W2(), *U = x.U();
     cplx *M = slot(x, BIG), *Xi = slot(x, X), *VRi = slot(x, VRI), *VLi = slot(x, VLI), *ULs = slot(x, UL);
     stab_UR(x);                      // U = U_R, A.DRc = D_R, A.VRc and W2 = V_R
-    tau_copy(n, M, W2);
+    tau_copy<NMAX>(n, M, W2);
     set_identity(n, LD, VRi);
     __syncthreads();
     tau_solve(x, M, VRi);            // V_R^-1
@@ -2065,15 +2075,17 @@ COLD void tau_wrap(Ctx<144>& x, const Arena& A, int nt, double* dr) {
                 dr[6] += 1.0;
             }
         }
-        tau_copy(n, dst[k], W2);
+        tau_copy<NMAX>(n, dst[k], W2);
     }
 }
 
 // Dyn_reset + Dyn_sweep_R of one chain (dynamics.f90:37-57): copies of G and of
 // the right factors, L slices, a wrap every Nwrap slices; the arena's D_R and
 // V_R (which stab_UR updates) are put back at the end.
-COLD void tau_pass(Ctx<144>& x, const KernelArgs& ka, int chain) {
+template <int NMAX>
+COLD void tau_pass(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     using namespace taud;
+    constexpr int LD = taud::LD<NMAX>;
     const int n = x.n, L = x.P().L;
     const Arena A = x.A();
     cplx *G = x.G(), *T0 = slot(x, GT0), *T1 = slot(x, G0T), *T2 = slot(x, GTT);
@@ -2118,12 +2130,16 @@ COLD void tau_pass(Ctx<144>& x, const KernelArgs& ka, int chain) {
 }
 
 // One CTA per SM walks its share of the listed chains; its matrix region of
-// tau_region_elems() complex values is indexed by blockIdx.x.
-__global__ void __launch_bounds__(Cfg<144>::THREADS, 1) tau_kernel(KernelArgs ka, const int* idx, int count) {
+// tau_region_elems() complex values is indexed by blockIdx.x.  The N <= 72
+// class's kernel takes the chains with N <= 36, the N <= 144 class's those
+// with 36 < N <= kTauMaxN.
+template <int NMAX>
+__global__ void __launch_bounds__(Cfg<NMAX>::THREADS, 1) tau_kernel(KernelArgs ka, const int* idx, int count) {
     for (int k = blockIdx.x; k < count; k += gridDim.x) {
         const int chain = idx[k];
-        Ctx<144> x;
-        const bool ok = setup_ctx(x, ka, chain) && x.n <= kTauMaxN && !(x.sc->status & 1);
+        Ctx<NMAX> x;
+        const bool ok = setup_ctx(x, ka, chain) && 2 * x.n <= NMAX && (NMAX == 72 || 2 * x.n > 72) &&
+                        x.n <= kTauMaxN && !(x.sc->status & 1);
         if (ok) {
             x.wg = ka.tau_ws + (long long)blockIdx.x * taud::REGION;
             tau_pass(x, ka, chain);
@@ -2132,13 +2148,18 @@ __global__ void __launch_bounds__(Cfg<144>::THREADS, 1) tau_kernel(KernelArgs ka
     }
 }
 
+template <int NMAX>
+static cudaError_t launch_tau_cls(const KernelArgs& ka, const int* idx, int count, int grid, cudaStream_t st) {
+    const size_t sm = Smem<NMAX>::bytes();
+    const cudaError_t e = cudaFuncSetAttribute(tau_kernel<NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    tau_kernel<NMAX><<<grid < count ? grid : count, Cfg<NMAX>::THREADS, sm, st>>>(ka, idx, count);
+    return cudaGetLastError();
+}
 cudaError_t launch_tau(const KernelArgs& ka, const int* idx, int count, int grid, cudaStream_t st) {
     if (count <= 0) return cudaSuccess;
-    const size_t sm = Smem<144>::bytes();
-    const cudaError_t e = cudaFuncSetAttribute(tau_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    tau_kernel<<<grid < count ? grid : count, Cfg<144>::THREADS, sm, st>>>(ka, idx, count);
-    return cudaGetLastError();
+    const cudaError_t e = launch_tau_cls<72>(ka, idx, count, grid, st);
+    return e != cudaSuccess ? e : launch_tau_cls<144>(ka, idx, count, grid, st);
 }
 
 // ---------------------------------------------------------------------------

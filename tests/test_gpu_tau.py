@@ -13,6 +13,8 @@
   functions at a wrap slice and a propagated slice within 1e-9 of the largest
   entry, and the drifts Wrap_tau records are rounding-level (below 1e-9 of
   sum |G|; the reference warns at 5.5e-5).
+* 8x8 (N = 64, the pass in the larger size class): the four functions within
+  1e-9 at a wrap slice and a propagated slice (measured 1.4e-11 and 8e-11).
 * Refusals: Nambu chains, Ndim > 72, a probe slice outside 0..Ltrot.
 """
 import numpy as np
@@ -145,6 +147,26 @@ def test_time_displaced_functions_6x6_beta8(mods):
     print("device drifts", st[0, :3], "oracle", ch.pg.Xmaxm)
     assert st[0, 6] == 2 and st[0, 7] == 0
     assert np.all(st[0, 0:3] < 1e-9 * scale), st[0]
+
+
+def test_time_displaced_functions_8x8_larger_class(mods):
+    """N = 64 (36 < N <= 72): the pass runs in the N <= 144 class's context (2N = 128)."""
+    solver, _ = mods
+    kw = dict(KW, Nlx=8, Nly=8, NlxTherm=8, NlyTherm=8)
+    op, sp = O.Params(**kw), SolverParams(**kw)
+    _, _, (ch,) = O.init_chains(op, seeds=[77])
+    ch.pre()
+    with solver.Ensemble([sp], [0]) as ens:
+        ens.fields_from_seeds([77])
+        ens.pre()
+        for probe in (5, 12):
+            ens.set_time_displaced(True, probe)
+            ens.sweep(1)
+            worst = _compare(ens.time_displaced_probe(0), _oracle_bin(ch, probe), 1e-9, probe)
+            print(f"8x8 slice {probe}: max relative error {worst:.2e}")
+            s, phis = ens.get_state()
+            assert int(s[0]) == ch.seed
+            np.testing.assert_array_equal(phis[0], ch.phi)
 
 
 def test_refusals(mods):
