@@ -1106,9 +1106,6 @@ int bafqmc_set_time_displaced(bafqmc_handle* h, int enable, int probe_nt) {
     }
     for (int c = 0; c < h->nchains; ++c) {
         const PointHost& p = h->pts[h->chain_point[c]];
-        if (p.pairing)
-            return fail(BAFQMC_EUNSUPPORTED, "the time-displaced pass runs number-conserving chains only (chain " +
-                                                 std::to_string(c) + " is a Nambu chain)");
         if (p.N > bq::kTauMaxN)
             return fail(BAFQMC_EUNSUPPORTED, "the time-displaced pass needs N <= " + std::to_string(bq::kTauMaxN) +
                                                  " (chain " + std::to_string(c) + " has N = " + std::to_string(p.N) + ")");

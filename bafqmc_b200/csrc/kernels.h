@@ -31,9 +31,10 @@ struct KernelArgs {
     int tau_probe_nt = 0;
 };
 
-// time-displaced pass of number-conserving chains with N <= kTauMaxN (2N x 2N
-// inverse in the N <= 144 routines).  Per chain: drift max of G(0,tau),
-// G(tau,0), G(tau,tau), their sums, passes run, non-finite recomputations.
+// time-displaced pass of chains with N <= kTauMaxN (the Nambu chains' {b, c^dagger}
+// block; 2N x 2N inverse in the N <= 72 or N <= 144 routines).  Per chain: drift
+// max of G(0,tau), G(tau,0), G(tau,tau), their sums, passes run, non-finite
+// recomputations.
 constexpr int kTauMaxN = 72;
 constexpr int kTauStats = 8;
 constexpr long long kTauProbeElems = 4LL * kTauMaxN * kTauMaxN;   // G(0,0), G(0,tau), G(tau,0), G(tau,tau)

@@ -1983,9 +1983,9 @@ DEVI double tau_l1(Ctx<NMAX>& x, int n, const cplx* a, const cplx* b) {
     return v[0];
 }
 
-// slice nt (1-based, propgrU_R then propgrT_R, multiply.f90:48-97): the HS
-// factors of both channels, then e^{-dtau K} from the left and e^{+dtau K} from
-// the right (real, in the EP and EM slots)
+// slice nt (1-based, propgrU_R then propgrT_R, multiply.f90:48-97 of both
+// solvers): the HS factors of both channels, then e^{-dtau K} from the left and
+// e^{+dtau K} from the right (real, in the EP and EM slots)
 template <int NMAX>
 COLD void tau_slice(Ctx<NMAX>& x, int nt) {
     constexpr int LD = taud::LD<NMAX>;
@@ -1996,8 +1996,18 @@ COLD void tau_slice(Ctx<NMAX>& x, int nt) {
     cplx *ep = x.s.ean(), *em = x.s.ebn();
     for (int ch = 0; ch < 2; ++ch) {
         if (!P.active[ch]) continue;
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-            hs_factors(P.alpha_re[ch], P.alpha_im[ch], x.phi[((long)(nt - 1) * n + i) * 2 + ch], ep[i], em[i]);
+        // row i's factor e^{+-alpha phi}; on a Nambu chain's {b, c^dagger} block
+        // row Ns + i (c^dagger_i) takes site i's field, with the inverse factor in
+        // a flipped channel (src/pairing/src/operator_Hubbard.f90:139-199)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const bool cd = i >= P.Ns;
+            const int site = cd ? i - P.Ns : i;
+            cplx a, b;
+            hs_factors(P.alpha_re[ch], P.alpha_im[ch], x.phi[((long)(nt - 1) * P.Ns + site) * 2 + ch], a, b);
+            const bool inv = cd && P.flip[ch];
+            ep[i] = inv ? b : a;
+            em[i] = inv ? a : b;
+        }
         __syncthreads();
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
             const int r = e / n, c = e - r * n;

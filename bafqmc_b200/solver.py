@@ -431,11 +431,10 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
     run_dir = Path(run_dir)
     t0 = time.time()
     p = SolverParams.from_file(run_dir / "paramC_sets.txt", pairing=pairing)
-    if p.is_tau and (pairing or p.Ndim > 72):
-        # the time-displaced pass (dynamics.f90) is built for number-conserving chains with Ndim <= 72
-        raise ParamError("is_tau = .true. (line 5 of paramC_sets.txt) is supported for number-conserving runs with "
-                         f"Ndim <= 72 only (this run: {'Nambu' if pairing else 'Ndim = %d' % p.Ndim}); "
-                         "set is_tau = .false.")
+    if p.is_tau and p.block_dim > 72:
+        # the time-displaced pass (dynamics.f90) is built for stored dimensions up to 72
+        raise ParamError("is_tau = .true. (line 5 of paramC_sets.txt) is supported up to a stored dimension of 72 "
+                         f"(this run: {p.block_dim}); set is_tau = .false.")
     info = open(run_dir / "info.txt", "w")
     w = lambda label, v: info.write(f" {label:<47}:{_scalar(v)!r:>26}\n")
     if pairing:   # write_info (src/pairing/src/calc_basic.f90:140-180)
@@ -513,6 +512,8 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
         # Xmaxm(1..3) hold the drifts of G(0,tau), G(tau,0), G(tau,tau) in that order
         # (stabilization.f90:384-398) while the lines name them GRtt, GRt0, GR0t.
         ts = ens.time_displaced_stats()
+        if pairing:   # the reference's 4Ns matrices hold the block and its complex conjugate
+            ts[:, :6] *= 2.0
         tau_record = {"tau_passes": int(ts[:, 6].sum()), "tau_drift_max": [float(ts[:, k].max()) for k in range(3)],
                       "tau_nonfinite": int(ts[:, 7].sum())}
         norm = nchains * p.Nbin * p.Nst * p.Nsweep

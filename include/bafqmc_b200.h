@@ -307,8 +307,11 @@ int bafqmc_set_precision(bafqmc_handle* h, int mode);
  * propagates G(tau,0), G(0,tau) and G(tau,tau) slice by slice and every Nwrap
  * slices recomputes them from the stabilised factors (Wrap_tau,
  * stabilization.f90:368-404), recording the L1 drift of each.  The Markov chain
- * is unchanged (the pass works on copies).  Number-conserving chains with
- * N <= 72 only (BAFQMC_EUNSUPPORTED otherwise).  The U2 operator uses the U2
+ * is unchanged (the pass works on copies).  Chains with N <= 72 (for a Nambu
+ * chain N is its stored {b, c^dagger} block, 2 Lx Ly, and the pass works on
+ * that block of the reference's 4Ns matrices; BAFQMC_EUNSUPPORTED above).  The
+ * reference's L1 drifts on the 4Ns matrices are twice the block's (the
+ * {c, b^dagger} block is its complex conjugate).  The U2 operator uses the U2
  * field and the 2N x 2N matrix the bosonic sign; dynamics.f90:52 passes the U1
  * field to the U2 operator and stabilization.f90:206-209 use the fermion sign,
  * both of which this library does not reproduce.
@@ -321,7 +324,8 @@ int bafqmc_set_time_displaced(bafqmc_handle* h, int enable, int probe_nt);
  * the copy. */
 int bafqmc_time_displaced_stats(bafqmc_handle* h, double* out, int reset);
 /* out: 4 row-major N x N complex matrices (interleaved re, im) of the chain:
- * G(0,0), G(0,tau), G(tau,0), G(tau,tau) at the probe slice of the last pass. */
+ * G(0,0), G(0,tau), G(tau,0), G(tau,tau) at the probe slice of the last pass
+ * (a Nambu chain: their {b, c^dagger} blocks). */
 int bafqmc_time_displaced_probe(bafqmc_handle* h, int chain, double* out);
 
 /* Per-phase SM cycle counters of the sweep kernel (the reference has only a

@@ -1143,9 +1143,10 @@ class Chain:
         wr.UR[st] = pr.UUR; wr.VR[st] = pr.VUR; wr.DR[st] = pr.DUR
 
     # ---- time-displaced Green's functions (dynamics.f90:38-58, multiply.f90:48-97,
-    # Wrap_tau stabilization.f90:368-404), number-conserving chains
+    # Wrap_tau stabilization.f90:368-404)
     def tau_sweep_R(self, u2_slot_bug: bool = False, fermion_sign: bool = False, on_slice=None):
-        """Dyn_reset + Dyn_sweep_R at the start of a right traversal: G(tau,0),
+        """Dyn_reset + Dyn_sweep_R at the start of a right traversal (both solvers;
+        the pairing solver's dynamics.f90 is the same code on its 4Ns matrices): G(tau,0),
         G(0,tau) and G(tau,tau) propagated slice by slice from G(0,0), recomputed by
         stab_green_big every Nwrap slices, the drifts recorded in self.pg.
         The reference passes the U1 field slot to the U2 operator
@@ -1164,6 +1165,16 @@ class Chain:
                 if not self.op[nf].active:
                     continue
                 slot = 0 if (u2_slot_bug and nf == 1) else nf
+                if p.pairing:   # propgrU_R of the pairing solver (src/pairing/src/multiply.f90:48-64)
+                    for ii in range(p.Nsite):
+                        ph = self.phi[nt - 1, ii, slot]
+                        self._mmult_R(pg.Grt0, nf, ii, ph, 1)
+                        self._mmult_L(pg.Gr0t, nf, ii, ph, -1)
+                        self._mmult_R(pg.Grtt, nf, ii, ph, 1)
+                        self._mmult_L(pg.Grtt, nf, ii, ph, -1)
+                    for ii in range(p.Nsite):
+                        self._mmult_R(prop.UUR, nf, ii, self.phi[nt - 1, ii, slot], 1)
+                    continue
                 ep = np.array([self._expalpha(nf, self.phi[nt - 1, ii, slot], 1) for ii in range(p.Ndim)])
                 em = np.array([self._expalpha(nf, self.phi[nt - 1, ii, slot], -1) for ii in range(p.Ndim)])
                 pg.Grt0 = ep[:, None] * pg.Grt0

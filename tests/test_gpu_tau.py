@@ -15,7 +15,9 @@
   sum |G|; the reference warns at 5.5e-5).
 * 8x8 (N = 64, the pass in the larger size class): the four functions within
   1e-9 at a wrap slice and a propagated slice (measured 1.4e-11 and 8e-11).
-* Refusals: Nambu chains, Ndim > 72, a probe slice outside 0..Ltrot.
+* A Nambu chain: the {b, c^dagger} block of the oracle's 4Ns functions.
+* Refusals: Ndim > 72, a probe slice outside 0..Ltrot, statistics before the
+  pass was enabled.
 """
 import numpy as np
 import pytest
@@ -169,14 +171,38 @@ def test_time_displaced_functions_8x8_larger_class(mods):
             np.testing.assert_array_equal(phis[0], ch.phi)
 
 
+def test_nambu_time_displaced_functions_match_oracle(mods):
+    """A Nambu chain (3x3, Delta = 0.3, beta = 1): the device's pass on the
+    {b, c^dagger} block against that block of the oracle's 4Ns functions
+    (src/pairing/src/dynamics.f90 restated in oracle.Chain.tau_sweep_R), at a
+    propagated slice, a wrap slice and the last slice: within 1e-9 of each
+    block's largest entry; seeds and fields bit-exact."""
+    solver, _ = mods
+    from test_gpu_pairing import oracle_block, pair_params
+    op, sp = pair_params(0.3, mu=-5.0, Nlx=3, Nly=3, Ltrot=20, Beta=1.0, Nwrap=5, Nbin=1)
+    seeds = [41, 42]
+    _, _, chains = O.init_chains(op, seeds=seeds)
+    for ch in chains:
+        ch.pre()
+    with solver.Ensemble([sp], [0] * len(seeds)) as ens:
+        ens.fields_from_seeds(seeds)
+        ens.pre()
+        for probe in (3, 5, 20):
+            ens.set_time_displaced(True, probe)
+            ens.sweep(1)
+            s, phis = ens.get_state()
+            for c, ch in enumerate(chains):
+                ora = [oracle_block(m, op.Lq) for m in _oracle_bin(ch, probe)]
+                worst = _compare(ens.time_displaced_probe(c), ora, 1e-9, (probe, c))
+                print(f"Nambu slice {probe} chain {c}: max relative error {worst:.2e}")
+                assert int(s[c]) == ch.seed
+                np.testing.assert_array_equal(phis[c], ch.phi)
+        st = ens.time_displaced_stats()
+    assert np.all(st[:, 6] == 3) and np.all(st[:, 7] == 0)
+
+
 def test_refusals(mods):
     solver, _lib = mods
-    from test_gpu_pairing import pair_params
-    _, sp = pair_params(0.5, mu=-5.0, Nlx=3, Nly=3, Ltrot=8, Beta=0.4, Nwrap=4)
-    with solver.Ensemble([sp], [0]) as ens:
-        with pytest.raises(_lib.BafqmcError) as ei:
-            ens.set_time_displaced(True)
-        assert ei.value.code == -3
     big = SolverParams(**dict(KW, Nlx=12, Nly=12, NlxTherm=12, NlyTherm=12))
     with solver.Ensemble([big], [0]) as ens:
         with pytest.raises(_lib.BafqmcError) as ei:

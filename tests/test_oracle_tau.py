@@ -101,3 +101,48 @@ def test_a_sweep_with_the_pass_keeps_the_markov_chain():
     assert runs[0][0] == runs[1][0]
     np.testing.assert_array_equal(runs[0][1], runs[1][1])
     np.testing.assert_array_equal(runs[0][2], runs[1][2])
+
+
+def test_pairing_pass_matches_dense_products():
+    """The pairing solver's pass (src/pairing/src/dynamics.f90, multiply.f90:48-97)
+    on the 4Ns matrices: the propagated functions equal the dense products of
+    the slice matrices (B_nt = e^{-dtau H} D_nt, D_nt from opU_mmult_R on the
+    identity; G(tau,0) = B G to 1e-10, the two with B^-1 to the dense inverse's
+    own accuracy, 1e-14 cond(B)), the stabilised G(0,0) block reproduces G, and the functions keep
+    the block structure of the Nambu matrices ({b, c^dagger} and {c, b^dagger}
+    decoupled)."""
+    p = O.Params(U1=1.0, U2=-0.5, mu=-5.0, Nlx=3, Nly=3, Ltrot=20, Beta=1.0, NlxTherm=3, NlyTherm=3,
+                 LtrotTherm=20, Nwrap=5, Nbin=1, Nsweep=1, shiftLoc=1.5, iniType=2, iniAmpl=1.0, RDelta=0.3,
+                 pairing=True)
+    _, opT, (ch,) = O.init_chains(p, seeds=[5])
+    ch.pre()
+    ch.sweep_L()
+    G = ch.prop.Gr.copy()
+    n = G.shape[0]
+    eye = np.eye(n)
+    rec = {}
+    ch.tau_sweep_R(on_slice=lambda nt, pg: rec.__setitem__(nt, (pg.Gr00.copy(), pg.Gr0t.copy(), pg.Grt0.copy(),
+                                                                   pg.Grtt.copy())))
+    B = np.eye(n, dtype=complex)
+    ns = p.Lq
+    blk = list(range(ns)) + list(range(3 * ns, 4 * ns))
+    off = [i for i in range(n) if i not in blk]
+    for nt in range(1, p.Ltrot + 1):
+        D = np.eye(n, dtype=complex)
+        for nf in (0, 1):
+            if ch.op[nf].active:
+                for ii in range(p.Nsite):
+                    ch._mmult_R(D, nf, ii, ch.phi[nt - 1, ii, nf], 1)
+        B = opT.expT_P @ D @ B
+        g00, g0t, gt0, gtt = rec[nt]
+        Binv = np.linalg.inv(B)
+        # the dense inverse carries ~cond(B) eps (cond(B) reaches 8e6 at nt = 15, 1.5e9 at nt = 20)
+        tol_inv = max(1e-10, 1e-14 * np.linalg.cond(B))
+        for got, want, tol in ((gt0, B @ G, 1e-10), (g0t, -(eye - G) @ Binv, tol_inv),
+                               (gtt, B @ G @ Binv, tol_inv)):
+            scale = max(1.0, np.max(np.abs(want)))
+            assert np.max(np.abs(got - want)) <= tol * scale, nt
+            assert np.max(np.abs(got[np.ix_(blk, off)])) <= 1e-12 * scale
+        if nt % p.Nwrap == 0:
+            assert np.max(np.abs(g00 - G)) <= 1e-10 * max(1.0, np.max(np.abs(G)))
+    assert max(ch.pg.Xmaxm) < 1e-10 * np.sum(np.abs(G))
