@@ -212,3 +212,31 @@ def test_nambu_6x6_in_the_n72_class(solver_mod):
     """2Ns = 72: G and U in shared memory, the two workspaces in HBM."""
     op, sp = pair_params(0.5, mu=-6.0, Nlx=6, Nly=6, Ltrot=20, Beta=1.0, Nwrap=5)
     _run_both([op], [sp], [0, 0], [606, 607], nbins=1)
+
+
+def test_run_directory_pairing_time_displaced(solver_mod, tmp_path):
+    """The pairing program with is_tau = .true. and Nthermal = 1 over 2 bins: the
+    pass runs in bin 2 only, info.txt gets Dyn_control_print's six lines after
+    the acceptance and phase lines, with the drifts of the 4Ns matrices (twice
+    the stored block's), and the checkpoint equals a run without the pass."""
+    import dataclasses
+    _, sp = pair_params(0.3, Nbin=2)
+    out = {}
+    for tau in (False, True):
+        d = tmp_path / ("tau" if tau else "plain")
+        d.mkdir()
+        (d / "paramC_sets.txt").write_text(dataclasses.replace(sp, is_tau=tau, Nthermal=1).to_text())
+        (d / "confin.txt").write_text("0\n")
+        (d / "seeds.txt").write_text("4099\n777\n")
+        solver_mod.run_directory(d, nchains=2, pairing=True)
+        out[tau] = d
+    assert (out[False] / "confout.txt").read_text() == (out[True] / "confout.txt").read_text()
+    lines = (out[True] / "info.txt").read_text().splitlines()
+    labels = [ln.split(":")[0].strip() for ln in lines]
+    i = labels.index("Max diff GRtt")
+    assert labels[i:i + 6] == ["Max diff GRtt", "Mean diff GRtt", "Max diff GRt0", "Mean diff GRt0",
+                               "Max diff GR0t", "Mean diff GR0t"]
+    vals = [float(lines[i + k].split(":")[1]) for k in range(6)]
+    assert all(0 < v < 1e-8 for v in vals), vals
+    rec = json.loads((out[True] / "run_record.json").read_text())
+    assert rec["tau_passes"] == 2 and rec["tau_nonfinite"] == 0
