@@ -230,9 +230,6 @@ struct bafqmc_handle {
     double* d_stats = nullptr;   // [npts*stride] x (current block sum, mean, sem, then stats_max block means)
     cudaGraphExec_t bin_graph = nullptr;
     int graph_nsweep = 0, graph_timers = 0, graph_mixed = 0, graph_tau = 0, graph_probe = 0;
-    // one stream per kernel class: a bin's class launches run concurrently (record_bin)
-    cudaStream_t cls_stream[bq::kNumClasses] = {};
-    cudaEvent_t ev_fork = nullptr, ev_cls[bq::kNumClasses] = {};
     // time-displaced pass (bafqmc_set_time_displaced): the chains it runs, one
     // matrix region per CTA, per-chain drift statistics, the optional probe
     int tau_on = 0, tau_probe_nt = 0, tau_grid = 0;
@@ -392,11 +389,6 @@ void free_handle(bafqmc_handle* h) {
     for (int c = 0; c < bq::kNumClasses; ++c)
         if (h->d_cls[c]) cudaFree(h->d_cls[c]);
     if (h->bin_graph) cudaGraphExecDestroy(h->bin_graph);
-    for (int c = 0; c < bq::kNumClasses; ++c) {
-        if (h->cls_stream[c]) cudaStreamDestroy(h->cls_stream[c]);
-        if (h->ev_cls[c]) cudaEventDestroy(h->ev_cls[c]);
-    }
-    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -509,13 +501,6 @@ int bafqmc_create_tuned(const bafqmc_point* pts, int npts, const int32_t* chain_
     };
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(e, "cudaStreamCreate");
-    for (int c = 0; c < bq::kNumClasses; ++c) {
-        if ((e = cudaStreamCreateWithFlags(&h->cls_stream[c], cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&h->ev_cls[c], cudaEventDisableTiming)) != cudaSuccess)
-            return bail(e, "class streams");
-    }
-    if ((e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming)) != cudaSuccess)
-        return bail(e, "cudaEventCreate");
     // a^k mod 2^31 table for the in-kernel skip-ahead of the LCG
     std::vector<uint32_t> apow(bq::kMaxPow);
     unsigned long long v = 1;
@@ -718,56 +703,28 @@ int bafqmc_pre(bafqmc_handle* h) {
 }
 
 namespace {
-// The classes' launches between a fork and a join run concurrently, each
-// non-empty class on its own stream: chains of different classes share
-// nothing, so their order does not matter.
-cudaError_t fork_classes(bafqmc_handle* h) {
-    cudaError_t e = cudaEventRecord(h->ev_fork, h->stream);
-    for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
-        if (!h->cls_list[c].empty()) e = cudaStreamWaitEvent(h->cls_stream[c], h->ev_fork, 0);
-    return e;
-}
-cudaError_t join_classes(bafqmc_handle* h) {
-    cudaError_t e = cudaSuccess;
-    for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
-        if (!h->cls_list[c].empty()) {
-            e = cudaEventRecord(h->ev_cls[c], h->cls_stream[c]);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->ev_cls[c], 0);
-        }
-    return e;
-}
-cudaError_t sweep_classes(bafqmc_handle* h, const bq::KernelArgs& k) {
-    cudaError_t e = cudaSuccess;
-    for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
-        e = bq::launch_sweep(c, k, h->d_cls[c], (int)h->cls_list[c].size(), h->cls_stream[c]);
-    return e;
-}
-
 // The launches of one bin: accumulator reset, nsweep persistent sweep launches
-// per kernel class (the classes concurrently), bin averages.  With the
-// time-displaced pass on, each sweep is a left-traversal launch per class, the
-// pass over all chains, and a right-traversal launch per class (Local_sweep_R's
-// toggle, local_sweep.f90:119-123).
+// per kernel class, bin averages.  With the time-displaced pass on, each sweep
+// is a left-traversal launch, the pass, and a right-traversal launch
+// (Local_sweep_R's toggle, local_sweep.f90:119-123).
 cudaError_t record_bin(bafqmc_handle* h, int nsweep) {
     const bq::KernelArgs ka = h->args();
     bq::KernelArgs kl = ka, kr = ka;
     kl.traverse = 1;
     kr.traverse = 2;
     cudaError_t e = bq::launch_bin_reset(ka, h->stream);
-    if (e == cudaSuccess) e = fork_classes(h);
     for (int s = 0; s < nsweep && e == cudaSuccess; ++s) {
         if (h->tau_on) {
-            e = sweep_classes(h, kl);
-            if (e == cudaSuccess) e = join_classes(h);
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, kl, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
             if (e == cudaSuccess) e = bq::launch_tau(ka, h->d_tau_idx, h->nchains, h->tau_grid, h->stream);
-            if (e == cudaSuccess) e = fork_classes(h);
-            if (e == cudaSuccess) e = sweep_classes(h, kr);
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, kr, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
         } else {
-            e = sweep_classes(h, ka);
+            for (int c = 0; c < bq::kNumClasses && e == cudaSuccess; ++c)
+                e = bq::launch_sweep(c, ka, h->d_cls[c], (int)h->cls_list[c].size(), h->stream);
         }
     }
-    const cudaError_t ej = join_classes(h);   // every forked stream rejoins, also after an error
-    if (e == cudaSuccess) e = ej;
     if (e == cudaSuccess) e = bq::launch_bin_finish(ka, h->stream);
     return e;
 }
