@@ -21,13 +21,12 @@ template <int NMAX> struct Cfg;
 // R8 rows per lane and CPS columns per 8-lane segment for the register-resident
 // factorisation routines: R8 >= NMAX/8, CPS >= NMAX/(THREADS/8).
 // LD: leading dimension of the shared-memory matrices, odd so that a column
-// walk over 16-byte elements touches all eight bank groups.  NB: threads of the
-// site strip (>= NMAX, a multiple of 32).  MINB: CTAs per SM for the register
+// walk over 16-byte elements touches all eight bank groups.  MINB: CTAs per SM for the register
 // budget.  GW: the two workspaces live in HBM (after the chain's arena) and
 // only G and U in shared memory.
 template <> struct Cfg<16> {
     static constexpr bool TCORE = false;
-    static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, NB = 64, MINB = 2;
+    static constexpr int THREADS = 128, TR = 1, TC = 2, MAXE = 2, KB = 4, R8 = 2, CPS = 1, LD = 17, MINB = 2;
     static constexpr bool GW = false, GG = false;
     static constexpr int RW = 1, CPW = 1;
 };
@@ -37,14 +36,14 @@ static_assert(16 % 1 == 0 && 16 % 2 == 0, "tile must divide NMAX");
 // slice products and wraps slow down more than the third chain adds.)
 template <> struct Cfg<36> {
     static constexpr bool TCORE = false;
-    static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, NB = 64, MINB = 2;
+    static constexpr int THREADS = 256, TR = 2, TC = 3, MAXE = 6, KB = 4, R8 = 5, CPS = 2, LD = 37, MINB = 2;
     static constexpr bool GW = false, GG = false;
     static constexpr int RW = 2, CPW = 1;
 };
 // N <= 72: G and U in shared memory, the workspaces in HBM (one CTA per SM)
 template <> struct Cfg<72> {
     static constexpr bool TCORE = false;
-    static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = 73, NB = 96, MINB = 1;
+    static constexpr int THREADS = 512, TR = 3, TC = 4, MAXE = 11, KB = 4, R8 = 9, CPS = 2, LD = 73, MINB = 1;
     static constexpr bool GW = true, GG = false;
     static constexpr int RW = 3, CPW = 1;
 };
@@ -57,7 +56,7 @@ template <> struct Cfg<72> {
 static_assert(kTcPer * 512 >= 144 * kTcKC, "tensor-core staging: elements per thread must cover a chunk");
 template <> struct Cfg<144> {
     static constexpr bool TCORE = true;   // slice products may run on the tensor cores (tc.cuh)
-    static constexpr int THREADS = 512, TR = 2, TC = 3, MAXE = 41, KB = 4, R8 = 18, CPS = 3, LD = 145, NB = 160,
+    static constexpr int THREADS = 512, TR = 2, TC = 3, MAXE = 41, KB = 4, R8 = 18, CPS = 3, LD = 145,
                          MINB = 1;
     static constexpr bool GW = true, GG = true;
     static constexpr int RW = 5, CPW = 2;
@@ -68,7 +67,7 @@ constexpr bool cfg_ok() {
     return NMAX % C::TR == 0 && NMAX % C::TC == 0 && (C::GG || (NMAX / C::TR) * (NMAX / C::TC) <= C::THREADS) &&
            (!C::GG || (C::RW * 32 >= NMAX && C::THREADS >= NMAX && C::GW)) &&
            C::MAXE * C::THREADS >= NMAX * NMAX && C::R8 * 8 >= NMAX && C::CPS * (C::THREADS / 8) >= NMAX &&
-           C::NB >= NMAX && C::NB % 32 == 0 && C::NB <= C::THREADS && (C::LD & 1) == 1 && C::LD >= NMAX;
+           (C::LD & 1) == 1 && C::LD >= NMAX;
 }
 static_assert(cfg_ok<16>() && cfg_ok<36>() && cfg_ok<72>() && cfg_ok<144>(),
               "class tiles and register layouts must cover NMAX");
@@ -177,7 +176,7 @@ struct Ctx {
     ChainScalars* sc;
     cplx* wg;   // HBM region after the arena: W1, W2 (N > 36), then G, U and a product scratch (N > 72)
     int n;
-    int sw0;    // first warp of the site strip
+    int sw0;    // the local update's deciding warp
     DEVI const PointDev& P() const { return *s.P(); }
     DEVI Arena A() const { return make_arena(abase, n); }
     DEVI cplx* W1() const {
@@ -502,7 +501,7 @@ DEVI cplx wrap_col(const Smem<NMAX>& s, int c) {
     else return s.ebo()[c];
 }
 
-// Step 1, by the lead warp (the site strip's first warp).  Lane l < KB*KB holds
+// Step 1, by the lead warp (warp sw0 of the CTA).  Lane l < KB*KB holds
 // the element (l / KB, l % KB) of the block's kb x kb submatrix of the current
 // G; the decisions run in visiting order, every lane computing the same
 // Metropolis ratio from the diagonal element it receives by shuffle.  Records
@@ -721,8 +720,8 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     }
     __syncthreads();
 
-    // Blocks of KB sites in visiting order.  The lead warp (the site strip's first
-    // warp) decides block b + 1 while the other warps run block b's rank pass: it
+    // Blocks of KB sites in visiting order.  The lead warp (warp sw0) decides
+    // block b + 1 while the other warps run block b's rank pass: it
     // copies block b + 1's submatrix during block b's vector step (G is not
     // written then) and adds block b's terms itself, exactly as the pass does.  The last block's pass applies the channel's deferred wrap.
     constexpr int NT = Cfg<NMAX>::THREADS;
@@ -766,7 +765,7 @@ COLD void prop_channel(Ctx<NMAX> x, int ch, int slice) {
     // accepted fields, counters, seed, and the U factor wrap with the final fields
     for (int i = tid; i < n; i += blockDim.x)
         if (s.accf()[i]) phis[i * 2 + ch] = s.phin()[i];
-    if (tid == 32 * x.sw0) {   // the strip's first thread: AccCounter%count, kept in shared memory
+    if (tid == 32 * x.sw0) {   // the lead thread: AccCounter%count, kept in shared memory
         s.cnt()[ch] += nacc;
         s.cnt()[2 + ch] += n;
         *s.seed() = lcg_mul(c_apow[2 * n], s0);
@@ -1461,10 +1460,10 @@ DEVI bool setup_ctx(Ctx<NMAX>& x, const KernelArgs& ka, int chain) {
     const ChainDev cd = ka.chains[chain];
     if (threadIdx.x == 0) {
         *x.s.P() = ka.pts[cd.point];
-        // The SM's schedulers take warps by slot modulo 4, so the site strips of
-        // two CTAs on one SM would share two schedulers if both used warps 0-1.
-        // A CTA whose warp slots start at an odd multiple of 8 runs its strip on
-        // warps 2-3.  Thread 0 decides for the whole CTA.
+        // The SM's schedulers take warps by slot modulo 4, so the deciding warps
+        // of two CTAs on one SM would share a scheduler if both used warp 0.  A
+        // CTA whose warp slots start at an odd multiple of 8 decides on warp 2.
+        // Thread 0 decides for the whole CTA.
         unsigned slot;
         asm volatile("mov.u32 %0, %%warpid;" : "=r"(slot));
         *x.s.strip_warp() = (Cfg<NMAX>::THREADS >= 192 && ((slot >> 3) & 1)) ? 2 : 0;
