@@ -1113,21 +1113,44 @@ int bafqmc_set_time_displaced(bafqmc_handle* h, int enable, int probe_nt) {
             return fail(BAFQMC_EARG, "probe slice outside 0..Ltrot");
     }
     CK(cudaSetDevice(h->device));
-    if (!h->d_tau_idx) {
+    // each buffer on its own, so that a failed allocation is retried by the next call
+    if (!h->tau_grid) {
         int sms = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
         h->tau_grid = std::max(1, std::min(sms, h->nchains));
+    }
+    if (!h->d_tau_idx) {
         std::vector<int> idx(h->nchains);
         for (int c = 0; c < h->nchains; ++c) idx[c] = c;
-        CK(cudaMalloc(&h->d_tau_idx, sizeof(int) * h->nchains));
-        CK(cudaMemcpy(h->d_tau_idx, idx.data(), sizeof(int) * h->nchains, cudaMemcpyHostToDevice));
-        CK(cudaMalloc(&h->d_tau_ws, sizeof(double2) * bq::tau_region_elems() * h->tau_grid));
-        CK(cudaMalloc(&h->d_tau_stats, sizeof(double) * bq::kTauStats * h->nchains));
-        CK(cudaMemset(h->d_tau_stats, 0, sizeof(double) * bq::kTauStats * h->nchains));
+        int* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(int) * h->nchains));
+        const cudaError_t e = cudaMemcpy(p, idx.data(), sizeof(int) * h->nchains, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_fail(e, "chain list of the time-displaced pass");
+        }
+        h->d_tau_idx = p;
+    }
+    if (!h->d_tau_ws) CK(cudaMalloc(&h->d_tau_ws, sizeof(double2) * bq::tau_region_elems() * h->tau_grid));
+    if (!h->d_tau_stats) {
+        double* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(double) * bq::kTauStats * h->nchains));
+        const cudaError_t e = cudaMemset(p, 0, sizeof(double) * bq::kTauStats * h->nchains);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_fail(e, "drift statistics of the time-displaced pass");
+        }
+        h->d_tau_stats = p;
     }
     if (probe_nt > 0 && !h->d_tau_probe) {
-        CK(cudaMalloc(&h->d_tau_probe, sizeof(double2) * bq::kTauProbeElems * h->nchains));
-        CK(cudaMemset(h->d_tau_probe, 0, sizeof(double2) * bq::kTauProbeElems * h->nchains));
+        double2* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(double2) * bq::kTauProbeElems * h->nchains));
+        const cudaError_t e = cudaMemset(p, 0, sizeof(double2) * bq::kTauProbeElems * h->nchains);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_fail(e, "probe of the time-displaced pass");
+        }
+        h->d_tau_probe = p;
     }
     h->tau_on = 1;
     h->tau_probe_nt = probe_nt;
