@@ -421,6 +421,9 @@ def read_confin_npz(path: Path, p: SolverParams, nchains: int):
     return [(int(seeds[c]), phi[c]) for c in range(nchains)]
 
 
+UNSTABLE_DRIFT = 5.5e-5   # the reference's warning threshold (stabilization.f90:320, 358)
+
+
 def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print,
                   pairing: bool = False) -> dict:
     """The reference program for `mpirun -np nchains` in run_dir, on one GPU.
@@ -490,6 +493,22 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
             if c not in seen:   # the reference has no counterpart: it would carry the NaN on
                 seen.add(c)
                 log(f" WARNING: chain {c} quarantined after bin {nbc + 1}: non-finite Green's function")
+        # the reference's stability warnings (stabilization.f90:320, 358, 387-397): a drift
+        # of 5.5e-5 or more between the propagated and the recomputed functions, here once
+        # per chain and kind, from the drift maxima after each bin
+        drift = ens.counters()[:, 4]
+        for c in np.nonzero(drift >= UNSTABLE_DRIFT)[0]:
+            if ("G", c) not in seen:
+                seen.add(("G", c))
+                log(f" WARNING: chain {c}: drift {drift[c]:.3e} >= {UNSTABLE_DRIFT} by bin {nbc + 1} (ortho unstable)")
+        if istau:
+            ts = ens.time_displaced_stats() * (2.0 if pairing else 1.0)
+            for k, name in enumerate(("GR0T", "GRT0", "GRTT")):
+                for c in np.nonzero(ts[:, k] >= UNSTABLE_DRIFT)[0]:
+                    if (name, c) not in seen:
+                        seen.add((name, c))
+                        log(f" WARNING: chain {c}: {name} drift {ts[c, k]:.3e} >= {UNSTABLE_DRIFT} by bin {nbc + 1} "
+                            "(ortho unstable)")
         append_bin(run_dir, ens.point_obs()[0], pairing=pairing)
         if pole and not pairing:
             append_pole(run_dir, ens.pole_diagnostics())
