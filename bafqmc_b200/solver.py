@@ -424,6 +424,29 @@ def read_confin_npz(path: Path, p: SolverParams, nchains: int):
 UNSTABLE_DRIFT = 5.5e-5   # the reference's warning threshold (stabilization.f90:320, 358)
 
 
+def drift_warnings(drift, tau_stats, seen: set, nbin: int, log=print) -> list[str]:
+    """The reference's stability warnings (stabilization.f90:320, 358, 387-397): a
+    drift of 5.5e-5 or more between the propagated and the recomputed functions.
+    The reference prints one line per wrap; here one line per chain and kind, from
+    the drift maxima after bin nbin (drift: per chain, of G; tau_stats: the
+    time-displaced statistics, or None).  seen holds what was reported already.
+    Returns the new lines."""
+    out = []
+    kinds = [("G", np.asarray(drift))]
+    if tau_stats is not None:
+        kinds += [(name, np.asarray(tau_stats)[:, k]) for k, name in enumerate(("GR0T", "GRT0", "GRTT"))]
+    for name, d in kinds:
+        for c in np.nonzero(d >= UNSTABLE_DRIFT)[0]:
+            if (name, int(c)) in seen:
+                continue
+            seen.add((name, int(c)))
+            what = "drift" if name == "G" else f"{name} drift"
+            out.append(f" WARNING: chain {int(c)}: {what} {d[c]:.3e} >= {UNSTABLE_DRIFT} by bin {nbin} (ortho unstable)")
+    for line in out:
+        log(line)
+    return out
+
+
 def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True, log=print,
                   pairing: bool = False) -> dict:
     """The reference program for `mpirun -np nchains` in run_dir, on one GPU.
@@ -493,22 +516,8 @@ def run_directory(run_dir, nchains: int = 1, device: int = 0, pole: bool = True,
             if c not in seen:   # the reference has no counterpart: it would carry the NaN on
                 seen.add(c)
                 log(f" WARNING: chain {c} quarantined after bin {nbc + 1}: non-finite Green's function")
-        # the reference's stability warnings (stabilization.f90:320, 358, 387-397): a drift
-        # of 5.5e-5 or more between the propagated and the recomputed functions, here once
-        # per chain and kind, from the drift maxima after each bin
-        drift = ens.counters()[:, 4]
-        for c in np.nonzero(drift >= UNSTABLE_DRIFT)[0]:
-            if ("G", c) not in seen:
-                seen.add(("G", c))
-                log(f" WARNING: chain {c}: drift {drift[c]:.3e} >= {UNSTABLE_DRIFT} by bin {nbc + 1} (ortho unstable)")
-        if istau:
-            ts = ens.time_displaced_stats() * (2.0 if pairing else 1.0)
-            for k, name in enumerate(("GR0T", "GRT0", "GRTT")):
-                for c in np.nonzero(ts[:, k] >= UNSTABLE_DRIFT)[0]:
-                    if (name, c) not in seen:
-                        seen.add((name, c))
-                        log(f" WARNING: chain {c}: {name} drift {ts[c, k]:.3e} >= {UNSTABLE_DRIFT} by bin {nbc + 1} "
-                            "(ortho unstable)")
+        ts = (ens.time_displaced_stats() * (2.0 if pairing else 1.0)) if istau else None
+        drift_warnings(ens.counters()[:, 4], ts, seen, nbc + 1, log)
         append_bin(run_dir, ens.point_obs()[0], pairing=pairing)
         if pole and not pairing:
             append_pole(run_dir, ens.pole_diagnostics())

@@ -110,3 +110,24 @@ def test_time_displaced_request_outside_its_range_is_refused(tmp_path):
     with pytest.raises(ParamError, match="is_tau"):
         run_directory(tmp_path, nchains=1)
     assert not (tmp_path / "info.txt").exists()
+
+
+def test_drift_warnings_once_per_chain_and_kind():
+    """The reference warns when a recomputed Green's function moved by 5.5e-5 or more
+    (stabilization.f90:320, 358, 387-397); run directories report it once per
+    chain and kind, from the drift maxima after each bin."""
+    import numpy as np
+    from bafqmc_b200.solver import drift_warnings
+    seen, lines = set(), []
+    drift = np.array([1e-12, 6e-5, 5.5e-5, 1e-3])
+    ts = np.zeros((4, 8))
+    ts[1, 1] = 1e-4   # G(tau,0) of chain 1
+    new = drift_warnings(drift, ts, seen, 1, lines.append)
+    assert new == lines and len(new) == 4
+    assert [ln.split(":")[0] for ln in new] == [" WARNING", " WARNING", " WARNING", " WARNING"]
+    assert "chain 1: drift" in new[0] and "chain 2: drift" in new[1] and "chain 3: drift" in new[2]
+    assert "chain 1: GRT0 drift" in new[3]
+    # already reported: nothing new; a new chain crossing the threshold is
+    drift[0] = 1.0
+    assert len(drift_warnings(drift, ts, seen, 2, lines.append)) == 1 and "by bin 2" in lines[-1]
+    assert drift_warnings(drift, None, seen, 3, lines.append) == []
